@@ -1,0 +1,207 @@
+/* macis_b200 -- C ABI of the B200 (sm_100a) selected-CI hot path.
+ *
+ * Plain pointers and sizes only. Each entry point names the reference MACIS
+ * interface it replaces (paths relative to the MACIS source tree). The C++
+ * drop-in shim include/macis_b200/macis_b200.hpp wraps these calls behind
+ * the reference's own template API; INTEGRATION.md shows the bindings.
+ *
+ * Determinants: arrays of little-endian uint64 words, nbits/64 words per
+ * determinant, in the std::bitset<nbits> layout (nbits = 64, 128 or 256):
+ *   nbits=64 : word0 bits 0..31 alpha, bits 32..63 beta
+ *   nbits=128: word0 alpha, word1 beta
+ *   nbits=256: words 0-1 alpha, words 2-3 beta
+ * Integrals: column-major T(p,q) = T[p + q*LDT], V(p,q,r,s) =
+ * V[p + LDV*(q + LDV*(r + LDV*s))] (include/macis/types.hpp:22-33).
+ *
+ * Memory: pointer arguments are host memory unless MACIS_B200_DEVICE_PTRS is
+ * set in `flags`, in which case they are device (HBM) pointers on the
+ * library's current device. All calls are synchronous at return and run on
+ * one CUDA stream per handle. Handles are not thread-safe (neither is the
+ * reference generator).
+ *
+ * Errors: every call returns 0 or one of the MACIS_B200_E* codes below;
+ * macis_b200_last_error() returns the message of the last failure on the
+ * calling thread. The C++ shim rethrows std::runtime_error with the
+ * reference's messages.
+ */
+#ifndef MACIS_B200_H
+#define MACIS_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MACIS_B200_OK 0
+#define MACIS_B200_EINVAL 1    /* bad argument */
+#define MACIS_B200_ENOMEM 2    /* device allocation failed */
+#define MACIS_B200_ECAPACITY 3 /* result exceeds the index type / buffer */
+#define MACIS_B200_ETIMEOUT 4  /* a bounded device wait gave up */
+#define MACIS_B200_ENOCONV 5   /* Davidson did not converge */
+#define MACIS_B200_ECUDA 6     /* CUDA runtime error */
+#define MACIS_B200_ENOGROW 7   /* ASCI search returned too few dets */
+
+#define MACIS_B200_DEVICE_PTRS 1u /* pointer arguments are device memory */
+
+/* Davidson precision modes. */
+#define MACIS_B200_FP64 0  /* FP64 H values and FP64 vectors */
+#define MACIS_B200_MIXED 1 /* FP32 off-diagonal H, FP64 diagonal, FP64
+                              residual / CGS2 / Rayleigh-Ritz / energy */
+
+typedef struct macis_b200_ham macis_b200_ham;
+typedef struct macis_b200_csr macis_b200_csr;
+
+/* ASCI settings, field for field macis::ASCISettings
+ * (include/macis/asci/determinant_search.hpp:34-51). */
+typedef struct {
+  uint64_t ntdets_max, ntdets_min, ncdets_max;
+  double h_el_tol, rv_prune_tol;
+  uint64_t pair_size_max;
+  int32_t just_singles, pad_;
+  uint64_t grow_factor, max_refine_iter;
+  double refine_energy_tol;
+} macis_b200_asci_settings;
+
+/* Diagnostics of the last asci_search call on a handle. */
+typedef struct {
+  uint64_t raw_pairs;     /* contributions generated (after h_el_tol) */
+  uint64_t unique_pairs;  /* after sort + accumulate */
+  uint64_t kept_pairs;    /* after dropping core dets and zero scores */
+  uint64_t batches;       /* core-det batches used */
+  double pairs_ms, sort_ms, keep_ms, topk_ms, total_ms;
+} macis_b200_asci_stats;
+
+const char* macis_b200_last_error(void);
+int macis_b200_version(void);
+/* Number of kernels this library has launched in the process (benchmark
+ * diagnostics; no reference counterpart). */
+unsigned long long macis_b200_launch_count(void);
+
+/* --- Hamiltonian generator ------------------------------------------------
+ * Replaces the HamiltonianGenerator<N> constructor and
+ * generate_integral_intermediates (include/macis/hamiltonian_generator.hpp:75,
+ * hamiltonian_generator/impl.hpp:26-70): uploads T, V and builds G, G_red,
+ * V_red, G2_red, V2_red in HBM. T and V are host pointers. */
+int macis_b200_ham_create(int nbits, size_t norb, const double* T, size_t LDT,
+                          const double* V, size_t LDV, macis_b200_ham** out);
+int macis_b200_ham_destroy(macis_b200_ham* h);
+
+/* Batched HamiltonianGenerator::matrix_element(bra, ket)
+ * (hamiltonian_generator/matrix_elements.hpp:15-32). */
+int macis_b200_matrix_element(macis_b200_ham* h, const uint64_t* bra,
+                              const uint64_t* ket, size_t n, double* out,
+                              unsigned flags);
+
+/* --- CSR Hamiltonian build ------------------------------------------------
+ * Replaces the make_csr_hamiltonian_block_32bit_/64bit_ virtual hook of
+ * HamiltonianGenerator (hamiltonian_generator.hpp:66-72) as implemented by
+ * DoubleLoopHamiltonianGenerator::make_csr_hamiltonian_block_
+ * (hamiltonian_generator/double_loop.hpp:31-98): rows follow the bra list,
+ * columns are ascending ket indices, entries with |h| > H_thresh are kept,
+ * zero determinants give empty rows/columns. idx_bytes = 4 (int32_t) or 8
+ * (int64_t); val_bytes = 8 (FP64 values) or 4 (FP32 off-diagonal values
+ * with the FP64 diagonal kept separately, the MIXED precision mode). The
+ * matrix stays in HBM, owned by the returned handle. */
+int macis_b200_build_csr(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
+                         const uint64_t* ket, size_t nket, double H_thresh,
+                         int idx_bytes, int val_bytes, unsigned flags,
+                         macis_b200_csr** out);
+int macis_b200_csr_destroy(macis_b200_csr* A);
+/* m, n, nnz, idx_bytes, val_bytes of a built matrix. */
+int macis_b200_csr_info(const macis_b200_csr* A, int64_t* m, int64_t* n,
+                        int64_t* nnz, int* idx_bytes, int* val_bytes);
+/* Copy the CSR arrays out (the by-value sparsexx::csr_matrix return of the
+ * hook, sparsexx/matrix_types/csr_matrix.hpp:67-76): rowptr (m+1) and colind
+ * (nnz) of idx_bytes each, nzval (nnz) of val_bytes each. Any pointer may be
+ * NULL to skip that array. */
+int macis_b200_csr_download(const macis_b200_csr* A, void* rowptr,
+                            void* colind, void* nzval, unsigned flags);
+/* Diagonal of the matrix, FP64 (sparsexx/util/submatrix.hpp:264-292). */
+int macis_b200_csr_diagonal(const macis_b200_csr* A, double* D,
+                            unsigned flags);
+
+/* AV = alpha * A * V + beta * AV for K column vectors (column-major, leading
+ * dimensions LDV, LDAV). Replaces sparsexx::spblas::gespmbv
+ * (sparsexx/spblas/spmbv.hpp:39-73) behind SparseMatrixOperator::
+ * operator_action (include/macis/solvers/davidson.hpp:47-58). */
+int macis_b200_spmv(const macis_b200_csr* A, int64_t K, double alpha,
+                    const double* V, int64_t LDV, double beta, double* AV,
+                    int64_t LDAV, unsigned flags);
+
+/* Single-vector Davidson for the lowest eigenpair of A, replacing
+ * macis::davidson (include/macis/solvers/davidson.hpp:129-225) with the
+ * diagonal preconditioner and CGS2 of the reference. X holds the guess on
+ * entry when use_guess != 0 (else the diagonal_guess unit vector,
+ * davidson.hpp:62-68) and the Ritz vector on exit. The precision follows
+ * the matrix: val_bytes=8 is MACIS_B200_FP64, val_bytes=4 MACIS_B200_MIXED.
+ * Returns MACIS_B200_ENOCONV (message "Davidson Did Not Converge!") when the
+ * residual stays above tol after max_m basis vectors. */
+int macis_b200_davidson(const macis_b200_csr* A, int64_t max_m, double tol,
+                        int use_guess, double* X, double* E, int64_t* niter,
+                        unsigned flags);
+
+/* Davidson options beyond the reference signature. restart_keep = 0 keeps
+ * the reference behaviour (no restart: stop after max_m basis vectors);
+ * restart_keep > 0 compresses a full basis to its lowest restart_keep Ritz
+ * vectors and continues (thick restart) until max_iter total iterations
+ * (0: unbounded). */
+typedef struct {
+  int64_t max_m;
+  double tol;
+  int32_t use_guess;
+  int32_t restart_keep;
+  int64_t max_iter;
+} macis_b200_davidson_opts;
+int macis_b200_davidson_ex(const macis_b200_csr* A,
+                           const macis_b200_davidson_opts* opts, double* X,
+                           double* E, int64_t* niter, unsigned flags);
+
+/* Lowest nwant eigenpairs (W ascending, eigenvectors in the columns of Vec,
+ * ld k) of the symmetric k x k matrix whose lower triangle is `lower`
+ * (column-major, ld k): the syev step of lobpcgxx::rayleigh_ritz
+ * (src/lobpcgxx/include/lobpcgxx/rayleigh_ritz.hpp:70-77) used inside
+ * Davidson. Host-only; needs no GPU. */
+int macis_b200_small_syev(int k, const double* lower, int nwant, double* W,
+                          double* Vec);
+
+/* Timings of the last build of a CSR handle (CUDA events on the build
+ * stream): whole build, the fill kernel (the HBM-bound writer of colind /
+ * nzval), the candidate count before thresholding and the path taken. */
+typedef struct {
+  double build_ms, fill_ms;
+  int64_t nnz_candidates;
+  int32_t direct_product, long_rows;
+} macis_b200_build_stats;
+int macis_b200_csr_build_stats(const macis_b200_csr* A,
+                               macis_b200_build_stats* out);
+
+/* --- ASCI search ----------------------------------------------------------
+ * Replaces macis::asci_search (include/macis/asci/determinant_search.hpp:
+ * 395-663) at MPI world size 1: singles/doubles contributions of the core
+ * dets (determinant_contributions.hpp:26-160), sort + accumulate
+ * (determinant_sort.hpp:40-83), core merge (determinant_sort.hpp:86-120,
+ * determinant_search.hpp:528-544) and top-k (determinant_search.hpp:622-626).
+ * out_dets must hold ndets_max + ncdets determinants; *nout receives the
+ * count. The top-k states come first in ascending determinant order (ties at
+ * the k-th score resolved towards smaller determinants), followed by the core
+ * dets in input order. C holds the ncdets core coefficients. */
+int macis_b200_asci_search(macis_b200_ham* h,
+                           const macis_b200_asci_settings* s,
+                           size_t ndets_max, const uint64_t* cdets,
+                           size_t ncdets, double E0, const double* C,
+                           uint64_t* out_dets, size_t* nout, unsigned flags);
+/* The accumulated (state, score) pairs before the core merge -- the list the
+ * reference top-k works on (determinant_search.hpp:498). Two calls: with
+ * states == NULL only *npairs is set. States ascend. */
+int macis_b200_asci_pairs(macis_b200_ham* h, const macis_b200_asci_settings* s,
+                          const uint64_t* cdets, size_t ncdets, double E0,
+                          const double* C, uint64_t* states, double* rv,
+                          size_t* npairs);
+int macis_b200_asci_last_stats(const macis_b200_ham* h,
+                               macis_b200_asci_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

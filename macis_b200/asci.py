@@ -1,0 +1,187 @@
+"""ASCI drivers on the B200.
+
+* ``ASCISettings`` / ``MCSCFSettings`` -- include/macis/asci/
+  determinant_search.hpp:34-51 and include/macis/util/mcscf.hpp:15-30
+* ``asci_search``  -- determinant_search.hpp:395-663 (GPU search)
+* ``reorder_ci_on_coeff`` -- asci/determinant_sort.hpp:19-37 (stable)
+* ``asci_iter``    -- asci/iteration.hpp:17-68
+* ``asci_grow``    -- asci/grow.hpp:17-171 (the natural-orbital rotation
+  branch, grow_with_rot, is not part of this path)
+* ``asci_refine``  -- asci/refine.hpp:15-66
+
+The search returns the top-k states in ascending determinant order followed
+by the core determinants; the reference returns them in nth_element order.
+"""
+import ctypes as ct
+import logging
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import LIB, check
+from .solvers import FP64, selected_ci_diag
+
+__all__ = ["ASCISettings", "MCSCFSettings", "asci_search", "asci_pairs",
+           "asci_iter", "asci_grow", "asci_refine", "reorder_ci_on_coeff",
+           "last_search_stats"]
+
+
+@dataclass
+class ASCISettings:
+    ntdets_max: int = 100000
+    ntdets_min: int = 100
+    ncdets_max: int = 100
+    h_el_tol: float = 1e-8
+    rv_prune_tol: float = 1e-8
+    pair_size_max: int = 500000000
+    just_singles: bool = False
+    grow_factor: int = 8
+    max_refine_iter: int = 6
+    refine_energy_tol: float = 1e-6
+    grow_with_rot: bool = False
+    rot_size_start: int = 1000
+    constraint_level: int = 2
+
+    def c_struct(self):
+        return _lib.AsciSettingsC(
+            int(self.ntdets_max), int(self.ntdets_min), int(self.ncdets_max),
+            float(self.h_el_tol), float(self.rv_prune_tol),
+            int(self.pair_size_max), int(bool(self.just_singles)), 0,
+            int(self.grow_factor), int(self.max_refine_iter),
+            float(self.refine_energy_tol))
+
+
+@dataclass
+class MCSCFSettings:
+    ci_res_tol: float = 1e-8
+    ci_max_subspace: int = 20
+    ci_matel_tol: float = float(np.finfo(np.float64).eps)
+    precision: str = FP64  # FP64 or MIXED Davidson inside asci_iter
+    # thick restart of the Davidson (0: the reference solver, no restart)
+    davidson_restart_keep: int = 0
+    davidson_max_iter: int = 0
+    iteration_log: list = field(default_factory=list)
+
+
+def reorder_ci_on_coeff(dets, C):
+    """Sort by |C| descending; equal magnitudes keep their order."""
+    order = np.argsort(-np.abs(C), kind="stable")
+    return dets[order], C[order]
+
+
+def _dets(d, nbits):
+    return np.ascontiguousarray(d, dtype=np.uint64).reshape(-1, nbits // 64)
+
+
+def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen):
+    """New determinant list: top-(ndets_max - ncdets) contributions then the
+    core determinants (determinant_search.hpp:395-663)."""
+    log = logging.getLogger("asci_search")
+    cdets = _dets(cdets, ham_gen.nbits)
+    C = np.ascontiguousarray(C, dtype=np.float64)[:len(cdets)]
+    s = asci_settings.c_struct()
+    out = np.empty((int(ndets_max) + len(cdets), ham_gen.nbits // 64),
+                   dtype=np.uint64)
+    nout = ct.c_size_t()
+    check(LIB.macis_b200_asci_search(ham_gen.handle, ct.byref(s),
+                                     int(ndets_max), cdets.ctypes.data,
+                                     len(cdets), float(E_ASCI), C.ctypes.data,
+                                     out.ctypes.data, ct.byref(nout), 0))
+    st = last_search_stats(ham_gen)
+    log.info("  * ASCI Kept %d Pairs; %d unique; PAIR_DUR = %.2e s, "
+             "SORT_ACC_DUR = %.2e s, ASCI_SEARCH DUR = %.2e s",
+             st["raw_pairs"], st["unique_pairs"], st["pairs_ms"] / 1e3,
+             st["sort_ms"] / 1e3, st["total_ms"] / 1e3)
+    return out[:nout.value]
+
+
+def asci_pairs(asci_settings, cdets, E_ASCI, C, ham_gen):
+    """Accumulated (states, rv) before the core merge, states ascending."""
+    cdets = _dets(cdets, ham_gen.nbits)
+    C = np.ascontiguousarray(C, dtype=np.float64)[:len(cdets)]
+    s = asci_settings.c_struct()
+    n = ct.c_size_t()
+    check(LIB.macis_b200_asci_pairs(ham_gen.handle, ct.byref(s),
+                                    cdets.ctypes.data, len(cdets),
+                                    float(E_ASCI), C.ctypes.data, None, None,
+                                    ct.byref(n)))
+    st = np.empty((max(n.value, 1), ham_gen.nbits // 64), dtype=np.uint64)
+    rv = np.empty(max(n.value, 1))
+    check(LIB.macis_b200_asci_pairs(ham_gen.handle, ct.byref(s),
+                                    cdets.ctypes.data, len(cdets),
+                                    float(E_ASCI), C.ctypes.data,
+                                    st.ctypes.data, rv.ctypes.data,
+                                    ct.byref(n)))
+    return st[:n.value], rv[:n.value]
+
+
+def last_search_stats(ham_gen):
+    st = _lib.AsciStatsC()
+    check(LIB.macis_b200_asci_last_stats(ham_gen.handle, ct.byref(st)))
+    return {k: getattr(st, k) for k, _ in st._fields_}
+
+
+def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
+              norb):
+    """One ASCI iteration: reorder, search on the ncdets_max largest, then
+    rediagonalise without guess reuse (iteration.hpp:17-68)."""
+    wfn = _dets(wfn, ham_gen.nbits)
+    X = np.asarray(X, dtype=np.float64)
+    if len(wfn) > 1:
+        wfn, X = reorder_ci_on_coeff(wfn, X)
+    nkeep = min(int(asci_settings.ncdets_max), len(wfn))
+    t0 = time.perf_counter()
+    wfn = asci_search(asci_settings, ndets_max, wfn[:nkeep], E0, X[:nkeep],
+                      norb, ham_gen)
+    t1 = time.perf_counter()
+    tim = {}
+    E, X = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,
+                            mcscf_settings.ci_max_subspace,
+                            mcscf_settings.ci_res_tol, None,
+                            precision=mcscf_settings.precision, timings=tim,
+                            restart_keep=mcscf_settings.davidson_restart_keep,
+                            max_iter=mcscf_settings.davidson_max_iter)
+    t2 = time.perf_counter()
+    mcscf_settings.iteration_log.append(dict(
+        ndets=len(wfn), E=E, search_ms=(t1 - t0) * 1e3,
+        diag_ms=(t2 - t1) * 1e3, **tim))
+    return E, wfn, X
+
+
+def asci_grow(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb):
+    log = logging.getLogger("asci_grow")
+    wfn = _dets(wfn, ham_gen.nbits)
+    if asci_settings.grow_with_rot:
+        raise NotImplementedError("grow_with_rot is outside the GPU path")
+    it = 1
+    while len(wfn) < asci_settings.ntdets_max:
+        ndets_new = min(max(asci_settings.ntdets_min,
+                            len(wfn) * asci_settings.grow_factor),
+                        asci_settings.ntdets_max)
+        E, wfn, X = asci_iter(asci_settings, mcscf_settings, ndets_new, E0,
+                              wfn, X, ham_gen, norb)
+        if ndets_new > len(wfn):
+            raise RuntimeError("Wavefunction didn't grow enough...")
+        log.info("iter = %4d, E0 = %20.12e, dE = %14.6e, WFN_SIZE = %d", it, E,
+                 E - E0, len(wfn))
+        it += 1
+        E0 = E
+    return E0, wfn, X
+
+
+def asci_refine(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb):
+    log = logging.getLogger("asci_refine")
+    ndets = len(wfn)
+    for it in range(asci_settings.max_refine_iter):
+        E, wfn, X = asci_iter(asci_settings, mcscf_settings, ndets, E0, wfn, X,
+                              ham_gen, norb)
+        if len(wfn) != ndets:
+            raise RuntimeError("Wavefunction size can't change in refinement")
+        dE = E - E0
+        log.info("iter = %4d, E0 = %20.12e, dE = %14.6e", it + 1, E, dE)
+        E0 = E
+        if abs(dE) < asci_settings.refine_energy_tol:
+            return E0, wfn, X
+    raise RuntimeError("ACCI Refine did not converge")

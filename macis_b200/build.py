@@ -1,0 +1,66 @@
+"""Build libmacis_b200.so in-tree with nvcc for sm_100a.
+
+    python macis_b200/build.py
+
+The library is written next to this file so that it ships with the source
+tree; it is the only native artefact the package loads.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libmacis_b200.so")
+SOURCES = ["ham.cu", "hbuild.cu", "spmv.cu", "davidson.cu", "asci.cu",
+           "capi.cu"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+         "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3"]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose=False, jobs=None):
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+               if f.endswith((".cuh", ".hpp"))]
+    headers.append(os.path.join(HERE, "..", "include", "macis_b200.h"))
+    objs, procs = [], []
+    for src in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(objdir, src.replace(".cu", ".o"))
+        objs.append(o)
+        if _stale(o, [s] + headers):
+            cmd = [NVCC] + ARCH + FLAGS + ["-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd))
+            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                                stderr=subprocess.STDOUT)))
+    failed = []
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            failed.append(out.decode())
+        elif verbose and out:
+            print(out.decode())
+    if failed:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(failed))
+    if _stale(OUT, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", OUT] + objs
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv)
+    print(OUT)

@@ -1,0 +1,751 @@
+// ASCI search on the GPU, replacing macis::asci_search at MPI world size 1
+// (include/macis/asci/determinant_search.hpp:395-663):
+//
+//  1. per core det: occupied/virtual lists, orbital energies
+//     (single_orbital_ens, fast_diagonals.hpp:34-53) and H_ii
+//  2. contributions (determinant_contributions.hpp:26-160) in two passes --
+//     a count pass over "units" (singles of a spin, or one (i,a) outer pair
+//     of a double loop) and a fill pass writing every (det, rv) record at its
+//     exact position -- so the raw list is the reference push_back order
+//  3. stable radix sort by determinant and a sequential per-segment sum:
+//     duplicates are added in generation order (sort_and_accumulate_asci_pairs,
+//     determinant_sort.hpp:40-83)
+//  4. drop core dets and zero scores (keep_only_largest_copy_asci_pairs +
+//     partition, determinant_sort.hpp:86-120, determinant_search.hpp:528-544)
+//  5. top-k by |rv| with an MSD radix select; ties at the k-th score are
+//     resolved towards smaller determinants (determinant_search.hpp:622-626
+//     leaves them unspecified)
+//
+// Core dets are processed in batches sized to the free HBM; batch results are
+// merged into the running unique list by a merge-path style rank merge.
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+
+#include "internal.hpp"
+#include "primitives.cuh"
+
+namespace mb {
+
+constexpr int MAXORB = 128;
+
+struct CoreData {
+  int n;
+  const uint64_t* dets;  // ncdets x NW
+  const double* C;
+  size_t ncdets;
+  uint8_t* occ;   // ncdets x 2 x MAXORB  (alpha, beta) ascending occupied
+  uint8_t* vir;   // ncdets x 2 x MAXORB  ascending virtual (below n)
+  uint8_t* cnt;   // ncdets x 4: nocc_a, nocc_b, nvir_a, nvir_b
+  double* eps;    // ncdets x 2 x n
+  double* hd;     // ncdets
+  int64_t* uoff;  // ncdets+1 unit offsets
+};
+
+// Per core det precompute; one warp per det (bitset_to_occ_vir,
+// sd_operations.hpp:82-97; single_orbital_ens; matrix_element diag).
+template <int NBITS>
+__global__ void core_prep_k(Ints I, CoreData cd, int just_singles,
+                            int64_t* units) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  const int lane = threadIdx.x & 31;
+  const int n = cd.n;
+  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
+  for(size_t c = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      c < cd.ncdets; c += nwarp) {
+    const uint64_t* d = cd.dets + c * D::NW;
+    const Spin<NSW> sp[2] = {D::alpha(d), D::beta(d)};
+    int no[2], nv[2];
+    for(int s = 0; s < 2; ++s) {
+      // lists: lane 0 writes sequentially (n <= 128)
+      if(lane == 0) {
+        int a = 0, v = 0;
+        for(int i = 0; i < n; ++i) {
+          if(sp_test(sp[s], i))
+            cd.occ[(c * 2 + s) * MAXORB + a++] = uint8_t(i);
+          else
+            cd.vir[(c * 2 + s) * MAXORB + v++] = uint8_t(i);
+        }
+      }
+      no[s] = sp_popc(sp[s]);
+      nv[s] = n - no[s];
+    }
+    if(lane == 0) {
+      cd.cnt[c * 4 + 0] = uint8_t(no[0]);
+      cd.cnt[c * 4 + 1] = uint8_t(no[1]);
+      cd.cnt[c * 4 + 2] = uint8_t(nv[0]);
+      cd.cnt[c * 4 + 3] = uint8_t(nv[1]);
+      cd.hd[c] = me_diag(I, sp[0], sp[1]);
+      const int64_t u = just_singles
+                            ? 2
+                            : 2 + int64_t(no[0]) * nv[0] + int64_t(no[1]) * nv[1] +
+                                  int64_t(no[0]) * nv[0];
+      units[c] = u;
+    }
+    // eps_same for spin s: ss = sp[s], os = sp[1-s]
+    for(int s = 0; s < 2; ++s)
+      for(int i = lane; i < n; i += 32) {
+        double e = __ldg(I.T + size_t(i) * (n + 1));
+        for(Spin<NSW> q = sp[s]; sp_popc(q);) {
+          const int p = sp_lowest(q);
+          q = sp_flip(q, p);
+          e += __ldg(I.G2_red + i + size_t(p) * n) + __ldg(I.G2_red + p + size_t(i) * n);
+        }
+        e -= __ldg(I.G2_red + size_t(i) * (n + 1));
+        for(Spin<NSW> q = sp[1 - s]; sp_popc(q);) {
+          const int p = sp_lowest(q);
+          q = sp_flip(q, p);
+          e += __ldg(I.V2_red + i + size_t(p) * n);
+        }
+        cd.eps[(c * 2 + s) * n + i] = e;
+      }
+  }
+}
+
+template <int NBITS>
+__device__ __forceinline__ void det_flip(uint64_t* d, int spin, int orb) {
+  if constexpr(NBITS == 64) {
+    d[0] ^= 1ull << (orb + 32 * spin);
+  } else if constexpr(NBITS == 128) {
+    d[spin] ^= 1ull << orb;
+  } else {
+    d[2 * spin + (orb >> 6)] ^= 1ull << (orb & 63);
+  }
+}
+
+#define G2R(p, q) __ldg(I.G2_red + (p) + size_t(q) * n)
+#define V2R(p, q) __ldg(I.V2_red + (p) + size_t(q) * n)
+
+// One unit of contributions; MODE 0 counts, MODE 1 writes. Warp-synchronous.
+template <int NBITS, int MODE>
+__device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
+                         double E0, double tol, int64_t* count_out,
+                         int64_t out0, uint64_t* keys, double* rv) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  const int lane = threadIdx.x & 31;
+  const int n = cd.n;
+  const int nA = cd.cnt[c * 4], nB = cd.cnt[c * 4 + 1];
+  const int nvA = cd.cnt[c * 4 + 2], nvB = cd.cnt[c * 4 + 3];
+  const uint8_t* occA = cd.occ + (c * 2) * MAXORB;
+  const uint8_t* occB = cd.occ + (c * 2 + 1) * MAXORB;
+  const uint8_t* virA = cd.vir + (c * 2) * MAXORB;
+  const uint8_t* virB = cd.vir + (c * 2 + 1) * MAXORB;
+  const double* epsA = cd.eps + (c * 2) * n;
+  const double* epsB = cd.eps + (c * 2 + 1) * n;
+  const double coeff = cd.C[c], hii = cd.hd[c];
+  const uint64_t* det = cd.dets + c * D::NW;
+  const Spin<NSW> sA = D::alpha(det), sB = D::beta(det);
+
+  // decode the unit
+  int kind, ii = 0, aa = 0;
+  int64_t ninner;
+  if(t == 0) {
+    kind = 0;
+    ninner = int64_t(nA) * nvA;
+  } else if(t == 1) {
+    kind = 1;
+    ninner = int64_t(nB) * nvB;
+  } else if(t < 2 + int64_t(nA) * nvA) {
+    kind = 2;
+    ii = int((t - 2) / nvA);
+    aa = int((t - 2) % nvA);
+    ninner = int64_t(nA - 1 - ii) * (nvA - 1 - aa);
+  } else if(t < 2 + int64_t(nA) * nvA + int64_t(nB) * nvB) {
+    kind = 3;
+    const int64_t u = t - 2 - int64_t(nA) * nvA;
+    ii = int(u / nvB);
+    aa = int(u % nvB);
+    ninner = int64_t(nB - 1 - ii) * (nvB - 1 - aa);
+  } else {
+    kind = 4;
+    const int64_t u = t - 2 - int64_t(nA) * nvA - int64_t(nB) * nvB;
+    ii = int(u / nvA);
+    aa = int(u % nvA);
+    ninner = int64_t(nB) * nvB;
+  }
+  int64_t done = 0;
+  for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
+    const int64_t q = q0 + lane;
+    bool keep = false;
+    double r = 0;
+    uint64_t ex[D::NW];
+    if(q < ninner) {
+      if(kind <= 1) {
+        // append_singles_asci_contributions (determinant_contributions.hpp:25-66)
+        const int S = kind;
+        const int nS = S ? nB : nA, nvS = S ? nvB : nvA;
+        const uint8_t* occS = S ? occB : occA;
+        const uint8_t* virS = S ? virB : virA;
+        const int nO = S ? nA : nB;
+        const uint8_t* occO = S ? occA : occB;
+        const int i = occS[q / nvS], a = virS[q % nvS];
+        double h = __ldg(I.T + a + size_t(i) * n);
+        const double* Gov = I.G_red + size_t(a) * n + size_t(i) * n * n;
+        const double* Vov = I.V_red + size_t(a) * n + size_t(i) * n * n;
+        for(int p = 0; p < nS; ++p) h += __ldg(Gov + occS[p]);
+        for(int p = 0; p < nO; ++p) h += __ldg(Vov + occO[p]);
+        keep = !(fabs(h) < tol);
+        if(MODE == 1 && keep) {
+          const double* eps = S ? epsB : epsA;
+          h *= ex_sign(S ? sB : sA, a, i);
+          const double hd = hii + eps[a] - eps[i] - G2R(a, i) - G2R(i, a);
+          h /= (E0 - hd);
+          r = coeff * h;
+#pragma unroll
+          for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
+          det_flip<NBITS>(ex, S, i);
+          det_flip<NBITS>(ex, S, a);
+        }
+        (void)nS;
+      } else if(kind <= 3) {
+        // append_ss_doubles_asci_contributions (determinant_contributions.hpp:68-120)
+        const int S = kind - 2;
+        const int nvS = S ? nvB : nvA;
+        const uint8_t* occS = S ? occB : occA;
+        const uint8_t* virS = S ? virB : virA;
+        const int span = nvS - 1 - aa;
+        const int jj = ii + 1 + int(q / span), bb = aa + 1 + int(q % span);
+        const int i = occS[ii], a = virS[aa], j = occS[jj], b = virS[bb];
+        const double Gv = __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
+        keep = !(fabs(Gv) < tol);
+        if(MODE == 1 && keep) {
+          const Spin<NSW> st = S ? sB : sA;
+          Spin<NSW> fx = sp_flip(sp_flip(sp_flip(sp_flip(sp_zero<NSW>(), i), j), a), b);
+          const uint32_t e = double_ex(st, st ^ fx);
+          double h = ex_sgn(e) * Gv;
+          const double* eps = S ? epsB : epsA;
+          const double hd = hii + eps[a] + eps[b] - eps[i] - eps[j] + G2R(i, j) +
+                            G2R(j, i) + G2R(a, b) + G2R(b, a) - G2R(a, i) -
+                            G2R(i, a) - G2R(b, i) - G2R(i, b) - G2R(a, j) -
+                            G2R(j, a) - G2R(b, j) - G2R(j, b);
+          h /= (E0 - hd);
+          r = coeff * h;
+#pragma unroll
+          for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
+          det_flip<NBITS>(ex, S, i);
+          det_flip<NBITS>(ex, S, j);
+          det_flip<NBITS>(ex, S, a);
+          det_flip<NBITS>(ex, S, b);
+        }
+      } else {
+        // append_os_doubles_asci_contributions (determinant_contributions.hpp:122-160)
+        const int i = occA[ii], a = virA[aa];
+        const int j = occB[q / nvB], b = virB[q % nvB];
+        const double Vv = __ldg(I.V + a + size_t(i) * n + size_t(b + size_t(j) * n) * n * n);
+        keep = !(fabs(Vv) < tol);
+        if(MODE == 1 && keep) {
+          const double sign = ex_sign(sA, a, i) * ex_sign(sB, b, j);
+          double h = sign * Vv;
+          const double hd = hii + epsA[a] + epsB[b] - epsA[i] - epsB[j] +
+                            V2R(i, j) + V2R(a, b) - G2R(a, i) - G2R(i, a) -
+                            G2R(b, j) - G2R(j, b) - V2R(a, j) - V2R(i, b);
+          h /= (E0 - hd);
+          r = coeff * h;
+#pragma unroll
+          for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
+          det_flip<NBITS>(ex, 0, a);
+          det_flip<NBITS>(ex, 0, i);
+          det_flip<NBITS>(ex, 1, j);
+          det_flip<NBITS>(ex, 1, b);
+        }
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if(MODE == 1 && keep) {
+      const int64_t pos = out0 + done + __popc(m & lanemask_lt());
+#pragma unroll
+      for(int w = 0; w < D::NW; ++w) keys[pos * D::NW + w] = ex[w];
+      rv[pos] = r;
+    }
+    done += __popc(m);
+  }
+  if(MODE == 0 && lane == 0) *count_out = done;
+}
+#undef G2R
+#undef V2R
+
+// Warp per unit over the global unit range [u0, u1) of the batch.
+template <int NBITS, int MODE>
+__global__ void __launch_bounds__(256)
+    units_k(Ints I, CoreData cd, int64_t u0, int64_t u1, size_t c0, size_t c1,
+            double E0, double tol, int64_t* counts, const int64_t* outoff,
+            uint64_t* keys, double* rv) {
+  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
+  for(int64_t u = u0 + int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      u < u1; u += int64_t(nwarp)) {
+    // det owning unit u: last c in [c0, c1) with uoff[c] <= u
+    size_t lo = c0, hi = c1;
+    while(hi - lo > 1) {
+      const size_t mid = (lo + hi) >> 1;
+      if(cd.uoff[mid] <= u)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int64_t t = u - cd.uoff[lo];
+    unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
+                          MODE ? outoff[u - u0] : 0, keys, rv);
+  }
+}
+
+// --------------------------------------------------- accumulate / merge
+template <int NW>
+__global__ void seg_flags_k(const uint64_t* keys, size_t n, uint32_t* f) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    f[i] = (i == 0 || !key_eq<NW>(load_key<NW>(keys, i), load_key<NW>(keys, i - 1)))
+               ? 1u
+               : 0u;
+}
+template <int NW>
+__global__ void seg_starts_k(const uint32_t* f, const uint32_t* fx, size_t n,
+                             int64_t* start, const uint64_t* keys,
+                             uint64_t* ukeys) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    if(f[i]) {
+      start[fx[i]] = int64_t(i);
+      store_key<NW>(ukeys, fx[i], load_key<NW>(keys, i));
+    }
+}
+// Sequential sum of each segment in sorted (= generation) order.
+__global__ void seg_sum_k(const int64_t* start, size_t nseg, size_t n,
+                          const double* rv, double* out) {
+  for(size_t s = size_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nseg;
+      s += size_t(gridDim.x) * blockDim.x) {
+    const int64_t b = start[s], e = s + 1 < nseg ? start[s + 1] : int64_t(n);
+    double a = rv[b];
+    for(int64_t j = b + 1; j < e; ++j) a += rv[j];
+    out[s] = a;
+  }
+}
+
+// Rank of every key of X among Y (lower bound if before_ties, else upper).
+template <int NW>
+__global__ void merge_rank_k(const uint64_t* X, size_t nx, const uint64_t* Y,
+                             size_t ny, int upper, int64_t* pos) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nx;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const Key<NW> k = load_key<NW>(X, i);
+    size_t lo = 0, hi = ny;
+    while(lo < hi) {
+      const size_t mid = (lo + hi) >> 1;
+      const int c = key_cmp<NW>(load_key<NW>(Y, mid), k);
+      if(c < 0 || (upper && c == 0))
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    pos[i] = int64_t(i + lo);
+  }
+}
+template <int NW>
+__global__ void merge_scatter_k(const uint64_t* X, const double* xv, size_t nx,
+                                const int64_t* pos, uint64_t* out,
+                                double* ov) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nx;
+      i += size_t(gridDim.x) * blockDim.x) {
+    store_key<NW>(out, pos[i], load_key<NW>(X, i));
+    ov[pos[i]] = xv[i];
+  }
+}
+
+// --------------------------------------------------------- core / top-k
+template <int NW>
+__global__ void keep_flags_k(const uint64_t* keys, const double* rv, size_t n,
+                             const uint64_t* core, size_t nc, uint32_t* f) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const Key<NW> k = load_key<NW>(keys, i);
+    size_t lo = 0, hi = nc;
+    bool found = false;
+    while(lo < hi) {
+      const size_t mid = (lo + hi) >> 1;
+      const int c = key_cmp<NW>(load_key<NW>(core, mid), k);
+      if(c == 0) {
+        found = true;
+        break;
+      }
+      if(c < 0)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    f[i] = (!found && (-fabs(rv[i]) < 0.0)) ? 1u : 0u;
+  }
+}
+template <int NW>
+__global__ void compact_k(const uint64_t* keys, const double* rv, size_t n,
+                          const uint32_t* f, const uint32_t* fx,
+                          uint64_t* ok, double* orv) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    if(f[i]) {
+      store_key<NW>(ok, fx[i], load_key<NW>(keys, i));
+      orv[fx[i]] = rv[i];
+    }
+}
+// Prune: keep |rv| > tol (determinant_search.hpp:122-127).
+__global__ void prune_flags_k(const double* rv, size_t n, double tol,
+                              uint32_t* f) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    f[i] = fabs(rv[i]) > tol ? 1u : 0u;
+}
+
+__global__ void select_hist_k(const double* rv, size_t n, uint64_t prefix,
+                              uint64_t mask, int shift,
+                              unsigned long long* hist) {
+  __shared__ unsigned int h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const uint64_t k = uint64_t(__double_as_longlong(fabs(rv[i])));
+    if((k & mask) == prefix) atomicAdd(&h[(k >> shift) & 255], 1u);
+  }
+  __syncthreads();
+  if(h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], (unsigned long long)h[threadIdx.x]);
+}
+__global__ void select_flags_k(const double* rv, size_t n, uint64_t T,
+                               uint32_t* gt, uint32_t* eq) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const uint64_t k = uint64_t(__double_as_longlong(fabs(rv[i])));
+    gt[i] = k > T;
+    eq[i] = k == T;
+  }
+}
+__global__ void select_final_k(const uint32_t* gt, const uint32_t* eq,
+                               const uint32_t* eqx, size_t n, uint64_t need,
+                               uint32_t* f) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    f[i] = gt[i] || (eq[i] && eqx[i] < need);
+}
+
+// ----------------------------------------------------------------- driver
+namespace {
+struct Pairs {
+  uint64_t* keys = nullptr;
+  double* rv = nullptr;
+  size_t n = 0;
+};
+double ms_since(std::chrono::steady_clock::time_point t) {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now() - t)
+      .count();
+}
+}  // namespace
+
+template <int NBITS>
+static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
+                      size_t ndets_max, const uint64_t* cdets, size_t ncdets,
+                      double E0, const double* C, uint64_t* out_dets,
+                      size_t* nout, std::vector<uint64_t>* ps,
+                      std::vector<double>* pr, bool pairs_only) {
+  constexpr int NW = DetTraits<NBITS>::NW;
+  cudaStream_t s = h->stream;
+  Arena A(s);
+  const Ints I = h->ints();
+  const int n = h->norb;
+  const int sms = num_sms();
+  auto t_all = std::chrono::steady_clock::now();
+  macis_b200_asci_stats stats{};
+
+  // ------------------------------------------------ core precompute
+  CoreData cd{};
+  cd.n = n;
+  cd.dets = cdets;
+  cd.C = C;
+  cd.ncdets = ncdets;
+  cd.occ = A.get<uint8_t>(ncdets * 2 * MAXORB + 1);
+  cd.vir = A.get<uint8_t>(ncdets * 2 * MAXORB + 1);
+  cd.cnt = A.get<uint8_t>(ncdets * 4 + 1);
+  cd.eps = A.get<double>(ncdets * 2 * n + 1);
+  cd.hd = A.get<double>(ncdets + 1);
+  int64_t* units = A.get<int64_t>(ncdets + 1);
+  cd.uoff = A.get<int64_t>(ncdets + 1);
+  if(ncdets) {
+    core_prep_k<NBITS><<<grid_for(ncdets * 32, 256, 16 * sms), 256, 0, s>>>(
+        I, cd, st.just_singles, units), note_launch();
+    MB_CUDA(cudaGetLastError());
+  }
+  exclusive_scan<int64_t, int64_t>(units, cd.uoff, ncdets, cd.uoff + ncdets, A);
+  const int64_t U = ncdets ? to_host(cd.uoff + ncdets, s) : 0;
+
+  // unit counts of the whole search (count pass over all units at once)
+  int64_t* ucnt = A.get<int64_t>(U + 1);
+  if(U)
+    units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
+        I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt, nullptr, nullptr,
+        nullptr), note_launch();
+  int64_t* uout = A.get<int64_t>(U + 1);
+  exclusive_scan<int64_t, int64_t>(ucnt, uout, size_t(U), uout + U, A);
+  const int64_t Ptot = U ? to_host(uout + U, s) : 0;
+  stats.raw_pairs = uint64_t(Ptot);
+
+  // per-det raw counts on the host to form batches
+  std::vector<int64_t> h_uoff(ncdets + 1), h_uout;
+  if(ncdets) {
+    MB_CUDA(cudaMemcpyAsync(h_uoff.data(), cd.uoff, (ncdets + 1) * 8,
+                            cudaMemcpyDeviceToHost, s));
+    h_uout.resize(U + 1);
+    MB_CUDA(cudaMemcpyAsync(h_uout.data(), uout, (U + 1) * 8,
+                            cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
+  size_t freeb = 0, totb = 0;
+  MB_CUDA(cudaMemGetInfo(&freeb, &totb));
+  // raw record + sort scratch + flags ~ 2.6 x (NW*8 + 8) + 16 bytes
+  const size_t rec = size_t(2.6 * (NW * 8 + 8)) + 16;
+  int64_t cap = int64_t(double(freeb) * 0.45 / double(rec));
+  cap = std::max<int64_t>(cap, int64_t(1) << 20);
+  cap = std::min<int64_t>(cap, int64_t(1) << 31);
+  // MACIS_B200_ASCI_BATCH_PAIRS caps the raw pairs per batch (exercises the
+  // batch merge on small problems).
+  if(const char* e = getenv("MACIS_B200_ASCI_BATCH_PAIRS"))
+    cap = std::max<int64_t>(1, atoll(e));
+  stats.pairs_ms = ms_since(t_all);
+
+  Pairs acc;  // running unique list (sorted)
+  double sort_ms = 0, pair_ms = 0;
+  size_t c0 = 0;
+  while(c0 < ncdets) {
+    // grow the batch while its raw count fits
+    size_t c1 = c0 + 1;
+    while(c1 < ncdets &&
+          h_uout[h_uoff[c1 + 1]] - h_uout[h_uoff[c0]] <= cap)
+      ++c1;
+    const int64_t u0 = h_uoff[c0], u1 = h_uoff[c1];
+    const int64_t p0 = h_uout[u0], P = h_uout[u1] - p0;
+    stats.batches++;
+    auto tb = std::chrono::steady_clock::now();
+    Arena B(s);
+    uint64_t* keys = B.get<uint64_t>(size_t(P) * NW + NW);
+    double* rv = B.get<double>(size_t(P) + 1);
+    if(P) {
+      // offsets relative to the batch
+      int64_t* boff = B.get<int64_t>(size_t(u1 - u0) + 1);
+      exclusive_scan<int64_t, int64_t>(ucnt + u0, boff, size_t(u1 - u0),
+                                       nullptr, B);
+      units_k<NBITS, 1><<<grid_for(size_t(u1 - u0) * 32, 256, 32 * sms), 256,
+                          0, s>>>(I, cd, u0, u1, c0, c1, E0, st.h_el_tol,
+                                  ucnt + u0, boff, keys, rv), note_launch();
+      MB_CUDA(cudaGetLastError());
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    pair_ms += ms_since(tb);
+    tb = std::chrono::steady_clock::now();
+    Pairs bat;
+    if(P) {
+      uint64_t* k2 = B.get<uint64_t>(size_t(P) * NW + NW);
+      double* r2 = B.get<double>(size_t(P) + 1);
+      radix_sort<NW, double>(keys, rv, k2, r2, size_t(P), B);
+      uint32_t* f = B.get<uint32_t>(size_t(P) + 1);
+      uint32_t* fx = B.get<uint32_t>(size_t(P) + 1);
+      seg_flags_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
+          keys, size_t(P), f), note_launch();
+      exclusive_scan<uint32_t, uint32_t>(f, fx, size_t(P), fx + P, B);
+      const uint32_t nu = to_host(fx + P, s);
+      int64_t* start = B.get<int64_t>(nu + 1);
+      // unique keys reuse k2, sums reuse r2
+      seg_starts_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
+          f, fx, size_t(P), start, keys, k2), note_launch();
+      seg_sum_k<<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(start, nu,
+                                                            size_t(P), rv, r2), note_launch();
+      // move into A-owned storage
+      bat.n = nu;
+      bat.keys = A.get<uint64_t>(size_t(nu) * NW + NW);
+      bat.rv = A.get<double>(size_t(nu) + 1);
+      MB_CUDA(cudaMemcpyAsync(bat.keys, k2, size_t(nu) * NW * 8,
+                              cudaMemcpyDeviceToDevice, s));
+      MB_CUDA(cudaMemcpyAsync(bat.rv, r2, size_t(nu) * 8,
+                              cudaMemcpyDeviceToDevice, s));
+    }
+    if(acc.n == 0) {
+      acc = bat;
+    } else if(bat.n) {
+      // merge two sorted unique lists, then add equal neighbours (acc first)
+      const size_t nm = acc.n + bat.n;
+      int64_t* pa = B.get<int64_t>(acc.n);
+      int64_t* pb = B.get<int64_t>(bat.n);
+      merge_rank_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
+          acc.keys, acc.n, bat.keys, bat.n, 0, pa), note_launch();
+      merge_rank_k<NW><<<grid_for(bat.n, 256, 16 * sms), 256, 0, s>>>(
+          bat.keys, bat.n, acc.keys, acc.n, 1, pb), note_launch();
+      uint64_t* mk = B.get<uint64_t>(nm * NW + NW);
+      double* mr = B.get<double>(nm + 1);
+      merge_scatter_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
+          acc.keys, acc.rv, acc.n, pa, mk, mr), note_launch();
+      merge_scatter_k<NW><<<grid_for(bat.n, 256, 16 * sms), 256, 0, s>>>(
+          bat.keys, bat.rv, bat.n, pb, mk, mr), note_launch();
+      uint32_t* f = B.get<uint32_t>(nm + 1);
+      uint32_t* fx = B.get<uint32_t>(nm + 1);
+      seg_flags_k<NW><<<grid_for(nm, 256, 16 * sms), 256, 0, s>>>(mk, nm, f), note_launch();
+      exclusive_scan<uint32_t, uint32_t>(f, fx, nm, fx + nm, B);
+      const uint32_t nu = to_host(fx + nm, s);
+      int64_t* start = B.get<int64_t>(nu + 1);
+      Pairs m2;
+      m2.n = nu;
+      m2.keys = A.get<uint64_t>(size_t(nu) * NW + NW);
+      m2.rv = A.get<double>(size_t(nu) + 1);
+      seg_starts_k<NW><<<grid_for(nm, 256, 16 * sms), 256, 0, s>>>(
+          f, fx, nm, start, mk, m2.keys), note_launch();
+      seg_sum_k<<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(start, nu, nm, mr,
+                                                           m2.rv), note_launch();
+      A.release(acc.keys);
+      A.release(acc.rv);
+      A.release(bat.keys);
+      A.release(bat.rv);
+      acc = m2;
+    }
+    // pruning when the list outgrows pair_size_max (determinant_search.hpp:
+    // 121-137), applied to the running sums
+    if(acc.n > st.pair_size_max) {
+      uint32_t* f = B.get<uint32_t>(acc.n + 1);
+      uint32_t* fx = B.get<uint32_t>(acc.n + 1);
+      prune_flags_k<<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
+          acc.rv, acc.n, st.rv_prune_tol, f), note_launch();
+      exclusive_scan<uint32_t, uint32_t>(f, fx, acc.n, fx + acc.n, B);
+      const uint32_t nk = to_host(fx + acc.n, s);
+      Pairs p2;
+      p2.n = nk;
+      p2.keys = A.get<uint64_t>(size_t(nk) * NW + NW);
+      p2.rv = A.get<double>(size_t(nk) + 1);
+      compact_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
+          acc.keys, acc.rv, acc.n, f, fx, p2.keys, p2.rv), note_launch();
+      A.release(acc.keys);
+      A.release(acc.rv);
+      acc = p2;
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    sort_ms += ms_since(tb);
+    c0 = c1;
+  }
+  stats.unique_pairs = acc.n;
+  stats.pairs_ms += pair_ms;
+  stats.sort_ms = sort_ms;
+
+  if(pairs_only) {
+    ps->resize(acc.n * NW);
+    pr->resize(acc.n);
+    if(acc.n) {
+      MB_CUDA(cudaMemcpyAsync(ps->data(), acc.keys, acc.n * NW * 8,
+                              cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaMemcpyAsync(pr->data(), acc.rv, acc.n * 8,
+                              cudaMemcpyDeviceToHost, s));
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    h->last_asci = stats;
+    return;
+  }
+
+  // ------------------------------------------- drop core dets, zero scores
+  auto tk = std::chrono::steady_clock::now();
+  uint64_t* core = A.get<uint64_t>(ncdets * NW + NW);
+  if(ncdets) {
+    uint64_t* ct = A.get<uint64_t>(ncdets * NW + NW);
+    MB_CUDA(cudaMemcpyAsync(core, cdets, ncdets * NW * 8,
+                            cudaMemcpyDeviceToDevice, s));
+    radix_sort<NW, uint32_t>(core, nullptr, ct, nullptr, ncdets, A);
+  }
+  Pairs kept;
+  if(acc.n) {
+    uint32_t* f = A.get<uint32_t>(acc.n + 1);
+    uint32_t* fx = A.get<uint32_t>(acc.n + 1);
+    keep_flags_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
+        acc.keys, acc.rv, acc.n, core, ncdets, f), note_launch();
+    exclusive_scan<uint32_t, uint32_t>(f, fx, acc.n, fx + acc.n, A);
+    kept.n = to_host(fx + acc.n, s);
+    kept.keys = A.get<uint64_t>(kept.n * NW + NW);
+    kept.rv = A.get<double>(kept.n + 1);
+    compact_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
+        acc.keys, acc.rv, acc.n, f, fx, kept.keys, kept.rv), note_launch();
+  }
+  stats.kept_pairs = kept.n;
+  stats.keep_ms = ms_since(tk);
+
+  // ------------------------------------------------------------- top-k
+  auto tt = std::chrono::steady_clock::now();
+  const size_t topk = ndets_max - ncdets;  // size_t arithmetic (:547)
+  size_t nsel = kept.n;
+  uint32_t* sel = nullptr;
+  uint32_t* selx = nullptr;
+  if(kept.n > topk) {
+    auto* hist = A.get<unsigned long long>(256);
+    uint64_t prefix = 0, mask = 0;
+    uint64_t need = topk;  // still to take from the current prefix bucket
+    for(int shift = 56; shift >= 0; shift -= 8) {
+      MB_CUDA(cudaMemsetAsync(hist, 0, 256 * 8, s));
+      select_hist_k<<<grid_for(kept.n, 256, 8 * sms), 256, 0, s>>>(
+          kept.rv, kept.n, prefix, mask, shift, hist), note_launch();
+      unsigned long long hh[256];
+      MB_CUDA(cudaMemcpyAsync(hh, hist, sizeof(hh), cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaStreamSynchronize(s));
+      int d = 255;
+      for(; d > 0; --d) {
+        if(hh[d] >= need) break;
+        need -= hh[d];
+      }
+      prefix |= uint64_t(d) << shift;
+      mask |= uint64_t(255) << shift;
+    }
+    // prefix = k-th largest |rv| bits; take all > T and the first `need`
+    // equal ones in ascending determinant order
+    uint32_t* gt = A.get<uint32_t>(kept.n + 1);
+    uint32_t* eq = A.get<uint32_t>(kept.n + 1);
+    uint32_t* eqx = A.get<uint32_t>(kept.n + 1);
+    select_flags_k<<<grid_for(kept.n, 256, 16 * sms), 256, 0, s>>>(
+        kept.rv, kept.n, prefix, gt, eq), note_launch();
+    exclusive_scan<uint32_t, uint32_t>(eq, eqx, kept.n, eqx + kept.n, A);
+    sel = A.get<uint32_t>(kept.n + 1);
+    selx = A.get<uint32_t>(kept.n + 1);
+    select_final_k<<<grid_for(kept.n, 256, 16 * sms), 256, 0, s>>>(
+        gt, eq, eqx, kept.n, need, sel), note_launch();
+    exclusive_scan<uint32_t, uint32_t>(sel, selx, kept.n, selx + kept.n, A);
+    nsel = to_host(selx + kept.n, s);
+  }
+  MB_REQUIRE(nsel <= ndets_max, MACIS_B200_ECAPACITY,
+             "ASCI search result exceeds ndets_max + ncdets determinants");
+  if(nsel) {
+    if(sel) {
+      double* tmp = A.get<double>(nsel + 1);
+      compact_k<NW><<<grid_for(kept.n, 256, 16 * sms), 256, 0, s>>>(
+          kept.keys, kept.rv, kept.n, sel, selx, out_dets, tmp), note_launch();
+    } else {
+      MB_CUDA(cudaMemcpyAsync(out_dets, kept.keys, nsel * NW * 8,
+                              cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  if(ncdets)
+    MB_CUDA(cudaMemcpyAsync(out_dets + nsel * NW, cdets, ncdets * NW * 8,
+                            cudaMemcpyDeviceToDevice, s));
+  *nout = nsel + ncdets;
+  MB_CUDA(cudaGetLastError());
+  MB_CUDA(cudaStreamSynchronize(s));
+  stats.topk_ms = ms_since(tt);
+  stats.total_ms = ms_since(t_all);
+  h->last_asci = stats;
+}
+
+void asci_search_device(macis_b200_ham* h, const macis_b200_asci_settings& s,
+                        size_t ndets_max, const uint64_t* cdets, size_t ncdets,
+                        double E0, const double* C, uint64_t* out_dets,
+                        size_t* nout, std::vector<uint64_t>* ps,
+                        std::vector<double>* pr, bool pairs_only) {
+  MB_REQUIRE(h->norb <= MAXORB, MACIS_B200_EINVAL, "norb too large for ASCI");
+  if(h->nbits == 64)
+    asci_impl<64>(h, s, ndets_max, cdets, ncdets, E0, C, out_dets, nout, ps,
+                  pr, pairs_only);
+  else if(h->nbits == 128)
+    asci_impl<128>(h, s, ndets_max, cdets, ncdets, E0, C, out_dets, nout, ps,
+                   pr, pairs_only);
+  else
+    asci_impl<256>(h, s, ndets_max, cdets, ncdets, E0, C, out_dets, nout, ps,
+                   pr, pairs_only);
+}
+
+}  // namespace mb

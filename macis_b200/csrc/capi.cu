@@ -1,0 +1,364 @@
+// C ABI of libmacis_b200 (declared in include/macis_b200.h). Every entry
+// point converts exceptions into status codes and stages host buffers
+// through HBM when MACIS_B200_DEVICE_PTRS is not set.
+#include <cstring>
+#include <string>
+
+#include "internal.hpp"
+#include "primitives.cuh"
+
+namespace mb {
+void ham_create(macis_b200_ham* h, int nbits, size_t norb, const double* T,
+                size_t LDT, const double* V, size_t LDV);
+void ham_destroy(macis_b200_ham* h);
+
+static thread_local std::string g_err;
+void set_error(const std::string& s) { g_err = s; }
+
+template <class F>
+static int guarded(F&& f) {
+  try {
+    f();
+    return MACIS_B200_OK;
+  } catch(const Error& e) {
+    g_err = e.what();
+    return e.code;
+  } catch(const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return MACIS_B200_ENOMEM;
+  } catch(const std::exception& e) {
+    g_err = e.what();
+    return MACIS_B200_EINVAL;
+  }
+}
+
+// Device view of a possibly-host buffer.
+template <typename T>
+struct DevBuf {
+  T* d = nullptr;
+  bool owned = false;
+  cudaStream_t s;
+  DevBuf(const T* p, size_t n, unsigned flags, cudaStream_t st) : s(st) {
+    if(flags & MACIS_B200_DEVICE_PTRS) {
+      d = const_cast<T*>(p);
+    } else {
+      MB_CUDA(cudaMallocAsync(&d, n * sizeof(T) + 16, s));
+      owned = true;
+      if(n && p)
+        MB_CUDA(cudaMemcpyAsync(d, p, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+  }
+  DevBuf(const DevBuf&) = delete;
+  ~DevBuf() {
+    if(owned) cudaFreeAsync(d, s);
+  }
+};
+
+static void require_dets(const void* p, size_t n, unsigned flags = 0) {
+  MB_REQUIRE(n == 0 || p != nullptr, MACIS_B200_EINVAL,
+             "null determinant array");
+  MB_REQUIRE(!(flags & MACIS_B200_DEVICE_PTRS) ||
+                 (reinterpret_cast<uintptr_t>(p) & 15) == 0,
+             MACIS_B200_EINVAL, "device determinant arrays must be 16-byte aligned");
+}
+
+}  // namespace mb
+
+using namespace mb;
+
+extern "C" {
+
+const char* macis_b200_last_error(void) { return g_err.c_str(); }
+int macis_b200_version(void) { return 1; }
+
+int macis_b200_ham_create(int nbits, size_t norb, const double* T, size_t LDT,
+                          const double* V, size_t LDV, macis_b200_ham** out) {
+  return guarded([&] {
+    MB_REQUIRE(out && T && V, MACIS_B200_EINVAL, "null argument");
+    auto* h = new macis_b200_ham;
+    try {
+      ham_create(h, nbits, norb, T, LDT, V, LDV);
+    } catch(...) {
+      ham_destroy(h);
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int macis_b200_ham_destroy(macis_b200_ham* h) {
+  return guarded([&] {
+    if(!h) return;
+    ham_destroy(h);
+    delete h;
+  });
+}
+
+int macis_b200_matrix_element(macis_b200_ham* h, const uint64_t* bra,
+                              const uint64_t* ket, size_t n, double* out,
+                              unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(h, MACIS_B200_EINVAL, "null handle");
+    require_dets(bra, n);
+    require_dets(ket, n);
+    const size_t nw = h->nbits / 64;
+    DevBuf<uint64_t> b(bra, n * nw, flags, h->stream), k(ket, n * nw, flags,
+                                                          h->stream);
+    DevBuf<double> o(out, 0, flags | MACIS_B200_DEVICE_PTRS, h->stream);
+    double* dout = out;
+    if(!(flags & MACIS_B200_DEVICE_PTRS))
+      MB_CUDA(cudaMallocAsync(&dout, n * 8 + 8, h->stream));
+    matrix_elements_device(h, b.d, k.d, n, dout);
+    if(!(flags & MACIS_B200_DEVICE_PTRS)) {
+      MB_CUDA(cudaMemcpyAsync(out, dout, n * 8, cudaMemcpyDeviceToHost, h->stream));
+      cudaFreeAsync(dout, h->stream);
+    }
+    MB_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int macis_b200_build_csr(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
+                         const uint64_t* ket, size_t nket, double H_thresh,
+                         int idx_bytes, int val_bytes, unsigned flags,
+                         macis_b200_csr** out) {
+  return guarded([&] {
+    MB_REQUIRE(h && out, MACIS_B200_EINVAL, "null argument");
+    require_dets(bra, nbra, flags);
+    require_dets(ket, nket, flags);
+    const size_t nw = h->nbits / 64;
+    // a bra list inside the ket array (same list, or a row block of it) is
+    // uploaded once and passed as a sub-range, which keeps the square /
+    // row-block fast paths
+    const bool inside = bra >= ket && bra + nbra * nw <= ket + nket * nw &&
+                        (bra - ket) % nw == 0;
+    DevBuf<uint64_t> k(ket, nket * nw, flags, h->stream);
+    const uint64_t* bd = nullptr;
+    DevBuf<uint64_t>* bb = nullptr;
+    if(inside && !(flags & MACIS_B200_DEVICE_PTRS)) {
+      bd = k.d + (bra - ket);
+    } else {
+      bb = new DevBuf<uint64_t>(bra, nbra * nw, flags, h->stream);
+      bd = bb->d;
+    }
+    try {
+      *out = build_csr_device(h, bd, nbra, k.d, nket, H_thresh, idx_bytes,
+                              val_bytes);
+    } catch(...) {
+      delete bb;
+      throw;
+    }
+    delete bb;
+  });
+}
+
+int macis_b200_csr_destroy(macis_b200_csr* A) {
+  return guarded([&] {
+    if(!A) return;
+    cudaFreeAsync(A->rowptr, A->stream);
+    cudaFreeAsync(A->colind, A->stream);
+    cudaFreeAsync(A->nzval, A->stream);
+    cudaFreeAsync(A->diag, A->stream);
+    cudaStreamSynchronize(A->stream);
+    if(A->own_stream) cudaStreamDestroy(A->stream);
+    delete A;
+  });
+}
+
+unsigned long long macis_b200_launch_count(void) { return launch_counter(); }
+
+int macis_b200_csr_info(const macis_b200_csr* A, int64_t* m, int64_t* n,
+                        int64_t* nnz, int* idx_bytes, int* val_bytes) {
+  return guarded([&] {
+    MB_REQUIRE(A, MACIS_B200_EINVAL, "null handle");
+    if(m) *m = A->m;
+    if(n) *n = A->n;
+    if(nnz) *nnz = A->nnz;
+    if(idx_bytes) *idx_bytes = A->idx_bytes;
+    if(val_bytes) *val_bytes = A->val_bytes;
+  });
+}
+
+int macis_b200_csr_download(const macis_b200_csr* A, void* rowptr,
+                            void* colind, void* nzval, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(A, MACIS_B200_EINVAL, "null handle");
+    const cudaMemcpyKind k = (flags & MACIS_B200_DEVICE_PTRS)
+                                 ? cudaMemcpyDeviceToDevice
+                                 : cudaMemcpyDeviceToHost;
+    if(rowptr)
+      MB_CUDA(cudaMemcpyAsync(rowptr, A->rowptr, (A->m + 1) * A->idx_bytes, k,
+                              A->stream));
+    if(colind && A->nnz)
+      MB_CUDA(cudaMemcpyAsync(colind, A->colind, A->nnz * A->idx_bytes, k,
+                              A->stream));
+    if(nzval && A->nnz)
+      MB_CUDA(cudaMemcpyAsync(nzval, A->nzval, A->nnz * A->val_bytes, k,
+                              A->stream));
+    MB_CUDA(cudaStreamSynchronize(A->stream));
+  });
+}
+
+int macis_b200_csr_diagonal(const macis_b200_csr* A, double* D,
+                            unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(A && D, MACIS_B200_EINVAL, "null argument");
+    const cudaMemcpyKind k = (flags & MACIS_B200_DEVICE_PTRS)
+                                 ? cudaMemcpyDeviceToDevice
+                                 : cudaMemcpyDeviceToHost;
+    if(A->m)
+      MB_CUDA(cudaMemcpyAsync(D, A->diag, A->m * 8, k, A->stream));
+    MB_CUDA(cudaStreamSynchronize(A->stream));
+  });
+}
+
+int macis_b200_spmv(const macis_b200_csr* A, int64_t K, double alpha,
+                    const double* V, int64_t LDV, double beta, double* AV,
+                    int64_t LDAV, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(A && (K == 0 || (V && AV)), MACIS_B200_EINVAL, "null argument");
+    MB_REQUIRE(K >= 0 && LDV >= A->n && LDAV >= A->m, MACIS_B200_EINVAL,
+               "bad leading dimension");
+    cudaStream_t s = A->stream;
+    if(flags & MACIS_B200_DEVICE_PTRS) {
+      for(int64_t k = 0; k < K; ++k)
+        spmv_device(A, alpha, V + k * LDV, beta, AV + k * LDAV, s);
+    } else {
+      Arena W(s);
+      double* dv = W.get<double>(size_t(A->n));
+      double* dy = W.get<double>(size_t(A->m));
+      for(int64_t k = 0; k < K; ++k) {
+        MB_CUDA(cudaMemcpyAsync(dv, V + k * LDV, A->n * 8,
+                                cudaMemcpyHostToDevice, s));
+        if(beta != 0.0)
+          MB_CUDA(cudaMemcpyAsync(dy, AV + k * LDAV, A->m * 8,
+                                  cudaMemcpyHostToDevice, s));
+        spmv_device(A, alpha, dv, beta, dy, s);
+        MB_CUDA(cudaMemcpyAsync(AV + k * LDAV, dy, A->m * 8,
+                                cudaMemcpyDeviceToHost, s));
+      }
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int macis_b200_davidson(const macis_b200_csr* A, int64_t max_m, double tol,
+                        int use_guess, double* X, double* E, int64_t* niter,
+                        unsigned flags) {
+  int rc = MACIS_B200_OK;
+  int st = guarded([&] {
+    MB_REQUIRE(A && X && E && niter, MACIS_B200_EINVAL, "null argument");
+    DevBuf<double> x(X, size_t(A->m), flags, A->stream);
+    rc = davidson_device(A, max_m, tol, use_guess != 0, x.d, E, niter, 0, 0);
+    if(!(flags & MACIS_B200_DEVICE_PTRS))
+      MB_CUDA(cudaMemcpyAsync(X, x.d, A->m * 8, cudaMemcpyDeviceToHost, A->stream));
+    MB_CUDA(cudaStreamSynchronize(A->stream));
+  });
+  if(st) return st;
+  if(rc == MACIS_B200_ENOCONV) g_err = "Davidson Did Not Converge!";
+  return rc;
+}
+
+int macis_b200_davidson_ex(const macis_b200_csr* A,
+                           const macis_b200_davidson_opts* o, double* X,
+                           double* E, int64_t* niter, unsigned flags) {
+  int rc = MACIS_B200_OK;
+  int st = guarded([&] {
+    MB_REQUIRE(A && o && X && E && niter, MACIS_B200_EINVAL, "null argument");
+    DevBuf<double> x(X, size_t(A->m), flags, A->stream);
+    rc = davidson_device(A, o->max_m, o->tol, o->use_guess != 0, x.d, E, niter,
+                         o->restart_keep, o->max_iter);
+    if(!(flags & MACIS_B200_DEVICE_PTRS))
+      MB_CUDA(cudaMemcpyAsync(X, x.d, A->m * 8, cudaMemcpyDeviceToHost, A->stream));
+    MB_CUDA(cudaStreamSynchronize(A->stream));
+  });
+  if(st) return st;
+  if(rc == MACIS_B200_ENOCONV) g_err = "Davidson Did Not Converge!";
+  return rc;
+}
+
+int macis_b200_small_syev(int k, const double* lower, int nwant, double* W,
+                          double* Vec) {
+  return guarded([&] {
+    MB_REQUIRE(k >= 1 && nwant >= 1 && lower && W && Vec, MACIS_B200_EINVAL,
+               "bad argument");
+    small_syev_lowest(k, lower, nwant, W, Vec);
+  });
+}
+
+int macis_b200_csr_build_stats(const macis_b200_csr* A,
+                               macis_b200_build_stats* out) {
+  return guarded([&] {
+    MB_REQUIRE(A && out, MACIS_B200_EINVAL, "null argument");
+    out->build_ms = A->build_ms;
+    out->fill_ms = A->fill_ms;
+    out->nnz_candidates = A->nnz_candidates;
+    out->direct_product = A->direct_product ? 1 : 0;
+    out->long_rows = int32_t(A->long_rows);
+  });
+}
+
+int macis_b200_asci_search(macis_b200_ham* h,
+                           const macis_b200_asci_settings* s,
+                           size_t ndets_max, const uint64_t* cdets,
+                           size_t ncdets, double E0, const double* C,
+                           uint64_t* out_dets, size_t* nout, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(h && s && out_dets && nout, MACIS_B200_EINVAL, "null argument");
+    require_dets(cdets, ncdets, flags);
+    require_dets(out_dets, 1, flags);
+    const size_t nw = h->nbits / 64;
+    DevBuf<uint64_t> cd(cdets, ncdets * nw, flags, h->stream);
+    DevBuf<double> cc(C, ncdets, flags, h->stream);
+    const size_t cap = ndets_max + ncdets;
+    uint64_t* od = out_dets;
+    if(!(flags & MACIS_B200_DEVICE_PTRS))
+      MB_CUDA(cudaMallocAsync(&od, cap * nw * 8 + 32, h->stream));
+    try {
+      asci_search_device(h, *s, ndets_max, cd.d, ncdets, E0, cc.d, od, nout,
+                         nullptr, nullptr, false);
+    } catch(...) {
+      if(!(flags & MACIS_B200_DEVICE_PTRS)) cudaFreeAsync(od, h->stream);
+      throw;
+    }
+    if(!(flags & MACIS_B200_DEVICE_PTRS)) {
+      MB_CUDA(cudaMemcpyAsync(out_dets, od, *nout * nw * 8,
+                              cudaMemcpyDeviceToHost, h->stream));
+      cudaFreeAsync(od, h->stream);
+    }
+    MB_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int macis_b200_asci_pairs(macis_b200_ham* h, const macis_b200_asci_settings* s,
+                          const uint64_t* cdets, size_t ncdets, double E0,
+                          const double* C, uint64_t* states, double* rv,
+                          size_t* npairs) {
+  return guarded([&] {
+    MB_REQUIRE(h && s && npairs, MACIS_B200_EINVAL, "null argument");
+    require_dets(cdets, ncdets);
+    const size_t nw = h->nbits / 64;
+    DevBuf<uint64_t> cd(cdets, ncdets * nw, 0, h->stream);
+    DevBuf<double> cc(C, ncdets, 0, h->stream);
+    std::vector<uint64_t> ps;
+    std::vector<double> pr;
+    size_t dummy = 0;
+    asci_search_device(h, *s, 0, cd.d, ncdets, E0, cc.d, nullptr, &dummy, &ps,
+                       &pr, true);
+    *npairs = pr.size();
+    if(states) {
+      std::memcpy(states, ps.data(), ps.size() * 8);
+      std::memcpy(rv, pr.data(), pr.size() * 8);
+    }
+  });
+}
+
+int macis_b200_asci_last_stats(const macis_b200_ham* h,
+                               macis_b200_asci_stats* out) {
+  return guarded([&] {
+    MB_REQUIRE(h && out, MACIS_B200_EINVAL, "null argument");
+    *out = h->last_asci;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,360 @@
+// Device-wide primitives written for this library: a workspace arena, an
+// exclusive scan and a stable LSD radix sort over multi-word keys.
+//
+// The radix sort is the dedup engine of the ASCI search (the reference's
+// std::sort by bitset_less, include/macis/asci/determinant_sort.hpp:40-57)
+// and the grouping step of the Hamiltonian build. Keys are NW little-endian
+// uint64 words stored item-contiguous; word NW-1 is the most significant
+// (the bitset_less order, bitset_operations.hpp:289-306). Only 8-bit digits
+// in which some key differs from the first key are sorted, so a 24-orbital
+// string costs 3 passes whatever its word width. Within a tile each warp
+// ranks its items with __match_any_sync, which keeps the sort stable: equal
+// keys leave in input order, which fixes the accumulation order of duplicate
+// ASCI contributions.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace mb {
+
+// ------------------------------------------------------------- workspace
+// Stream-ordered allocations from the device's default memory pool; freed on
+// destruction. Every buffer is 256-byte aligned.
+struct Arena {
+  cudaStream_t s;
+  std::vector<void*> ptrs;
+  explicit Arena(cudaStream_t st) : s(st) {}
+  template <typename T>
+  T* get(size_t n) {
+    void* p = nullptr;
+    size_t bytes = n * sizeof(T);
+    if(bytes == 0) bytes = 256;
+    MB_CUDA(cudaMallocAsync(&p, (bytes + 255) & ~size_t(255), s));
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  void release(void* p) {
+    for(auto& q : ptrs)
+      if(q == p) {
+        cudaFreeAsync(q, s);
+        q = nullptr;
+      }
+  }
+  ~Arena() {
+    for(void* p : ptrs)
+      if(p) cudaFreeAsync(p, s);
+  }
+};
+
+// ------------------------------------------------------------------ scan
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_IPT = 8;
+constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_IPT;
+
+template <typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T* sh, T* total) {
+  // sh: SCAN_THREADS/32 + 1 entries
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for(int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if(lane >= o) x += y;
+  }
+  if(lane == 31) sh[wid] = x;
+  __syncthreads();
+  if(wid == 0) {
+    T w = lane < (int)(blockDim.x >> 5) ? sh[lane] : T(0);
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, w, o);
+      if(lane >= o) w += y;
+    }
+    if(lane < (int)(blockDim.x >> 5)) sh[lane] = w;
+  }
+  __syncthreads();
+  T base = wid ? sh[wid - 1] : T(0);
+  if(total) *total = sh[(blockDim.x >> 5) - 1];
+  T r = base + x - v;
+  __syncthreads();
+  return r;
+}
+
+template <typename TI, typename TO>
+__global__ void scan_reduce_k(const TI* in, size_t n, TO* sums) {
+  __shared__ TO sh[SCAN_THREADS / 32 + 1];
+  size_t base = size_t(blockIdx.x) * SCAN_CHUNK;
+  TO acc = 0;
+#pragma unroll
+  for(int i = 0; i < SCAN_IPT; ++i) {
+    size_t j = base + size_t(threadIdx.x) * SCAN_IPT + i;
+    if(j < n) acc += TO(in[j]);
+  }
+  TO tot;
+  block_excl_scan<TO>(acc, sh, &tot);
+  if(threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+template <typename TI, typename TO>
+__global__ void scan_apply_k(const TI* in, size_t n, TO* out,
+                             const TO* offsets) {
+  __shared__ TO sh[SCAN_THREADS / 32 + 1];
+  size_t base = size_t(blockIdx.x) * SCAN_CHUNK;
+  TO v[SCAN_IPT];
+  TO acc = 0;
+#pragma unroll
+  for(int i = 0; i < SCAN_IPT; ++i) {
+    size_t j = base + size_t(threadIdx.x) * SCAN_IPT + i;
+    v[i] = j < n ? TO(in[j]) : TO(0);
+    acc += v[i];
+  }
+  TO pre = block_excl_scan<TO>(acc, sh, nullptr);
+  pre += offsets ? offsets[blockIdx.x] : TO(0);
+#pragma unroll
+  for(int i = 0; i < SCAN_IPT; ++i) {
+    size_t j = base + size_t(threadIdx.x) * SCAN_IPT + i;
+    if(j < n) out[j] = pre;
+    pre += v[i];
+  }
+}
+
+// out[i] = sum_{j<i} in[j]; out may alias in. If total != nullptr the grand
+// total is written to *total (device pointer). Returns nothing; sync-free.
+template <typename TI, typename TO>
+void exclusive_scan(const TI* in, TO* out, size_t n, TO* total, Arena& A) {
+  if(n == 0) {
+    if(total) MB_CUDA(cudaMemsetAsync(total, 0, sizeof(TO), A.s));
+    return;
+  }
+  size_t nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+  if(nb == 1) {
+    TO* sums = A.get<TO>(2);
+    scan_reduce_k<TI, TO><<<1, SCAN_THREADS, 0, A.s>>>(in, n, sums), note_launch();
+    if(total) MB_CUDA(cudaMemcpyAsync(total, sums, sizeof(TO), cudaMemcpyDeviceToDevice, A.s));
+    scan_apply_k<TI, TO><<<1, SCAN_THREADS, 0, A.s>>>(in, n, out, nullptr), note_launch();
+    return;
+  }
+  TO* sums = A.get<TO>(nb + 1);
+  scan_reduce_k<TI, TO><<<unsigned(nb), SCAN_THREADS, 0, A.s>>>(in, n, sums), note_launch();
+  exclusive_scan<TO, TO>(sums, sums, nb, total, A);
+  scan_apply_k<TI, TO><<<unsigned(nb), SCAN_THREADS, 0, A.s>>>(in, n, out,
+                                                               sums), note_launch();
+}
+
+// ------------------------------------------------------------ radix sort
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_IPT = 16;
+constexpr int RS_TILE = RS_THREADS * RS_IPT;  // 4096 items per block
+constexpr int RS_WARP_ITEMS = RS_TILE / RS_WARPS;
+
+template <int NW>
+struct Key {
+  uint64_t w[NW];
+};
+
+template <int NW>
+__device__ __forceinline__ Key<NW> load_key(const uint64_t* k, size_t i) {
+  Key<NW> r;
+  if constexpr(NW == 2) {
+    const ulonglong2 v = reinterpret_cast<const ulonglong2*>(k)[i];
+    r.w[0] = v.x;
+    r.w[1] = v.y;
+  } else if constexpr(NW == 4) {
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(k) + 2 * i;
+    ulonglong2 a = p[0], b = p[1];
+    r.w[0] = a.x;
+    r.w[1] = a.y;
+    r.w[2] = b.x;
+    r.w[3] = b.y;
+  } else {
+#pragma unroll
+    for(int j = 0; j < NW; ++j) r.w[j] = k[i * NW + j];
+  }
+  return r;
+}
+template <int NW>
+__device__ __forceinline__ void store_key(uint64_t* k, size_t i, Key<NW> r) {
+  if constexpr(NW == 2) {
+    reinterpret_cast<ulonglong2*>(k)[i] = make_ulonglong2(r.w[0], r.w[1]);
+  } else if constexpr(NW == 4) {
+    ulonglong2* p = reinterpret_cast<ulonglong2*>(k) + 2 * i;
+    p[0] = make_ulonglong2(r.w[0], r.w[1]);
+    p[1] = make_ulonglong2(r.w[2], r.w[3]);
+  } else {
+#pragma unroll
+    for(int j = 0; j < NW; ++j) k[i * NW + j] = r.w[j];
+  }
+}
+template <int NW>
+__device__ __forceinline__ int key_cmp(const Key<NW>& a, const Key<NW>& b) {
+#pragma unroll
+  for(int j = NW - 1; j >= 0; --j) {
+    if(a.w[j] < b.w[j]) return -1;
+    if(a.w[j] > b.w[j]) return 1;
+  }
+  return 0;
+}
+template <int NW>
+__device__ __forceinline__ bool key_eq(const Key<NW>& a, const Key<NW>& b) {
+  bool r = true;
+#pragma unroll
+  for(int j = 0; j < NW; ++j) r &= a.w[j] == b.w[j];
+  return r;
+}
+
+// OR over all keys of (key ^ key[0]) per word: the bits that vary.
+template <int NW>
+__global__ void key_vary_k(const uint64_t* keys, size_t n, uint64_t* vary) {
+  uint64_t acc[NW];
+  Key<NW> k0 = load_key<NW>(keys, 0);
+#pragma unroll
+  for(int j = 0; j < NW; ++j) acc[j] = 0;
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    Key<NW> k = load_key<NW>(keys, i);
+#pragma unroll
+    for(int j = 0; j < NW; ++j) acc[j] |= k.w[j] ^ k0.w[j];
+  }
+#pragma unroll
+  for(int j = 0; j < NW; ++j) {
+    uint64_t v = acc[j];
+    for(int o = 16; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+    if((threadIdx.x & 31) == 0 && v) atomicOr((unsigned long long*)&vary[j], v);
+  }
+}
+
+template <int NW>
+__device__ __forceinline__ unsigned digit_of(const Key<NW>& k, int shift) {
+  return unsigned(k.w[shift >> 6] >> (shift & 63)) & 255u;
+}
+
+template <int NW>
+__global__ void __launch_bounds__(RS_THREADS)
+    radix_hist_k(const uint64_t* keys, size_t n, int shift, uint32_t* counts,
+                 unsigned nblocks) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const size_t base = size_t(blockIdx.x) * RS_TILE;
+#pragma unroll 4
+  for(int r = 0; r < RS_IPT; ++r) {
+    size_t i = base + size_t(r) * RS_THREADS + threadIdx.x;
+    if(i < n) atomicAdd(&h[digit_of<NW>(load_key<NW>(keys, i), shift)], 1u);
+  }
+  __syncthreads();
+  counts[size_t(threadIdx.x) * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+template <int NW, typename P>
+__global__ void __launch_bounds__(RS_THREADS)
+    radix_scatter_k(const uint64_t* keys, const P* vals, size_t n, int shift,
+                    const uint64_t* offsets, unsigned nblocks,
+                    uint64_t* keys_out, P* vals_out) {
+  __shared__ uint32_t wcount[RS_WARPS][256];
+  __shared__ uint64_t boff[256];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for(int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS)
+    (&wcount[0][0])[d] = 0;
+  boff[threadIdx.x] = offsets[size_t(threadIdx.x) * nblocks + blockIdx.x];
+  __syncthreads();
+  const size_t wbase = size_t(blockIdx.x) * RS_TILE + size_t(wid) * RS_WARP_ITEMS;
+  Key<NW> k[RS_IPT];
+  uint32_t rank[RS_IPT];
+  unsigned dig[RS_IPT];
+#pragma unroll
+  for(int r = 0; r < RS_IPT; ++r) {
+    const size_t i = wbase + size_t(r) * 32 + lane;
+    const bool ok = i < n;
+    if(ok) k[r] = load_key<NW>(keys, i);
+    dig[r] = ok ? digit_of<NW>(k[r], shift) : 256u;
+    const unsigned peers = __match_any_sync(0xffffffffu, dig[r]);
+    const unsigned before = __popc(peers & lanemask_lt());
+    const int leader = __ffs(peers) - 1;
+    uint32_t c = 0;
+    if(ok) c = wcount[wid][dig[r]];
+    rank[r] = c + before;
+    __syncwarp();
+    if(ok && lane == leader) wcount[wid][dig[r]] = c + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // exclusive prefix over warps, per digit
+  {
+    const int d = threadIdx.x;
+    uint32_t acc = 0;
+#pragma unroll
+    for(int w = 0; w < RS_WARPS; ++w) {
+      uint32_t c = wcount[w][d];
+      wcount[w][d] = acc;
+      acc += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for(int r = 0; r < RS_IPT; ++r) {
+    const size_t i = wbase + size_t(r) * 32 + lane;
+    if(i < n) {
+      const unsigned d = dig[r];
+      const size_t dst = boff[d] + wcount[wid][d] + rank[r];
+      store_key<NW>(keys_out, dst, k[r]);
+      if(vals) vals_out[dst] = vals[i];
+    }
+  }
+}
+
+// Stable sort of n keys (NW words each) with optional payload. The sorted
+// result ends in (keys, vals); keys_alt/vals_alt are scratch of the same
+// size. Returns the number of digit passes run.
+template <int NW, typename P>
+int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
+               size_t n, Arena& A) {
+  if(n < 2) return 0;
+  uint64_t* d_vary = A.get<uint64_t>(NW);
+  MB_CUDA(cudaMemsetAsync(d_vary, 0, NW * 8, A.s));
+  key_vary_k<NW><<<grid_for(n, 256, 4 * num_sms()), 256, 0, A.s>>>(keys, n,
+                                                                   d_vary), note_launch();
+  uint64_t vary[NW];
+  MB_CUDA(cudaMemcpyAsync(vary, d_vary, NW * 8, cudaMemcpyDeviceToHost, A.s));
+  MB_CUDA(cudaStreamSynchronize(A.s));
+  const unsigned nblocks = unsigned((n + RS_TILE - 1) / RS_TILE);
+  uint32_t* counts = A.get<uint32_t>(size_t(256) * nblocks);
+  uint64_t* offs = A.get<uint64_t>(size_t(256) * nblocks);
+  int passes = 0;
+  uint64_t *kin = keys, *kout = keys_alt;
+  P *vin = vals, *vout = vals_alt;
+  for(int w = 0; w < NW; ++w)
+    for(int s = 0; s < 64; s += 8) {
+      if(((vary[w] >> s) & 255ull) == 0) continue;
+      const int shift = 64 * w + s;
+      radix_hist_k<NW><<<nblocks, RS_THREADS, 0, A.s>>>(kin, n, shift, counts,
+                                                        nblocks), note_launch();
+      exclusive_scan<uint32_t, uint64_t>(counts, offs, size_t(256) * nblocks,
+                                         nullptr, A);
+      radix_scatter_k<NW, P><<<nblocks, RS_THREADS, 0, A.s>>>(
+          kin, vin, n, shift, offs, nblocks, kout, vout), note_launch();
+      std::swap(kin, kout);
+      std::swap(vin, vout);
+      ++passes;
+    }
+  if(kin != keys) {
+    MB_CUDA(cudaMemcpyAsync(keys, kin, n * NW * 8, cudaMemcpyDeviceToDevice, A.s));
+    if(vals)
+      MB_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(P), cudaMemcpyDeviceToDevice, A.s));
+  }
+  return passes;
+}
+
+// Copy a device value to the host (synchronising the stream).
+template <typename T>
+T to_host(const T* d, cudaStream_t s) {
+  T h;
+  MB_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+}  // namespace mb

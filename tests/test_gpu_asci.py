@@ -1,0 +1,151 @@
+"""ASCI search on the GPU against the oracle (bit-exact pairs and selection,
+same summation order) and the compiled reference (pair sets identical, rv to
+1e-12 relative, top-k identical outside boundary ties)."""
+import os
+
+import numpy as np
+import pytest
+
+import macis_b200 as mb
+import oracle
+from cases import embed, fci
+from golden_data import constants, water
+
+pytestmark = pytest.mark.gpu
+K = constants()
+
+
+def _core(port, hp, nbits, norb, na, nb, n_core, ndets, seed=0):
+    """A core set from one oracle ASCI iteration starting at HF."""
+    s = oracle.AsciSettings.default()
+    ci = oracle.CiSettings.default()
+    hf = port.hf_det(nbits, na, nb)
+    E0 = port.matrix_element(hp, hf, hf)[0]
+    E, dets, X = port.asci_iter(hp, s, ci, ndets, E0, hf, np.ones(1))
+    order = np.argsort(-np.abs(X), kind="stable")
+    return dets[order][:n_core], X[order][:n_core], E
+
+
+def _settings(**kw):
+    s = mb.ASCISettings()
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def _tuples(a):
+    return set(map(tuple, np.asarray(a).tolist()))
+
+
+@pytest.fixture(scope="module")
+def wcase(port):
+    norb, T, V, _ = water()
+    hp = port.ham(64, norb, T, V)
+    cd, cc, E = _core(port, hp, 64, norb, 5, 5, 100, 800)
+    return norb, T, V, hp, cd, cc, E
+
+
+def test_pairs_bit_exact_vs_oracle_and_ref(port, ref, wcase):
+    norb, T, V, hp, cd, cc, E = wcase
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+    st, rv = mb.asci_pairs(_settings(), cd, E, cc, H)
+    so, ro = port.asci_pairs(hp, oracle.AsciSettings.default(), cd, E, cc)
+    assert np.array_equal(st, so)
+    assert np.array_equal(rv, ro)                     # same summation order
+    sr, rr = ref.asci_pairs(ref.ham(64, norb, T, V),
+                            oracle.AsciSettings.default(), cd, E, cc)
+    assert np.array_equal(st, sr)
+    assert np.all(np.abs(rv - rr) <= 1e-12 * np.abs(rr) + 1e-15 * np.abs(rr).max())
+
+
+@pytest.mark.parametrize("ndets", [800, 5000, 30000])
+def test_search_matches_oracle_and_ref(port, ref, wcase, ndets):
+    norb, T, V, hp, cd, cc, E = wcase
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+    got = mb.asci_search(_settings(), ndets, cd, E, cc, norb, H)
+    exp = port.asci_search(hp, oracle.AsciSettings.default(), ndets, cd, E, cc)
+    assert np.array_equal(got, exp)
+    r = ref.asci_search(ref.ham(64, norb, T, V), oracle.AsciSettings.default(),
+                        ndets, cd, E, cc)
+    assert len(r) == len(got)
+    diff = _tuples(got) ^ _tuples(r)
+    # only boundary ties may differ: their scores equal the k-th score
+    if diff:
+        st, rv = port.asci_pairs(hp, oracle.AsciSettings.default(), cd, E, cc)
+        score = {tuple(s): abs(v) for s, v in zip(st.tolist(), rv)}
+        kth = min(score[t] for t in _tuples(got[:-len(cd)]))
+        for t in diff:
+            assert abs(score[t] - kth) <= 1e-12 * kth
+
+
+def test_search_128_and_256_bits(port, wcase):
+    norb, T, V, hp, cd, cc, E = wcase
+    H64 = mb.HamiltonianGenerator(T, V, 64, norb)
+    base = mb.asci_search(_settings(), 5000, cd, E, cc, norb, H64)
+    for nbits in (128,):
+        H = mb.HamiltonianGenerator(T, V, nbits, norb)
+        got = mb.asci_search(_settings(), 5000, embed(cd, 64, nbits), E, cc,
+                             norb, H)
+        assert _tuples(embed(got, nbits, 64)) == _tuples(base)
+    # 256 bits (no reference): oracle restatement on a smaller problem
+    T2, V2, d2 = fci(10, 3, 3, 64, seed=2)
+    hp2 = port.ham(256, 10, T2, V2)
+    cd2 = embed(d2[:40], 64, 256)
+    c2 = np.linspace(1.0, 0.1, 40)
+    H2 = mb.HamiltonianGenerator(T2, V2, 256)
+    E2 = -1.0
+    got = mb.asci_search(_settings(), 1000, cd2, E2, c2, 10, H2)
+    exp = port.asci_search(hp2, oracle.AsciSettings.default(), 1000, cd2, E2, c2)
+    assert np.array_equal(got, exp)
+
+
+def test_search_edge_cases(port, wcase):
+    norb, T, V, hp, cd, cc, E = wcase
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+    os_ = oracle.AsciSettings.default
+    # just singles
+    got = mb.asci_search(_settings(just_singles=True), 300, cd, E, cc, norb, H)
+    exp = port.asci_search(hp, os_(just_singles=1), 300, cd, E, cc)
+    assert np.array_equal(got, exp)
+    # loose screening threshold
+    got = mb.asci_search(_settings(h_el_tol=1e-3), 2000, cd, E, cc, norb, H)
+    exp = port.asci_search(hp, os_(h_el_tol=1e-3), 2000, cd, E, cc)
+    assert np.array_equal(got, exp)
+    # k larger than the candidate count: everything kept
+    got = mb.asci_search(_settings(), 10 ** 7, cd[:3], E, cc[:3], norb, H)
+    exp = port.asci_search(hp, os_(), 10 ** 7, cd[:3], E, cc[:3])
+    assert np.array_equal(got, exp)
+    # single core determinant, empty core list
+    got = mb.asci_search(_settings(), 50, cd[:1], E, cc[:1], norb, H)
+    assert np.array_equal(got, port.asci_search(hp, os_(), 50, cd[:1], E, cc[:1]))
+    got = mb.asci_search(_settings(), 50, cd[:0], E, cc[:0], norb, H)
+    assert len(got) == 0
+
+
+def test_search_batched_merge(port, wcase, monkeypatch):
+    norb, T, V, hp, cd, cc, E = wcase
+    monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", "50000")
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+    st, rv = mb.asci_pairs(_settings(), cd, E, cc, H)
+    assert mb.last_search_stats(H)["batches"] > 1
+    so, ro = port.asci_pairs(hp, oracle.AsciSettings.default(), cd, E, cc)
+    assert np.array_equal(st, so)
+    np.testing.assert_allclose(rv, ro, rtol=1e-12, atol=1e-15 * np.abs(ro).max())
+    got = mb.asci_search(_settings(), 5000, cd, E, cc, norb, H)
+    exp = port.asci_search(hp, oracle.AsciSettings.default(), 5000, cd, E, cc)
+    assert len(_tuples(got) ^ _tuples(exp)) <= 2
+
+
+def test_water_grow_refine_golden():
+    norb, T, V, _ = water()
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+    s = _settings(ntdets_max=K["water_asci_ntdets_max"])
+    ci = mb.MCSCFSettings()
+    hf = mb.canonical_hf_determinant(5, 5, 64)
+    E0 = H.matrix_element(hf, hf)
+    E, dets, X = mb.asci_grow(s, ci, E0, hf, np.ones(1), H, norb)
+    assert len(dets) == 10000 and abs(X @ X - 1) < 1e-10
+    assert abs(E - K["water_asci_grow_e0"]) < 1e-8
+    E, dets, X = mb.asci_refine(s, ci, E, dets, X, H, norb)
+    assert len(dets) == 10000
+    assert abs(E - K["water_asci_refine_e0"]) < 1e-7

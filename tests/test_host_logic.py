@@ -1,0 +1,133 @@
+"""Host-side logic that needs no GPU: determinant spaces, integrals, the
+Rayleigh-Ritz eigensolver, the C ABI surface and the row-block partition."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import macis_b200 as mb
+import oracle
+from macis_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_header_symbols_exported():
+    hdr = open(os.path.join(ROOT, "include", "macis_b200.h")).read()
+    names = set(re.findall(r"\b(macis_b200_\w+)\s*\(", hdr))
+    assert names, "no declarations found"
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    for n in sorted(names):
+        assert hasattr(lib, n), n
+    assert names == set(_lib.EXPORTS)
+    assert _lib.LIB.macis_b200_version() == 1
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """ctypes mirrors agree with the C header (compiled here with gcc)."""
+    import subprocess
+    src = tmp_path / "sz.c"
+    src.write_text('#include <stdio.h>\n#include "macis_b200.h"\nint main(){'
+                   'printf("%zu %zu %zu %zu", sizeof(macis_b200_asci_settings),'
+                   'sizeof(macis_b200_asci_stats),'
+                   'sizeof(macis_b200_davidson_opts),'
+                   'sizeof(macis_b200_build_stats));return 0;}')
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True,
+                                          text=True).stdout.split()]
+    assert got == [ctypes.sizeof(_lib.AsciSettingsC),
+                   ctypes.sizeof(_lib.AsciStatsC),
+                   ctypes.sizeof(_lib.DavidsonOptsC),
+                   ctypes.sizeof(_lib.BuildStatsC)]
+    assert ctypes.sizeof(_lib.AsciSettingsC) == ctypes.sizeof(
+        oracle.AsciSettings)
+
+
+@pytest.mark.parametrize("nbits", [64, 128, 256])
+def test_spaces_match_oracle(port, nbits):
+    assert np.array_equal(mb.generate_hilbert_space(7, 3, 2, nbits),
+                          port.hilbert_space(nbits, 7, 3, 2))
+    hf = mb.canonical_hf_determinant(4, 3, nbits)
+    assert np.array_equal(hf, port.hf_det(nbits, 4, 3))
+    assert np.array_equal(mb.generate_cisd_hilbert_space(9, hf, nbits),
+                          port.cisd_space(nbits, 9, 4, 3))
+
+
+def test_hilbert_space_matches_reference(ref):
+    for nbits in (64, 128):
+        assert np.array_equal(mb.generate_hilbert_space(8, 4, 3, nbits),
+                              ref.hilbert_space(nbits, 8, 4, 3))
+        hf = mb.canonical_hf_determinant(4, 4, nbits)
+        assert np.array_equal(mb.generate_cisd_hilbert_space(10, hf, nbits),
+                              ref.cisd_space(nbits, 10, 4, 4))
+
+
+def test_canonical_strings_roundtrip():
+    d = mb.sd.make_dets([0b1011], [0b0110], 128)
+    s = mb.to_canonical_string(d, 128)
+    assert s[:4] == "u22u"[:1] + "2" + "d" + "u"
+    assert np.array_equal(mb.from_canonical_string(s, 128), d)
+
+
+def test_synthetic_integrals():
+    T, V = mb.synthetic_integrals(6, seed=3)
+    n = 6
+    T2 = T.reshape(n, n, order="F")
+    V4 = V.reshape(n, n, n, n, order="F")
+    assert np.array_equal(T2, T2.T)
+    np.testing.assert_allclose(np.diag(T2), -1.5 + 2.5 * np.arange(n) / (n - 1))
+    for perm in [(1, 0, 2, 3), (0, 1, 3, 2), (2, 3, 0, 1), (3, 2, 1, 0)]:
+        assert np.allclose(V4, V4.transpose(perm), atol=1e-15)
+    w = np.linalg.eigvalsh(V.reshape(n * n, n * n, order="F"))
+    assert w.min() > -1e-12
+    T3, V3 = mb.synthetic_integrals(6, seed=3)
+    assert np.array_equal(T, T3) and np.array_equal(V, V3)
+
+
+def test_water_fcidump_fill():
+    from golden_data import water
+    norb, T, V, ec = water()
+    assert norb == 24 and ec != 0.0
+    V4 = V.reshape((norb,) * 4, order="F")
+    assert np.allclose(V4, V4.transpose(1, 0, 3, 2))
+    assert np.allclose(V4, V4.transpose(2, 3, 0, 1))
+
+
+def test_small_syev_against_numpy():
+    rng = np.random.default_rng(0)
+    for k in (1, 3, 17, 64, 250):
+        M = rng.standard_normal((k, k))
+        S = np.tril(M) + np.tril(M, -1).T
+        w, v = np.linalg.eigh(S)
+        nw = min(6, k)
+        W, Vv = mb.small_syev(np.tril(M), nw)
+        np.testing.assert_allclose(W, w[:nw], atol=1e-12 * max(1, abs(w).max()))
+        np.testing.assert_allclose(np.abs(np.sum(Vv * v[:, :nw], 0)), 1,
+                                   atol=1e-10)
+    for M in (np.zeros((4, 4)), np.kron(np.eye(3), [[2., 1.], [1., 2.]])):
+        W, Vv = mb.small_syev(np.tril(M), 4)
+        assert np.abs(Vv.T @ Vv - np.eye(4)).max() < 1e-12
+        assert np.abs(M @ Vv - Vv * W).max() < 1e-12
+
+
+def test_row_bounds_partition():
+    for M in (0, 1, 7, 853776):
+        for w in (1, 2, 3, 8):
+            b = [mb.row_bounds(M, w, r) for r in range(w)]
+            assert b[0][0] == 0 and b[-1][1] == M
+            assert all(b[i][1] == b[i + 1][0] for i in range(w - 1))
+
+
+def test_settings_defaults_match_reference():
+    s = mb.ASCISettings()
+    o = oracle.AsciSettings.default()
+    for f, _ in _lib.AsciSettingsC._fields_:
+        if f != "pad_":
+            assert getattr(s.c_struct(), f) == getattr(o, f), f
+    m = mb.MCSCFSettings()
+    assert (m.ci_res_tol, m.ci_max_subspace) == (1e-8, 20)
+    assert m.ci_matel_tol == np.finfo(float).eps
