@@ -1,0 +1,483 @@
+#!/usr/bin/env python
+"""Benchmark of the selected-CI hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): the CSR Hamiltonian of the CAS(12e,12o) full-CI space --
+853,776 determinants as bitset<64>, seeded synthetic integrals (seed 0,
+orbital energies -1.5 + 2.5 p/(n-1), symmetric N(0, 0.02^2) one-electron
+off-diagonals, (pq|rs) = sum_{L<2n} B^L_pq B^L_rs with B^L entries
+N(0, (0.3 exp(-L/n))^2)), FP64 values, int32 indices, |h| > DBL_EPSILON.
+With N GPUs each rank builds the row block of the reference's row partition
+(make_dist_csr_hamiltonian) of the same matrix (strong scaling).
+
+`value` is H-build nnz/s with the determinants resident in HBM; `e2e` is the
+same through the C ABI with pinned host buffers (determinants in, full CSR
+out). After the timed steps (rank 0, N = 1) the same run reports the SpMV,
+FP64 and mixed-precision Davidson on this matrix and an ASCI search on an
+n = 48 bitset<128> instance, outside `value`.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("ASCI time & H-build nnz/s: learned+mixed vs plain FP64, one GPU, "
+          "ΔE≤0.1mEh")
+WORKLOAD = ("CAS(12e,12o) full-CI CSR Hamiltonian build: 853,776 dets "
+            "(bitset<64>), synthetic integrals seed 0, FP64 values, int32 "
+            "indices, |h| > DBL_EPSILON")
+NORB, NA, NB, SEED = 12, 6, 6, 0
+THRESH = float(np.finfo(np.float64).eps)
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def c2_inputs():
+    import macis_b200 as mb
+    T, V = mb.synthetic_integrals(NORB, SEED)
+    dets = mb.generate_hilbert_space(NORB, NA, NB, 64)
+    return T, V, dets
+
+
+def alg_bytes(nnz, nrows, nbra, nket, idx_b=4, val_b=8, det_b=8):
+    """Algorithmic bytes of one build: CSR written once, dets read once."""
+    return nnz * (idx_b + val_b) + (nrows + 1) * idx_b + (nbra + nket) * det_b
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                smax = float(c[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown",
+                                "sw_thermal_slowdown", "sw_power_cap"), c[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_reference_rate(T, V, dets, target_s=12.0, nthreads=None):
+    """Reference MACIS (compiled oracle/_ref) H build over a bounded sample of
+    rows, all host threads: nnz/s."""
+    import oracle
+    R = oracle.ref()
+    nthreads = nthreads or os.cpu_count() or 1
+    R.set_threads(1)
+    h = R.ham(64, NORB, T, V)
+    rows = max(nthreads * 4, 64)
+    t = time.perf_counter()
+    A = R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
+    dt = time.perf_counter() - t
+    per_row = dt / rows
+    rows = int(min(len(dets), max(rows, target_s / max(per_row, 1e-9))))
+    t = time.perf_counter()
+    A = R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
+    dt = time.perf_counter() - t
+    return {"value": A.nnz / dt, "unit": "nnz/s", "cores": nthreads,
+            "kind": "reference", "rows": rows, "seconds": dt, "nnz": A.nnz,
+            "sample": f"reference DoubleLoop make_csr_hamiltonian_block on "
+                      f"rows [0,{rows}) x all {len(dets)} kets of the same "
+                      f"matrix, {nthreads} threads over row blocks"}
+
+
+# ---------------------------------------------------------------- reference
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "compiled reference oracle/_ref/libmacis_ref.so "
+                          "missing"}))
+        return 0
+    T, V, dets = c2_inputs()
+    nthreads = os.cpu_count() or 1
+    R = oracle.ref()
+    R.set_threads(1)
+    h = R.ham(64, NORB, T, V)
+    # size each step to about 6 s of host work
+    probe = max(64, 4 * nthreads)
+    t = time.perf_counter()
+    R.csr(h, dets[:probe], dets, THRESH, nthreads=nthreads)
+    per_row = (time.perf_counter() - t) / probe
+    rows = int(min(len(dets), max(probe, 6.0 / max(per_row, 1e-9))))
+    for _ in range(args.warmup):
+        R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
+    times, nnz = [], 0
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        A = R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
+        times.append(time.perf_counter() - t)
+        nnz = A.nnz
+    tot = sum(times)
+    value = nnz * len(times) / tot
+    sample = (f"rows [0,{rows}) of the {len(dets)}-row matrix per step "
+              f"(DoubleLoopHamiltonianGenerator via make_csr_hamiltonian_block,"
+              f" {nthreads} threads over row blocks; the reference build loop "
+              f"itself is single-threaded)")
+    out = {"impl": "reference", "metric": METRIC, "value": value,
+           "unit": "nnz/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+           "higher_is_better": True, "scaling": "strong",
+           "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded integrals, BASELINE recipe)",
+           "config": {"workload": WORKLOAD, "sample_rows": rows},
+           "cpu_baseline": {"value": value, "unit": "nnz/s",
+                            "cores": nthreads, "kind": "reference",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": "nnz/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# --------------------------------------------------------------------- ours
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import macis_b200 as mb
+    from macis_b200 import _lib
+    from macis_b200._lib import LIB, check
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local_rank)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    def allsum(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return t.item()
+
+    T, V, dets = c2_inputs()
+    N = len(dets)
+    lo, hi = mb.row_bounds(N, world, rank)
+    H = mb.HamiltonianGenerator(T, V, 64)
+    d_dets = torch.from_numpy(dets.view(np.int64)).to(dev)  # resident input
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    import ctypes as C
+
+    def build_device():
+        c = C.c_void_p()
+        base = d_dets.data_ptr()
+        check(LIB.macis_b200_build_csr(H.handle, base + lo * 8, hi - lo, base,
+                                       N, THRESH, 4, 8, _lib.DEVICE_PTRS,
+                                       C.byref(c)))
+        return mb.DeviceCSR(c, H)
+
+    for _ in range(args.warmup):
+        A = build_device()
+        del A
+    barrier()
+    clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    launches0 = LIB.macis_b200_launch_count()
+    step_ms, fill_ms, nnz = [], [], 0
+    st = _lib.BuildStatsC()
+    barrier()
+    for _ in range(args.steps):
+        flush.zero_()                                   # L2 flush (256 MB)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        A = build_device()
+        e1.record()
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        check(LIB.macis_b200_csr_build_stats(A.handle, C.byref(st)))
+        fill_ms.append(st.fill_ms)
+        nnz = A.nnz
+        direct = bool(st.direct_product)
+        del A
+    barrier()
+    launches = LIB.macis_b200_launch_count() - launches0
+    ck = clocks.stop() if clocks else None
+    tot_ms = allmax(sum(step_ms))
+    nnz_all = allsum(float(nnz))
+    value = nnz_all * args.steps / (tot_ms / 1e3)
+    res = {}
+    if rank == 0:
+        peak, peak_kind = peaks()
+        fill_avg = sum(fill_ms) / len(fill_ms)
+        B = alg_bytes(nnz, hi - lo, hi - lo, N)
+        achieved = B / (fill_avg / 1e3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "hbuild_fill_c2_traffic.json")
+        if os.path.exists(tf):
+            with open(tf) as f:
+                traffic = json.load(f).get("dram_bytes_per_launch")
+        res.update({
+            "metric": METRIC, "value": value, "unit": "nnz/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded integrals, BASELINE recipe, seed 0)",
+            "config": {"workload": WORKLOAD, "ndets": N, "nnz": int(nnz_all),
+                       "rows_per_rank": hi - lo, "direct_product_path": direct,
+                       "l2": "256 MB flush between steps; output 18.6 GB > L2",
+                       "parallelism": f"row-block x{world}"},
+            "clocks": ck,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "dp_fill_k",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "frac_of_8TBs": achieved / 8000.0,
+                         "alg_bytes_per_launch": B, "fill_ms": fill_avg,
+                         "traffic": traffic},
+        })
+    # ---------------- end-to-end through the C ABI with host buffers
+    e2e = None
+    if world == 1 and not args.no_e2e:
+        e2e = bench_e2e(args, mb, LIB, check, _lib, H, dets, torch)
+    barrier()
+    if rank == 0:
+        res["e2e"] = e2e
+        if world == 1 and not args.no_extras:
+            res["extras"] = extras(mb, H, dets, torch)
+        if world == 1 and not args.no_cpu:
+            try:
+                res["cpu_baseline"] = cpu_reference_rate(T, V, dets)
+            except Exception as e:  # noqa: BLE001
+                res["cpu_baseline"] = {"unavailable": str(e)}
+        print(json.dumps(res))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def bench_e2e(args, mb, LIB, check, _lib, H, dets, torch):
+    import ctypes as C
+    N = len(dets)
+    h_dets = torch.from_numpy(dets.view(np.int64)).pin_memory()
+    c = C.c_void_p()
+    p = h_dets.data_ptr()
+    check(LIB.macis_b200_build_csr(H.handle, p, N, p, N, THRESH, 4, 8, 0,
+                                   C.byref(c)))
+    A = mb.DeviceCSR(c, H)
+    nnz = A.nnz
+    try:
+        rp = torch.empty(N + 1, dtype=torch.int32, pin_memory=True)
+        ci = torch.empty(nnz, dtype=torch.int32, pin_memory=True)
+        nz = torch.empty(nnz, dtype=torch.float64, pin_memory=True)
+        pinned = True
+    except RuntimeError:
+        rp = torch.empty(N + 1, dtype=torch.int32)
+        ci = torch.empty(nnz, dtype=torch.int32)
+        nz = torch.empty(nnz, dtype=torch.float64)
+        pinned = False
+    del A
+    steps = max(1, min(args.steps, 3))
+    times = []
+    for it in range(steps + 1):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = C.c_void_p()
+        check(LIB.macis_b200_build_csr(H.handle, p, N, p, N, THRESH, 4, 8, 0,
+                                       C.byref(c)))
+        check(LIB.macis_b200_csr_download(c, rp.data_ptr(), ci.data_ptr(),
+                                          nz.data_ptr(), 0))
+        LIB.macis_b200_csr_destroy(c)
+        e1.record()
+        torch.cuda.synchronize()
+        if it:                                    # first call is a warm-up
+            times.append(e0.elapsed_time(e1))
+    t = sum(times) / len(times) / 1e3
+    return {"value": nnz / t, "unit": "nnz/s", "ms_per_step": t * 1e3,
+            "h2d_bytes_per_step": int(h_dets.numel() * 8),
+            "d2h_bytes_per_step": int((N + 1) * 4 + nnz * 12),
+            "pinned": pinned, "steps": len(times)}
+
+
+def extras(mb, H, dets, torch):
+    """SpMV, Davidson (FP64 / mixed) and ASCI timings outside `value`."""
+    import ctypes as C
+
+    from macis_b200._lib import LIB, check
+    out = {}
+    N = len(dets)
+    peak, _ = peaks()
+    for prec, vt in (("fp64", np.float64), ("mixed", np.float32)):
+        A = mb.make_csr_hamiltonian(dets, H, THRESH, value_t=vt)
+        x = torch.randn(N, dtype=torch.float64, device="cuda")
+        y = torch.empty(N, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            check(LIB.macis_b200_spmv(A.handle, 1, 1.0, x.data_ptr(), N, 0.0,
+                                      y.data_ptr(), N, 1))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 10
+        e0.record()
+        for _ in range(reps):
+            check(LIB.macis_b200_spmv(A.handle, 1, 1.0, x.data_ptr(), N, 0.0,
+                                      y.data_ptr(), N, 1))
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        vb = 8 if prec == "fp64" else 4
+        B = A.nnz * (4 + vb) + (N + 1) * 4 + 2 * N * 8 + (N * 8 if vb == 4 else 0)
+        out[f"spmv_{prec}"] = {"ms": ms, "GBps": B / ms / 1e6,
+                               "frac_of_measured_hbm": B / ms / 1e6 / peak,
+                               "nnz": A.nnz}
+        X = np.zeros(N)
+        t = time.perf_counter()
+        try:
+            it, E = mb.davidson(N, 40, mb.SparseMatrixOperator(A), None, 1e-8,
+                                X, use_guess=False, restart_keep=8,
+                                max_iter=3000)
+            out[f"davidson_{prec}"] = {"seconds": time.perf_counter() - t,
+                                       "iterations": it, "E0": E,
+                                       "max_m": 40, "restart_keep": 8,
+                                       "tol": 1e-8}
+        except RuntimeError as e:
+            out[f"davidson_{prec}"] = {"error": str(e)}
+        del A
+    if "E0" in out.get("davidson_fp64", {}) and "E0" in out.get("davidson_mixed", {}):
+        out["mixed_dE_Eh"] = out["davidson_mixed"]["E0"] - out["davidson_fp64"]["E0"]
+    try:
+        out["asci_search_n48"] = asci_extra(mb)
+    except Exception as e:  # noqa: BLE001
+        out["asci_search_n48"] = {"error": str(e)}
+    return out
+
+
+def asci_extra(mb, ncore=10000, ndets_max=1000000, seed=0):
+    """One asci_search on n = 48 orbitals, 12 alpha / 12 beta, bitset<128>:
+    HF plus its lowest singles / doubles as the core set with decaying
+    coefficients (C3-shaped, exact FP64 search)."""
+    n, k = 48, 12
+    T, V = mb.synthetic_integrals(n, seed)
+    H = mb.HamiltonianGenerator(T, V, 128)
+    rng = np.random.default_rng(seed)
+    hf = (1 << k) - 1
+    alphas = {hf}
+    while len(alphas) < 400:
+        a = hf
+        for _ in range(rng.integers(1, 3)):
+            i = int(rng.integers(0, k))
+            v = int(rng.integers(k, n))
+            if a >> i & 1 and not a >> v & 1:
+                a ^= (1 << i) ^ (1 << v)
+        alphas.add(a)
+    alphas = sorted(alphas, key=lambda x: bin(x ^ hf).count("1"))
+    pairs = [(a, b) for a in alphas[:200] for b in alphas[:200]]
+    pairs.sort(key=lambda ab: bin(ab[0] ^ hf).count("1") + bin(ab[1] ^ hf).count("1"))
+    pairs = pairs[:ncore]
+    core = mb.sd.make_dets([a for a, _ in pairs], [b for _, b in pairs], 128)
+    C = np.exp(-0.5 * np.arange(len(core)) / 100.0)
+    C /= np.linalg.norm(C)
+    hd = H.matrix_element(core[:1], core[:1])
+    s = mb.ASCISettings()
+    t = time.perf_counter()
+    out = mb.asci_search(s, ndets_max, core, hd - 0.5, C, n, H)
+    dt = time.perf_counter() - t
+    st = mb.last_search_stats(H)
+    return {"seconds": dt, "ncdets": len(core), "ndets_max": ndets_max,
+            "returned": len(out), "raw_pairs": st["raw_pairs"],
+            "unique_pairs": st["unique_pairs"], "batches": st["batches"],
+            "raw_pairs_per_s": st["raw_pairs"] / dt,
+            "phase_ms": {k2: st[k2] for k2 in ("pairs_ms", "sort_ms",
+                                               "keep_ms", "topk_ms")}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local_rank = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

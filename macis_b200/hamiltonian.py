@@ -162,6 +162,12 @@ class DeviceCSR:
         check(LIB.macis_b200_csr_diagonal(self._c, d.ctypes.data, 0))
         return d
 
+    def build_stats(self):
+        """Timings and path of the build (CUDA events on the build stream)."""
+        st = _lib.BuildStatsC()
+        check(LIB.macis_b200_csr_build_stats(self._c, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
     def mem_footprint(self):
         ib = np.dtype(self.index_t).itemsize
         vb = np.dtype(self.value_t).itemsize

@@ -49,6 +49,23 @@ def test_c1_fci_exact(ref):
     assert_csr_equal(A.to_host(), r)
 
 
+def test_row_blocks_of_direct_product(ref):
+    # the row partition of make_dist_csr_hamiltonian (csr_hamiltonian.hpp:
+    # 49-82): bra = contiguous slice of the ket list keeps the direct path
+    T, V, dets = fci(8, 4, 4, 64, seed=12)
+    H = mb.HamiltonianGenerator(T, V, 64)
+    hr = ref.ham(64, 8, T, V)
+    thr = np.finfo(float).eps
+    for r in range(3):
+        lo, hi = mb.row_bounds(len(dets), 3, r)
+        A = mb.make_csr_hamiltonian_block(dets[lo:hi], dets, H, thr)
+        assert A.build_stats()["direct_product"] == 1
+        assert_csr_equal(A.to_host(), ref.build_csr(hr, dets[lo:hi], dets, thr))
+        A32 = mb.make_csr_hamiltonian_block(dets[lo:hi], dets, H, thr,
+                                            value_t=np.float32)
+        assert np.array_equal(A32.to_host()[1], A.to_host()[1])
+
+
 @pytest.mark.parametrize("nbits", [64, 128])
 def test_general_path_shuffled_and_rectangular(ref, nbits):
     T, V, dets = fci(9, 4, 4, nbits, seed=5)
