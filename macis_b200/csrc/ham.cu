@@ -117,6 +117,7 @@ void ham_destroy(macis_b200_ham* h) {
   cudaFree(h->V_red);
   cudaFree(h->G2_red);
   cudaFree(h->V2_red);
+  cudaFree(h->VT);
   if(h->stream) cudaStreamDestroy(h->stream);
 }
 

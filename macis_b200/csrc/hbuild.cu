@@ -26,6 +26,8 @@
 // Matrix elements follow the reference summation order exactly
 // (common.cuh), so values are bit-identical to the reference.
 #include <algorithm>
+#include <type_traits>
+#include <vector>
 
 #include "internal.hpp"
 #include "primitives.cuh"
@@ -243,105 +245,362 @@ __device__ __forceinline__ float store_val<float>(double h, bool is_diag) {
   return is_diag ? 0.0f : float(h);
 }
 
-// Direct-product fill: one warp per row, entries emitted in ascending
-// column order, threshold compaction by ballot.
+// Direct-product fill. A CTA of DP_WARPS warps takes DP_WARPS rows that
+// share one beta string B (rows (A..A+7, B)); the beta lists L2(B), L4(B)
+// are staged once in shared memory, as are T, G_red and V_red when they fit.
+// Each warp first evaluates all Slater-Condon singles of its bra into a
+// shared table F[spin][v*n + o] (lanes in parallel, reference summation
+// order), then emits the row: entries are produced in ascending column order
+// as the concatenation over connected alpha strings A' of the beta lists,
+// two 32-entry rounds in flight, threshold compaction by ballot and
+// streaming stores (the output must not evict the integrals from L2).
+constexpr int DP_WARPS = 8;
+constexpr int DP_THREADS = 32 * DP_WARPS;
+
+struct DPShared {
+  int n, stage_ints;
+  int64_t l2max, l4max;
+  size_t ints_off, f_off, l2_off, l4_off, occ_off, bytes;
+};
+
+__host__ __device__ inline DPShared dp_shared_layout(int n, int stage_ints,
+                                                     int64_t l2max,
+                                                     int64_t l4max) {
+  DPShared L;
+  L.n = n;
+  L.stage_ints = stage_ints;
+  L.l2max = l2max;
+  L.l4max = l4max;
+  size_t o = 0;
+  L.ints_off = o;
+  if(stage_ints) o += (size_t(n) * n + 2 * size_t(n) * n * n) * 8;
+  L.f_off = o;
+  o += size_t(DP_WARPS) * 2 * n * n * 8;
+  L.l2_off = o;
+  o += size_t(l2max) * 8;
+  L.l4_off = o;
+  o += size_t(l4max) * 8;
+  L.occ_off = o;
+  o += size_t(DP_WARPS) * 4 * 128;  // occ/vir lists, both spins
+  L.bytes = (o + 15) & ~size_t(15);
+  return L;
+}
+
+template <typename CI, typename VT>
+__device__ __forceinline__ void dp_store(CI* colind, VT* nzval, int64_t pos,
+                                         int64_t col, double h, bool isd) {
+  __stcs(reinterpret_cast<typename std::conditional<sizeof(CI) == 4, int,
+                                                    long long>::type*>(colind) +
+             pos,
+         (typename std::conditional<sizeof(CI) == 4, int, long long>::type)col);
+  __stcs(nzval + pos, store_val<VT>(h, isd));
+}
+
+// Packed list words of the fill (y of a uint2 whose x is the partner
+// string index): bits 0..27 an integral offset, bits 29..30 the excitation
+// class (0 none, 1 single, 2 double), bit 31 the fermionic sign.
+//   alpha list:  single -> pair index a = v1 + o1 n (row a of VT)
+//                double -> G offset of (v1,o1,v2,o2)
+//   beta L2:     single -> pair index b = v1 + o1 n (column b of VT)
+//   beta L4:     single -> singles-table index n^2 + v1 n + o1
+//                double -> G offset
+__global__ void dp_encode_k(uint32_t* info, int64_t m, int n, int which) {
+  const uint32_t n2 = uint32_t(n) * n;
+  for(int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+      i += int64_t(gridDim.x) * blockDim.x) {
+    const uint32_t e = info[i];
+    const int p = int(e >> 29);
+    const uint32_t sg = (e >> 28) & 1u;
+    uint32_t off = 0, cls = 0;
+    const uint32_t o1 = ex_o1(e), v1 = ex_v1(e), o2 = ex_o2(e), v2 = ex_v2(e);
+    if(p == 2) {
+      cls = 1;
+      if(which == 0 || which == 1)
+        off = v1 + o1 * n;  // pair index: row of VT (alpha) / column (beta)
+      else
+        off = n2 + v1 * n + o1;
+    } else if(p == 4) {
+      cls = 2;
+      off = v1 + n * (o1 + n * (v2 + n * o2));
+    }
+    info[i] = off | (cls << 29) | (sg << 31);
+  }
+}
+
+// VT[a n^2 + b] = V[a + b n^2] for pair indices a, b < n^2
+__global__ void v_pair_transpose_k(const double* V, double* VT, int n) {
+  const size_t n2 = size_t(n) * n, n4 = n2 * n2;
+  for(size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x; x < n4;
+      x += size_t(gridDim.x) * blockDim.x)
+    VT[(x % n2) * n2 + x / n2] = V[x];
+}
+
+__device__ __forceinline__ double sgnd(uint32_t w, double v) {
+  return (w >> 31) ? -v : v;  // == sign * v for sign in {+1, -1}
+}
+
 template <int NBITS, typename CI, typename VT>
-__global__ void __launch_bounds__(HB_THREADS)
-    dp_fill_k(Ints I, DPData d, const double* __restrict__ hdiag,
+__global__ void __launch_bounds__(DP_THREADS, 4)
+    dp_fill_k(Ints I, const double* __restrict__ Vt, DPData d, DPShared L,
+              const double* __restrict__ hdiag,
               const int64_t* __restrict__ rowptr, CI* __restrict__ colind,
               VT* __restrict__ nzval, double* __restrict__ diag,
               int64_t* __restrict__ rowcnt, double thresh, int64_t r0,
               int64_t nrows) {
   constexpr int NSW = DetTraits<NBITS>::NSW;
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarp = int64_t(gridDim.x) * HB_WARPS;
-  for(int64_t row = int64_t(blockIdx.x) * HB_WARPS + (threadIdx.x >> 5);
-      row < nrows; row += nwarp) {
-    const int64_t A = (r0 + row) / d.UB, B = (r0 + row) % d.UB;
-    const Spin<NSW> sa = ld_spin<NSW>(d.ua, A), sb = ld_spin<NSW>(d.ub, B);
-    const int64_t l2b = d.l2off[B], n2 = d.l2off[B + 1] - l2b;
-    const int64_t l4b = d.l4off[B], n4 = d.l4off[B + 1] - l4b;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ int32_t seg_pos[DP_WARPS][32];
+  __shared__ int32_t seg_col[DP_WARPS][32];
+  __shared__ uint32_t seg_a[DP_WARPS][32];  // sign bit | VT row offset
+  __shared__ double seg_single[DP_WARPS][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int n = L.n;
+  const int n2 = n * n;
+  const double* sT = I.T;
+  const double* sG = I.G_red;
+  const double* sV = I.V_red;
+  if(L.stage_ints) {
+    double* p = reinterpret_cast<double*>(dsm + L.ints_off);
+    for(int x = threadIdx.x; x < n2; x += DP_THREADS) p[x] = I.T[x];
+    for(int x = threadIdx.x; x < n2 * n; x += DP_THREADS) {
+      p[n2 + x] = I.G_red[x];
+      p[n2 + n2 * n + x] = I.V_red[x];
+    }
+    sT = p;
+    sG = p + n2;
+    sV = p + n2 + n2 * n;
+  }
+  double* F = reinterpret_cast<double*>(dsm + L.f_off) + size_t(wid) * 2 * n2;
+  const uint2* sl2 = reinterpret_cast<const uint2*>(dsm + L.l2_off);
+  const uint2* sl4 = reinterpret_cast<const uint2*>(dsm + L.l4_off);
+  uint8_t* occl = dsm + L.occ_off + size_t(wid) * 512;  // occ[2][128]
+  uint8_t* virl = occl + 256;                           // vir[2][128]
+  const double* __restrict__ gG = I.G;
+  const double* __restrict__ gVT = Vt;
+  const int32_t UB = int32_t(d.UB);
+  const int64_t A_lo = r0 / d.UB, A_hi = (r0 + nrows - 1) / d.UB;
+  const int64_t nachunk = (A_hi - A_lo + DP_WARPS) / DP_WARPS;
+  const int64_t nitems = nachunk * d.UB;
+  for(int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int32_t B = int32_t(item % d.UB);
+    const int64_t ac = item / d.UB;
+    const int64_t l2b = d.l2off[B], l4b = d.l4off[B];
+    const int32_t n2l = int32_t(d.l2off[B + 1] - l2b);
+    const int32_t n4l = int32_t(d.l4off[B + 1] - l4b);
+    __syncthreads();  // previous item's lists are no longer read
+    uint2* wl2 = reinterpret_cast<uint2*>(dsm + L.l2_off);
+    uint2* wl4 = reinterpret_cast<uint2*>(dsm + L.l4_off);
+    const bool s2 = n2l <= L.l2max, s4 = n4l <= L.l4max;
+    if(s2)
+      for(int x = threadIdx.x; x < n2l; x += DP_THREADS)
+        wl2[x] = make_uint2(uint32_t(d.l2col[l2b + x]), d.l2info[l2b + x]);
+    if(s4)
+      for(int x = threadIdx.x; x < n4l; x += DP_THREADS)
+        wl4[x] = make_uint2(uint32_t(d.l4col[l4b + x]), d.l4info[l4b + x]);
+    __syncthreads();
+    const int64_t A = A_lo + ac * DP_WARPS + wid;
+    const int64_t grow = A * d.UB + B;
+    if(A > A_hi || grow < r0 || grow >= r0 + nrows) continue;
+    const int32_t row = int32_t(grow - r0);
+    const Spin<NSW> sp[2] = {ld_spin<NSW>(d.ua, A), ld_spin<NSW>(d.ub, B)};
+    // occupied / virtual lists, one orbital per lane
+    int no[2], nv[2];
+#pragma unroll
+    for(int S = 0; S < 2; ++S) {
+      no[S] = sp_popc(sp[S]);
+      nv[S] = n - no[S];
+      for(int i = lane; i < n; i += 32) {
+        int below = 0;  // occupied orbitals below i
+#pragma unroll
+        for(int w = 0; w < NSW; ++w) {
+          const int lo = 64 * w;
+          if(i > lo)
+            below += __popcll(sp[S].w[w] &
+                              (i - lo >= 64 ? ~0ull : ((1ull << (i - lo)) - 1)));
+        }
+        if(sp_test(sp[S], i))
+          occl[S * 128 + below] = uint8_t(i);
+        else
+          virl[S * 128 + (i - below)] = uint8_t(i);
+      }
+    }
+    __syncwarp();
+    // singles table: F[spin][v*n + o] = T(v,o) + sum_{p in occ_same}
+    // G_red(p,v,o) + sum_{p in occ_other} V_red(p,v,o)  (matrix_elements.hpp:
+    // 76-96 without the sign), v occupied and o empty in the bra
+    {
+      const int nsa = no[0] * nv[0], nsb = no[1] * nv[1];
+      for(int t = lane; t < nsa + nsb; t += 32) {
+        const int S = t < nsa ? 0 : 1;
+        const int u = S ? t - nsa : t;
+        const int v = occl[S * 128 + u / nv[S]], o = virl[S * 128 + u % nv[S]];
+        double h = sT[v + o * n];
+        const double* Gov = sG + v * n + o * n2;
+        const double* Vov = sV + v * n + o * n2;
+        for(int p = 0; p < no[S]; ++p) h += Gov[occl[S * 128 + p]];
+        for(int p = 0; p < no[1 - S]; ++p) h += Vov[occl[(1 - S) * 128 + p]];
+        F[S * n2 + v * n + o] = h;
+      }
+    }
+    __syncwarp();
+    const double hd = hdiag[row];
     const int64_t out0 = rowptr[row];
-    int64_t kept = 0;
+    CI* __restrict__ rc = colind + out0;
+    VT* __restrict__ rv = nzval + out0;
+    int32_t pos = 0, dropped = 0;
+    uint2 el = make_uint2(0u, 0u);  // this lane's entry of the beta L2 list
+    if(lane < n2l)
+      el = s2 ? sl2[lane]
+              : make_uint2(uint32_t(__ldg(d.l2col + l2b + lane)),
+                           __ldg(d.l2info + l2b + lane));
+    auto put = [&](bool act, int32_t p, int32_t col, double h) {
+      const bool keep = act && fabs(h) > thresh;
+      dropped += __popc(__ballot_sync(0xffffffffu, act && !keep));
+      if(act) {
+        const bool isd = keep && col == row;
+        __stcs(reinterpret_cast<typename std::conditional<
+                   sizeof(CI) == 4, int, long long>::type*>(rc) + p,
+               (typename std::conditional<sizeof(CI) == 4, int, long long>::type)(
+                   keep ? col : -1));
+        __stcs(rv + p, store_val<VT>(h, isd));
+        if(isd) diag[row] = h;
+      }
+    };
     const int64_t c1 = d.aoff[A + 1];
     for(int64_t c = d.aoff[A]; c < c1; c += 32) {
       const int64_t j = c + lane;
-      int32_t Ap = 0;
-      uint32_t ainf = 0;
-      int pa = 7, cnt = 0;
+      int32_t colA = 0;
+      uint32_t ai = 0;
+      int cls = 3, cnt = 0;
       if(j < c1) {
-        Ap = __ldg(d.acol + j);
-        ainf = __ldg(d.ainfo + j);
-        pa = int(ainf >> 29);
-        cnt = pa == 0 ? int(n4) : pa == 2 ? int(n2) : 1;
+        colA = __ldg(d.acol + j) * UB;
+        ai = __ldg(d.ainfo + j);
+        cls = int((ai >> 29) & 3u);
+        cnt = cls == 0 ? n4l : cls == 1 ? n2l : 1;
       }
       const int incl = warp_incl_scan(cnt);
-      const int excl = incl - cnt;
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      for(int e0 = 0; e0 < total; e0 += 32) {
-        const int e = e0 + lane;
-        // owner lane: the last lane whose exclusive offset is <= e
-        int lo = 0;
-#pragma unroll
-        for(int step = 16; step; step >>= 1) {
-          const int cand = lo + step;
-          const int v = __shfl_sync(0xffffffffu, excl, cand & 31);
-          if(cand < 32 && v <= e) lo = cand;
-        }
-        const int owner = lo;
-        const int oex = __shfl_sync(0xffffffffu, excl, owner);
-        const int opa = __shfl_sync(0xffffffffu, pa, owner);
-        const int32_t oAp = __shfl_sync(0xffffffffu, Ap, owner);
-        const uint32_t oinf = __shfl_sync(0xffffffffu, ainf, owner);
-        bool keep = false;
+      const int32_t spos = pos + incl - cnt;
+      pos += __shfl_sync(0xffffffffu, incl, 31);
+      // (1) alpha doubles: beta unchanged, one entry each
+      {
+        const bool act = cls == 2;
         double h = 0;
-        int64_t colv = 0;
-        bool isd = false;
-        if(e < total) {
-          const int t = e - oex;
-          int32_t Bp;
-          uint32_t binf;
-          if(opa == 4) {
-            Bp = int32_t(B);
-            binf = 0;
-          } else if(opa == 2) {
-            Bp = __ldg(d.l2col + l2b + t);
-            binf = __ldg(d.l2info + l2b + t);
-          } else {
-            Bp = __ldg(d.l4col + l4b + t);
-            binf = __ldg(d.l4info + l4b + t);
-          }
-          const int pb = int(binf >> 29);
-          if(opa == 0) {
-            if(pb == 0)
-              h = hdiag[row];
-            else if(pb == 2)
-              h = me_single(I, binf, sb, sa);
-            else
-              h = me_ss_double(I, binf);
-          } else if(opa == 2) {
-            if(pb == 0)
-              h = me_single(I, oinf, sa, sb);
-            else
-              h = me_os_double(I, oinf, binf);
-          } else {
-            h = me_ss_double(I, oinf);
-          }
-          colv = int64_t(oAp) * d.UB + Bp;
-          isd = colv == row;  // extract_diagonal_elements: column == row
-          keep = fabs(h) > thresh;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if(keep) {
-          const int64_t pos = out0 + kept + __popc(m & lanemask_lt());
-          colind[pos] = CI(colv);
-          nzval[pos] = store_val<VT>(h, isd);
-          if(isd) diag[row] = h;
-        }
-        kept += __popc(m);
+        if(act) h = sgnd(ai, __ldg(gG + (ai & 0x0FFFFFFFu)));
+        put(act, spos, colA + B, h);
       }
+      // (2) the same-alpha segment: every beta string within two excitations
+      unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
+      while(m0) {
+        const int L0 = __ffs(m0) - 1;
+        m0 &= m0 - 1;
+        const int32_t sp0 = __shfl_sync(0xffffffffu, spos, L0);
+        const int32_t cA = __shfl_sync(0xffffffffu, colA, L0);
+        for(int32_t t = lane; t - lane < n4l; t += 32) {
+          const bool act = t < n4l;
+          double h = 0;
+          int32_t col = 0;
+          if(act) {
+            const uint2 ent = s4 ? sl4[t]
+                                 : make_uint2(uint32_t(__ldg(d.l4col + l4b + t)),
+                                              __ldg(d.l4info + l4b + t));
+            const uint32_t cb = (ent.y >> 29) & 3u, off = ent.y & 0x0FFFFFFFu;
+            // one generic load: singles table (shared) or G (global)
+            const double* src = cb == 1 ? F + off : gG + off;
+            const double v = *src;
+            col = cA + int32_t(ent.x);
+            h = cb == 0 ? hd : sgnd(ent.y, v);
+          }
+          put(act, sp0 + t, col, h);
+        }
+      }
+      // (3) alpha singles: one segment of n2l entries (beta within one
+      // excitation) per connected alpha string. Each lane keeps its beta
+      // list entry for the row; the warp sweeps the segments.
+      const unsigned m2 = __ballot_sync(0xffffffffu, cls == 1);
+      if(cls == 1) {
+        const int rk = __popc(m2 & lanemask_lt());
+        seg_pos[wid][rk] = spos;
+        seg_col[wid][rk] = colA;
+        const uint32_t pa_ = ai & 0x3FFFu;  // v1 + o1 n
+        seg_a[wid][rk] = (ai & 0x80000000u) | (pa_ * uint32_t(n2));
+        seg_single[wid][rk] =
+            sgnd(ai, F[(pa_ % uint32_t(n)) * n + pa_ / uint32_t(n)]);
+      }
+      __syncwarp();
+      const int k2 = __popc(m2);
+      {
+        const bool act = lane < n2l;
+        const bool bsame = ((el.y >> 29) & 3u) == 0;
+        const uint32_t boff = el.y & 0x0FFFFFFFu, bsg = el.y & 0x80000000u;
+        for(int q = 0; q < k2; ++q) {
+          const uint32_t sa = seg_a[wid][q];
+          const double v = __ldg(gVT + ((sa & 0x7FFFFFFFu) + boff));
+          const double h = bsame ? seg_single[wid][q] : sgnd(sa ^ bsg, v);
+          put(act, seg_pos[wid][q] + lane, seg_col[wid][q] + int32_t(el.x), h);
+        }
+      }
+      if(n2l > 32) {  // list entries 32.. of every segment, flattened
+        const int32_t w2 = n2l - 32;
+        const int32_t tot2 = k2 * w2;
+        const float invw = 1.0f / float(w2);
+        for(int32_t e = lane; e - lane < tot2; e += 32) {
+          const bool act = e < tot2;
+          double h = 0;
+          int32_t col = 0, p = 0;
+          if(act) {
+            int sg = int(float(e) * invw);
+            if(sg * w2 > e) --sg;
+            if((sg + 1) * w2 <= e) ++sg;
+            const int32_t t = 32 + e - sg * w2;
+            const uint2 ent = s2 ? sl2[t]
+                                 : make_uint2(uint32_t(__ldg(d.l2col + l2b + t)),
+                                              __ldg(d.l2info + l2b + t));
+            const uint32_t sa = seg_a[wid][sg];
+            const double v = __ldg(gVT + ((sa & 0x7FFFFFFFu) + (ent.y & 0x0FFFFFFFu)));
+            h = ((ent.y >> 29) & 3u) == 0 ? seg_single[wid][sg]
+                                           : sgnd(sa ^ (ent.y & 0x80000000u), v);
+            col = seg_col[wid][sg] + int32_t(ent.x);
+            p = seg_pos[wid][sg] + t;
+          }
+          put(act, p, col, h);
+        }
+      }
+      __syncwarp();
     }
-    if(lane == 0) rowcnt[row] = kept;
+    if(lane == 0) rowcnt[row] = int64_t(pos) - dropped;
+  }
+}
+
+// Removes the entries marked with column -1 while packing rows to their
+// final offsets (direct-product path with dropped elements).
+template <typename CI, typename VT>
+__global__ void compact_marked_k(const int64_t* oldptr, const int64_t* newptr,
+                                 size_t m, const CI* ci, const VT* nz, CI* ci2,
+                                 VT* nz2) {
+  const int lane = threadIdx.x & 31;
+  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
+  for(size_t r = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      r < m; r += nwarp) {
+    const int64_t s = oldptr[r], e = oldptr[r + 1];
+    int64_t o = newptr[r];
+    for(int64_t b = s; b < e; b += 32) {
+      const int64_t i = b + lane;
+      CI c = 0;
+      VT v = 0;
+      bool keep = false;
+      if(i < e) {
+        c = ci[i];
+        v = nz[i];
+        keep = c >= 0;
+      }
+      const unsigned msk = __ballot_sync(0xffffffffu, keep);
+      if(keep) {
+        const int64_t p = o + __popc(msk & lanemask_lt());
+        ci2[p] = c;
+        nz2[p] = v;
+      }
+      o += __popc(msk);
+    }
   }
 }
 
@@ -915,13 +1174,59 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     out->nnz_candidates = nnz_ub;
     MB_CUDA(cudaMallocAsync(&colind, std::max<int64_t>(nnz_ub, 1) * sizeof(CI), s));
     MB_CUDA(cudaMallocAsync(&nzval, std::max<int64_t>(nnz_ub, 1) * sizeof(VT), s));
+    {
+      const int nn0 = h->norb;
+      const int64_t na_ = to_host(aoff + UA, s), n2_ = to_host(l2off + UB, s),
+                    n4_ = to_host(l4off + UB, s);
+      dp_encode_k<<<grid_for(size_t(na_), 256, 8 * sms), 256, 0, s>>>(ainfo, na_, nn0, 0), note_launch();
+      dp_encode_k<<<grid_for(size_t(n2_), 256, 8 * sms), 256, 0, s>>>(l2info, n2_, nn0, 1), note_launch();
+      dp_encode_k<<<grid_for(size_t(n4_), 256, 8 * sms), 256, 0, s>>>(l4info, n4_, nn0, 2), note_launch();
+    }
     DPData d{int64_t(UA), int64_t(UB), ua, ub, aoff, acol, ainfo,
              l2off, l2col, l2info, l4off, l4col, l4info};
-    const unsigned g = grid_for(nbra, HB_WARPS, size_t(sms) * 16);
+    // shared-memory plan: integrals for the singles if they fit, the longest
+    // beta lists, per-warp singles tables
+    int64_t l2max = 0, l4max = 0;
+    {
+      std::vector<int64_t> h2(UB + 1), h4(UB + 1);
+      MB_CUDA(cudaMemcpyAsync(h2.data(), l2off, (UB + 1) * 8, cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaMemcpyAsync(h4.data(), l4off, (UB + 1) * 8, cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaStreamSynchronize(s));
+      for(size_t b = 0; b < UB; ++b) {
+        l2max = std::max(l2max, h2[b + 1] - h2[b]);
+        l4max = std::max(l4max, h4[b + 1] - h4[b]);
+      }
+    }
+    const int nn = h->norb;
+    const size_t ints_bytes = (size_t(nn) * nn + 2 * size_t(nn) * nn * nn) * 8;
+    int stage = ints_bytes <= 96 * 1024;
+    l2max = std::min<int64_t>(l2max, 2048);
+    l4max = std::min<int64_t>(l4max, 4096);
+    DPShared Ls = dp_shared_layout(nn, stage, l2max, l4max);
+    if(Ls.bytes > 200 * 1024) {
+      Ls = dp_shared_layout(nn, 0, std::min<int64_t>(l2max, 512),
+                            std::min<int64_t>(l4max, 1024));
+    }
+    MB_REQUIRE(Ls.bytes <= 220 * 1024, MACIS_B200_EINVAL,
+               "norb too large for the direct-product fill");
+    MB_REQUIRE(nket < (size_t(1) << 31) && nn <= 127, MACIS_B200_ECAPACITY,
+               "direct-product fill needs < 2^31 determinants");
+    MB_CUDA(cudaFuncSetAttribute(dp_fill_k<NBITS, CI, VT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(Ls.bytes)));
+    int per_sm = 0;
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, dp_fill_k<NBITS, CI, VT>, DP_THREADS, Ls.bytes));
+    const unsigned g = unsigned(std::max(1, per_sm) * sms);
+    if(!h->VT) {
+      const size_t n4 = size_t(nn) * nn * nn * nn;
+      MB_CUDA(cudaMalloc(&h->VT, n4 * 8));
+      v_pair_transpose_k<<<grid_for(n4, 256, 8 * sms), 256, 0, s>>>(h->V, h->VT, nn), note_launch();
+    }
     cudaEventRecord(ev[0], s);
-    dp_fill_k<NBITS, CI, VT><<<g, HB_THREADS, 0, s>>>(
-        I, d, hdiag, rowptr64, colind, nzval, out->diag, rowcnt, thresh, r0,
-        int64_t(nbra)), note_launch();
+    dp_fill_k<NBITS, CI, VT><<<g, DP_THREADS, Ls.bytes, s>>>(
+        I, h->VT, d, Ls, hdiag, rowptr64, colind, nzval, out->diag, rowcnt, thresh,
+        r0, int64_t(nbra)), note_launch();
     cudaEventRecord(ev[1], s);
     MB_CUDA(cudaGetLastError());
   } else {
@@ -1049,8 +1354,12 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     VT* nz2 = nullptr;
     MB_CUDA(cudaMallocAsync(&ci2, std::max<int64_t>(nnz, 1) * sizeof(CI), s));
     MB_CUDA(cudaMallocAsync(&nz2, std::max<int64_t>(nnz, 1) * sizeof(VT), s));
-    compact_rows_k<CI, VT><<<grid_for(nbra * 32, 256, 16 * sms), 256, 0, s>>>(
-        rowptr64, newptr, nbra, colind, nzval, ci2, nz2), note_launch();
+    if(direct)
+      compact_marked_k<CI, VT><<<grid_for(nbra * 32, 256, 16 * sms), 256, 0, s>>>(
+          rowptr64, newptr, nbra, colind, nzval, ci2, nz2), note_launch();
+    else
+      compact_rows_k<CI, VT><<<grid_for(nbra * 32, 256, 16 * sms), 256, 0, s>>>(
+          rowptr64, newptr, nbra, colind, nzval, ci2, nz2), note_launch();
     cudaFreeAsync(colind, s);
     cudaFreeAsync(nzval, s);
     colind = ci2;

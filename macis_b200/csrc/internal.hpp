@@ -15,6 +15,10 @@ struct macis_b200_ham {
   // Device integrals + intermediates (column-major, compact leading dims).
   double *T = nullptr, *V = nullptr, *G = nullptr, *G_red = nullptr,
          *V_red = nullptr, *G2_red = nullptr, *V2_red = nullptr;
+  // V with the two index pairs swapped, VT[(p + q n) n^2 + (r + s n)] =
+  // V[(p + q n) + (r + s n) n^2]; built on first use by the direct-product
+  // fill so that one alpha pair's row of V is contiguous
+  double* VT = nullptr;
   macis_b200_asci_stats last_asci{};
   mb::Ints ints() const {
     return mb::Ints{norb, T, V, G, G_red, V_red, G2_red, V2_red};

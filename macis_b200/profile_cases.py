@@ -1,0 +1,84 @@
+"""Small, self-contained workloads for kernel profiling (ncu) and timing.
+
+    python -m macis_b200.profile_cases hbuild_c1   # CAS(10e,10o) CSR build
+    python -m macis_b200.profile_cases hbuild_c2   # CAS(12e,12o) CSR build
+    python -m macis_b200.profile_cases spmv_c1     # FP64 SpMV on CAS(10e,10o)
+    python -m macis_b200.profile_cases hbuild_sel  # selected (shuffled) space
+    python -m macis_b200.profile_cases asci_n48    # one ASCI search, n = 48
+
+Each case runs its hot call a few times (--reps) and prints one timing line.
+"""
+import argparse
+import time
+
+import numpy as np
+
+import macis_b200 as mb
+
+EPS = float(np.finfo(np.float64).eps)
+
+
+def fci(norb, k, nbits=64, seed=0):
+    T, V = mb.synthetic_integrals(norb, seed)
+    return T, V, mb.generate_hilbert_space(norb, k, k, nbits)
+
+
+def hbuild(norb, k, reps, shuffle=False):
+    T, V, dets = fci(norb, k)
+    if shuffle:
+        dets = dets[np.random.default_rng(1).permutation(len(dets))]
+    H = mb.HamiltonianGenerator(T, V, 64)
+    for _ in range(reps):
+        A = mb.make_csr_hamiltonian(dets, H, EPS)
+        st = A.build_stats()
+        print(f"build nnz={A.nnz} build_ms={st['build_ms']:.3f} "
+              f"fill_ms={st['fill_ms']:.3f} direct={st['direct_product']}")
+        del A
+
+
+def spmv(norb, k, reps):
+    T, V, dets = fci(norb, k)
+    H = mb.HamiltonianGenerator(T, V, 64)
+    A = mb.make_csr_hamiltonian(dets, H, EPS)
+    x = np.random.default_rng(0).standard_normal(A.n)
+    for _ in range(reps):
+        t = time.perf_counter()
+        A.spmv(x)
+        print(f"spmv host-staged {1e3 * (time.perf_counter() - t):.3f} ms")
+
+
+def asci_n48(reps, ncore=2000):
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "bench", os.path.join(os.path.dirname(os.path.dirname(
+            os.path.abspath(__file__))), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for _ in range(reps):
+        r = bench.asci_extra(mb, ncore=ncore, ndets_max=200000)
+        print(f"asci {r['seconds']:.3f} s raw={r['raw_pairs']} "
+              f"unique={r['unique_pairs']}")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case")
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args()
+    if a.case == "hbuild_c1":
+        hbuild(10, 5, a.reps)
+    elif a.case == "hbuild_c2":
+        hbuild(12, 6, a.reps)
+    elif a.case == "hbuild_sel":
+        hbuild(10, 5, a.reps, shuffle=True)
+    elif a.case == "spmv_c1":
+        spmv(10, 5, a.reps)
+    elif a.case == "asci_n48":
+        asci_n48(a.reps)
+    else:
+        raise SystemExit(f"unknown case {a.case}")
+
+
+if __name__ == "__main__":
+    main()

@@ -32,10 +32,15 @@ def test_water_cisd_exact(port, ref, wat):
 def test_fci_direct_product_exact(ref, nbits):
     T, V, dets = fci(8, 4, 3, nbits, seed=3)
     H = mb.HamiltonianGenerator(T, V, nbits)
-    A = mb.make_csr_hamiltonian(dets, H, np.finfo(float).eps)
-    r = ref.build_csr(ref.ham(nbits, 8, T, V), dets, dets,
-                      np.finfo(float).eps, nthreads=4)
-    assert_csr_equal(A.to_host(), r)
+    hr = ref.ham(nbits, 8, T, V)
+    for thr in (np.finfo(float).eps, 1e-3, 0.05):   # 0.05 drops many entries
+        A = mb.make_csr_hamiltonian(dets, H, thr)
+        assert A.build_stats()["direct_product"] == 1
+        assert_csr_equal(A.to_host(), ref.build_csr(hr, dets, dets, thr,
+                                                    nthreads=4))
+        A32 = mb.make_csr_hamiltonian(dets, H, thr, value_t=np.float32)
+        assert np.array_equal(A32.to_host()[1], A.to_host()[1])
+        assert np.array_equal(A32.diagonal(), A.diagonal())
 
 
 def test_c1_fci_exact(ref):
