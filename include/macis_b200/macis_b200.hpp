@@ -1,0 +1,318 @@
+// C++ drop-in for MACIS's selected-CI hot path on a B200 (header-only).
+//
+// Include after the MACIS headers. It keeps MACIS's own template API:
+//
+//   macis_b200::HamiltonianGenerator<N>   a macis::HamiltonianGenerator<N>
+//       whose virtual CSR hook (include/macis/hamiltonian_generator.hpp:
+//       66-72) builds on the GPU, so macis::make_csr_hamiltonian[_block]
+//       (include/macis/csr_hamiltonian.hpp:23-45) and everything above it
+//       use the GPU build unchanged
+//   macis_b200::SparseMatrixOperator       the H.X hook of macis::davidson
+//       (include/macis/solvers/davidson.hpp:29-59) over a device CSR
+//   macis_b200::selected_ci_diag           selected_ci_diag.hpp:125-206 with
+//       H kept in HBM (build + Davidson on the GPU)
+//   macis_b200::asci_search / asci_iter / asci_grow / asci_refine
+//       include/macis/asci/{determinant_search.hpp:395,iteration.hpp:17,
+//       grow.hpp:17,refine.hpp:15}; the reference drivers call asci_search
+//       and selected_ci_diag directly, so same-signature drivers are shipped
+//
+// Link with libmacis_b200.so (C ABI in macis_b200.h). MPI world size 1.
+#pragma once
+#include <macis_b200.h>
+
+#include <bitset>
+#include <cstring>
+#include <macis/asci/determinant_search.hpp>
+#include <macis/hamiltonian_generator.hpp>
+#include <macis/util/mcscf.hpp>
+#include <sparsexx/matrix_types/csr_matrix.hpp>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace macis_b200 {
+
+inline void check(int rc) {
+  if(rc != MACIS_B200_OK) throw std::runtime_error(macis_b200_last_error());
+}
+
+template <size_t N>
+inline const uint64_t* words(const std::bitset<N>* p) {
+  static_assert(sizeof(std::bitset<N>) == N / 8, "bitset word layout");
+  return reinterpret_cast<const uint64_t*>(p);
+}
+
+// Device CSR owned by the library.
+class DeviceCSR {
+  macis_b200_csr* A_ = nullptr;
+
+ public:
+  explicit DeviceCSR(macis_b200_csr* A) : A_(A) {}
+  DeviceCSR(const DeviceCSR&) = delete;
+  DeviceCSR(DeviceCSR&& o) noexcept : A_(o.A_) { o.A_ = nullptr; }
+  ~DeviceCSR() {
+    if(A_) macis_b200_csr_destroy(A_);
+  }
+  macis_b200_csr* get() const { return A_; }
+  int64_t m() const {
+    int64_t v;
+    check(macis_b200_csr_info(A_, &v, nullptr, nullptr, nullptr, nullptr));
+    return v;
+  }
+  int64_t nnz() const {
+    int64_t v;
+    check(macis_b200_csr_info(A_, nullptr, nullptr, &v, nullptr, nullptr));
+    return v;
+  }
+  std::vector<double> diagonal() const {
+    std::vector<double> d(m());
+    check(macis_b200_csr_diagonal(A_, d.data(), 0));
+    return d;
+  }
+  template <typename index_t>
+  sparsexx::csr_matrix<double, index_t> to_host() const {
+    int64_t m, n, nnz;
+    int ib, vb;
+    check(macis_b200_csr_info(A_, &m, &n, &nnz, &ib, &vb));
+    if(ib != int(sizeof(index_t)) || vb != 8)
+      throw std::runtime_error("Unsupported index_t");
+    std::vector<index_t> rp(m + 1), ci(nnz);
+    std::vector<double> nz(nnz);
+    check(macis_b200_csr_download(A_, rp.data(), ci.data(), nz.data(), 0));
+    return sparsexx::csr_matrix<double, index_t>(m, n, std::move(rp),
+                                                 std::move(ci), std::move(nz));
+  }
+};
+
+template <size_t N>
+class HamiltonianGenerator : public macis::HamiltonianGenerator<N> {
+  using base = macis::HamiltonianGenerator<N>;
+  macis_b200_ham* h_ = nullptr;
+
+ public:
+  using full_det_iterator = typename base::full_det_iterator;
+  using matrix_span_t = typename base::matrix_span_t;
+  using rank4_span_t = typename base::rank4_span_t;
+
+  HamiltonianGenerator(matrix_span_t T, rank4_span_t V) : base(T, V) {
+    check(macis_b200_ham_create(int(N), T.extent(0), T.data_handle(),
+                                T.extent(0), V.data_handle(), V.extent(0),
+                                &h_));
+  }
+  ~HamiltonianGenerator() noexcept override {
+    if(h_) macis_b200_ham_destroy(h_);
+  }
+  macis_b200_ham* handle() const { return h_; }
+
+  // Device-resident build (no download): the selected_ci_diag path.
+  DeviceCSR build_device(full_det_iterator bb, full_det_iterator be,
+                         full_det_iterator kb, full_det_iterator ke,
+                         double thresh, int idx_bytes = 4,
+                         int val_bytes = 8) {
+    const size_t nb = std::distance(bb, be), nk = std::distance(kb, ke);
+    macis_b200_csr* A = nullptr;
+    check(macis_b200_build_csr(h_, nb ? words<N>(&*bb) : nullptr, nb,
+                               nk ? words<N>(&*kb) : nullptr, nk, thresh,
+                               idx_bytes, val_bytes, 0, &A));
+    return DeviceCSR(A);
+  }
+
+  void form_rdms(full_det_iterator, full_det_iterator, full_det_iterator,
+                 full_det_iterator, double*, matrix_span_t,
+                 rank4_span_t) override {
+    throw std::logic_error(
+        "form_rdms is not part of the B200 path; use "
+        "macis::DoubleLoopHamiltonianGenerator for RDMs");
+  }
+
+ protected:
+  template <typename index_t>
+  sparsexx::csr_matrix<double, index_t> build_host(full_det_iterator bb,
+                                                   full_det_iterator be,
+                                                   full_det_iterator kb,
+                                                   full_det_iterator ke,
+                                                   double thresh) {
+    return build_device(bb, be, kb, ke, thresh, int(sizeof(index_t)))
+        .template to_host<index_t>();
+  }
+  sparsexx::csr_matrix<double, int32_t> make_csr_hamiltonian_block_32bit_(
+      full_det_iterator bb, full_det_iterator be, full_det_iterator kb,
+      full_det_iterator ke, double thresh) override {
+    return build_host<int32_t>(bb, be, kb, ke, thresh);
+  }
+  sparsexx::csr_matrix<double, int64_t> make_csr_hamiltonian_block_64bit_(
+      full_det_iterator bb, full_det_iterator be, full_det_iterator kb,
+      full_det_iterator ke, double thresh) override {
+    return build_host<int64_t>(bb, be, kb, ke, thresh);
+  }
+};
+
+// operator_action(m, alpha, V, LDV, beta, AV, LDAV) on host blocks.
+class SparseMatrixOperator {
+  const DeviceCSR& A_;
+
+ public:
+  explicit SparseMatrixOperator(const DeviceCSR& A) : A_(A) {}
+  void operator_action(size_t m, double alpha, const double* V, size_t LDV,
+                       double beta, double* AV, size_t LDAV) const {
+    check(macis_b200_spmv(A_.get(), int64_t(m), alpha, V, int64_t(LDV), beta,
+                          AV, int64_t(LDAV), 0));
+  }
+};
+
+// davidson(N, max_m, op, D, tol, X) for a device operator: the reference
+// signature; D is taken from the matrix. Throws "Davidson Did Not Converge!".
+inline std::pair<int64_t, double> davidson(int64_t, int64_t max_m,
+                                           const SparseMatrixOperator& op,
+                                           const DeviceCSR& A, double tol,
+                                           double* X, bool use_guess = true) {
+  double E = 0;
+  int64_t it = 0;
+  check(macis_b200_davidson(A.get(), max_m, tol, use_guess, X, &E, &it, 0));
+  (void)op;
+  return {it, E};
+}
+
+template <size_t N, typename index_t = int32_t>
+double selected_ci_diag(macis::wavefunction_iterator_t<N> dets_begin,
+                        macis::wavefunction_iterator_t<N> dets_end,
+                        HamiltonianGenerator<N>& ham_gen, double h_el_tol,
+                        size_t davidson_max_m, double davidson_res_tol,
+                        std::vector<double>& C_local,
+                        const bool /*quiet*/ = false) {
+  const size_t ndets = std::distance(dets_begin, dets_end);
+  DeviceCSR H = ham_gen.build_device(dets_begin, dets_end, dets_begin,
+                                     dets_end, h_el_tol, sizeof(index_t));
+  C_local.resize(ndets, 0);
+  double max_c = 0;
+  for(double c : C_local) max_c = std::max(max_c, std::abs(c));
+  const bool guess = ndets && max_c > 1. / ndets;  // selected_ci_diag.hpp:96
+  double E = 0;
+  int64_t it = 0;
+  check(macis_b200_davidson(H.get(), int64_t(davidson_max_m),
+                            davidson_res_tol, guess, C_local.data(), &E, &it,
+                            0));
+  return E;
+}
+
+inline macis_b200_asci_settings to_c(const macis::ASCISettings& s) {
+  macis_b200_asci_settings c{};
+  c.ntdets_max = s.ntdets_max;
+  c.ntdets_min = s.ntdets_min;
+  c.ncdets_max = s.ncdets_max;
+  c.h_el_tol = s.h_el_tol;
+  c.rv_prune_tol = s.rv_prune_tol;
+  c.pair_size_max = s.pair_size_max;
+  c.just_singles = s.just_singles;
+  c.grow_factor = s.grow_factor;
+  c.max_refine_iter = s.max_refine_iter;
+  c.refine_energy_tol = s.refine_energy_tol;
+  return c;
+}
+
+// asci_search with the reference signature (world size 1). The integral
+// pointers are accepted for signature compatibility; the generator's
+// device copies are used.
+template <size_t N>
+std::vector<macis::wfn_t<N>> asci_search(
+    macis::ASCISettings asci_settings, size_t ndets_max,
+    macis::wavefunction_iterator_t<N> cdets_begin,
+    macis::wavefunction_iterator_t<N> cdets_end, const double E_ASCI,
+    const std::vector<double>& C, size_t /*norb*/, const double* /*T_pq*/,
+    const double* /*G_red*/, const double* /*V_red*/,
+    const double* /*G_pqrs*/, const double* /*V_pqrs*/,
+    HamiltonianGenerator<N>& ham_gen) {
+  const size_t nc = std::distance(cdets_begin, cdets_end);
+  const auto s = to_c(asci_settings);
+  std::vector<macis::wfn_t<N>> out(ndets_max + nc);
+  size_t nout = 0;
+  check(macis_b200_asci_search(ham_gen.handle(), &s, ndets_max,
+                               nc ? words<N>(&*cdets_begin) : nullptr, nc,
+                               E_ASCI, C.data(),
+                               reinterpret_cast<uint64_t*>(out.data()), &nout,
+                               0));
+  out.resize(nout);
+  return out;
+}
+
+// asci_iter (include/macis/asci/iteration.hpp:17-68)
+template <size_t N, typename index_t = int32_t>
+auto asci_iter(macis::ASCISettings asci_settings,
+               macis::MCSCFSettings mcscf_settings, size_t ndets_max,
+               double E0, std::vector<macis::wfn_t<N>> wfn,
+               std::vector<double> X, HamiltonianGenerator<N>& ham_gen,
+               size_t norb) {
+  if(wfn.size() > 1) {  // reorder_ci_on_coeff, ties kept in order
+    std::vector<size_t> idx(X.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t i, size_t j) {
+      return std::abs(X[i]) > std::abs(X[j]);
+    });
+    std::vector<macis::wfn_t<N>> w2(wfn.size());
+    std::vector<double> x2(X.size());
+    for(size_t i = 0; i < idx.size(); ++i) {
+      w2[i] = wfn[idx[i]];
+      x2[i] = X[idx[i]];
+    }
+    wfn = std::move(w2);
+    X = std::move(x2);
+  }
+  const size_t nkeep = std::min(asci_settings.ncdets_max, wfn.size());
+  wfn = asci_search<N>(asci_settings, ndets_max, wfn.begin(),
+                       wfn.begin() + nkeep, E0, X, norb, nullptr, nullptr,
+                       nullptr, nullptr, nullptr, ham_gen);
+  std::vector<double> X_local;
+  const double E = selected_ci_diag<N, index_t>(
+      wfn.begin(), wfn.end(), ham_gen, mcscf_settings.ci_matel_tol,
+      mcscf_settings.ci_max_subspace, mcscf_settings.ci_res_tol, X_local);
+  return std::make_tuple(E, wfn, std::move(X_local));
+}
+
+// asci_grow (include/macis/asci/grow.hpp:17-171, without grow_with_rot)
+template <size_t N, typename index_t = int32_t>
+auto asci_grow(macis::ASCISettings asci_settings,
+               macis::MCSCFSettings mcscf_settings, double E0,
+               std::vector<macis::wfn_t<N>> wfn, std::vector<double> X,
+               HamiltonianGenerator<N>& ham_gen, size_t norb) {
+  if(asci_settings.grow_with_rot)
+    throw std::logic_error("grow_with_rot is not part of the B200 path");
+  while(wfn.size() < asci_settings.ntdets_max) {
+    const size_t ndets_new = std::min(
+        std::max(asci_settings.ntdets_min,
+                 wfn.size() * asci_settings.grow_factor),
+        asci_settings.ntdets_max);
+    double E;
+    std::tie(E, wfn, X) = asci_iter<N, index_t>(
+        asci_settings, mcscf_settings, ndets_new, E0, std::move(wfn),
+        std::move(X), ham_gen, norb);
+    if(ndets_new > wfn.size())
+      throw std::runtime_error("Wavefunction didn't grow enough...");
+    E0 = E;
+  }
+  return std::make_tuple(E0, wfn, X);
+}
+
+// asci_refine (include/macis/asci/refine.hpp:15-66)
+template <size_t N, typename index_t = int32_t>
+auto asci_refine(macis::ASCISettings asci_settings,
+                 macis::MCSCFSettings mcscf_settings, double E0,
+                 std::vector<macis::wfn_t<N>> wfn, std::vector<double> X,
+                 HamiltonianGenerator<N>& ham_gen, size_t norb) {
+  const size_t ndets = wfn.size();
+  for(size_t iter = 0; iter < asci_settings.max_refine_iter; ++iter) {
+    double E;
+    std::tie(E, wfn, X) =
+        asci_iter<N, index_t>(asci_settings, mcscf_settings, ndets, E0,
+                              std::move(wfn), std::move(X), ham_gen, norb);
+    if(wfn.size() != ndets)
+      throw std::runtime_error("Wavefunction size can't change in refinement");
+    const double dE = E - E0;
+    E0 = E;
+    if(std::abs(dE) < asci_settings.refine_energy_tol)
+      return std::make_tuple(E0, wfn, X);
+  }
+  throw std::runtime_error("ACCI Refine did not converge");
+}
+
+}  // namespace macis_b200

@@ -1,0 +1,77 @@
+// Drop-in check (test infrastructure): the reference's own templates run
+// with the B200 generator plugged into the HamiltonianGenerator virtual hook
+// (include/macis/hamiltonian_generator.hpp:66-72), compared with the
+// reference DoubleLoopHamiltonianGenerator on the same inputs.
+//
+//   dropin_check T.bin V.bin norb nalpha nbeta ntdets_max
+//
+// T.bin / V.bin are raw column-major float64 integrals. Prints one JSON line.
+#include <spdlog/sinks/null_sink.h>
+#include <spdlog/spdlog.h>
+
+#include <cstdio>
+#include <fstream>
+#include <macis/asci/grow.hpp>
+#include <macis/csr_hamiltonian.hpp>
+#include <macis/hamiltonian_generator/double_loop.hpp>
+#include <macis/solvers/selected_ci_diag.hpp>
+#include <macis_b200/macis_b200.hpp>
+
+static std::vector<double> load(const char* f, size_t n) {
+  std::vector<double> v(n);
+  std::ifstream in(f, std::ios::binary);
+  in.read(reinterpret_cast<char*>(v.data()), n * 8);
+  if(!in) throw std::runtime_error(std::string("cannot read ") + f);
+  return v;
+}
+
+int main(int argc, char** argv) {
+  if(argc < 7) return 2;
+  for(const char* n : {"davidson", "ci_solver", "asci_search", "asci_grow",
+                       "asci_refine"})
+    spdlog::null_logger_mt(n);
+  const size_t norb = std::stoul(argv[3]), na = std::stoul(argv[4]),
+               nb = std::stoul(argv[5]), ntdets = std::stoul(argv[6]);
+  auto T = load(argv[1], norb * norb);
+  auto V = load(argv[2], norb * norb * norb * norb);
+  macis::matrix_span<double> Ts(T.data(), norb, norb);
+  macis::rank4_span<double> Vs(V.data(), norb, norb, norb, norb);
+  macis::DoubleLoopHamiltonianGenerator<64> cpu(Ts, Vs);
+  macis_b200::HamiltonianGenerator<64> gpu(Ts, Vs);
+
+  auto hf = macis::canonical_hf_determinant<64>(na, nb);
+  auto dets = macis::generate_cisd_hilbert_space<64>(norb, hf);
+  // 1. the reference free function through the virtual hook
+  auto Hc = macis::make_csr_hamiltonian<int32_t>(dets.begin(), dets.end(),
+                                                 cpu, 1e-16);
+  auto Hg = macis::make_csr_hamiltonian<int32_t>(dets.begin(), dets.end(),
+                                                 gpu, 1e-16);
+  const bool csr_equal = Hc.rowptr() == Hg.rowptr() &&
+                         Hc.colind() == Hg.colind() && Hc.nzval() == Hg.nzval();
+  // 2. the reference selected_ci_diag on both generators (CPU Davidson),
+  //    and the shim's GPU-resident selected_ci_diag
+  std::vector<double> C1, C2, C3;
+  const double e_cpu = macis::selected_ci_diag<64, int32_t>(
+      dets.begin(), dets.end(), cpu, 1e-16, 15, 1e-8, C1);
+  const double e_hook = macis::selected_ci_diag<64, int32_t>(
+      dets.begin(), dets.end(), gpu, 1e-16, 15, 1e-8, C2);
+  const double e_gpu = macis_b200::selected_ci_diag<64, int32_t>(
+      dets.begin(), dets.end(), gpu, 1e-16, 15, 1e-8, C3);
+  // 3. ASCI grow with the shim drivers
+  macis::ASCISettings as;
+  as.ntdets_max = ntdets;
+  macis::MCSCFSettings ms;
+  std::vector<macis::wfn_t<64>> w = {hf};
+  std::vector<double> X = {1.0};
+  double E0 = gpu.matrix_element(hf, hf);
+  std::tie(E0, w, X) = macis_b200::asci_grow<64>(as, ms, E0, w, X, gpu, norb);
+  double nrm = 0;
+  for(double x : X) nrm += x * x;
+  std::printf(
+      "{\"ndets\": %zu, \"nnz\": %ld, \"csr_equal\": %s, \"e_cpu\": %.15g, "
+      "\"e_hook\": %.15g, \"e_gpu\": %.15g, \"asci_e0\": %.15g, "
+      "\"asci_size\": %zu, \"asci_norm\": %.15g}\n",
+      dets.size(), long(Hg.nnz()), csr_equal ? "true" : "false", e_cpu,
+      e_hook, e_gpu, E0, w.size(), nrm);
+  return 0;
+}

@@ -1,0 +1,34 @@
+"""C++ drop-in: the reference's own make_csr_hamiltonian / selected_ci_diag
+templates with the B200 generator in the HamiltonianGenerator virtual hook,
+compiled against the unmodified reference headers (oracle/ref/dropin_check.cpp,
+built into oracle/_ref by oracle/ref/Makefile)."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from golden_data import constants, water
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "oracle", "_ref", "dropin_check")
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="dropin_check not built")
+def test_reference_templates_with_b200_generator(tmp_path):
+    norb, T, V, _ = water()
+    K = constants()
+    (tmp_path / "T.bin").write_bytes(np.ascontiguousarray(T).tobytes())
+    (tmp_path / "V.bin").write_bytes(np.ascontiguousarray(V).tobytes())
+    out = subprocess.run([EXE, str(tmp_path / "T.bin"), str(tmp_path / "V.bin"),
+                          str(norb), "5", "5", "10000"], capture_output=True,
+                         text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    assert r["ndets"] == 12636 and r["csr_equal"]
+    assert r["e_cpu"] == r["e_hook"]           # identical CSR -> same Davidson
+    assert abs(r["e_gpu"] - r["e_cpu"]) < 1e-8
+    assert r["asci_size"] == 10000 and abs(r["asci_norm"] - 1) < 1e-10
+    assert abs(r["asci_e0"] - K["water_asci_grow_e0"]) < 1e-8
