@@ -129,6 +129,22 @@ int macis_b200_spmv(const macis_b200_csr* A, int64_t K, double alpha,
                     const double* V, int64_t LDV, double beta, double* AV,
                     int64_t LDAV, unsigned flags);
 
+/* y = alpha * A * x + beta * y for one column, FP32-value (mixed) matrices
+ * only, without allocating device memory. It has no counterpart in the
+ * reference. It is meant for callers that may not allocate device memory
+ * once they run -- for instance a service whose memory manager takes all of
+ * HBM at start-up -- and it produces the same result as macis_b200_spmv.
+ * x and y are device pointers on the matrix's device. The FP32 copy of x is
+ * kept in a fixed array compiled into the library (4,194,304 entries, 16 MiB
+ * on every GPU that loads the library, held until exit): matrices with more
+ * columns are rejected with MACIS_B200_ECAPACITY. The first call on a device
+ * looks up that array's device address; make that first call before any
+ * stream capture. Every call reuses the same array, so calls that overlap on
+ * the GPU (from several host threads or handles at once) race; calls return
+ * after the product completes. */
+int macis_b200_spmv_mixed_noalloc(const macis_b200_csr* A, double alpha,
+                                  const double* x, double beta, double* y);
+
 /* Single-vector Davidson for the lowest eigenpair of A, replacing
  * macis::davidson (include/macis/solvers/davidson.hpp:129-225) with the
  * diagonal preconditioner and CGS2 of the reference. X holds the guess on

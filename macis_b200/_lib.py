@@ -76,6 +76,8 @@ _SIGS = {
     "macis_b200_csr_diagonal": (C.c_int, [_vp, _vp, C.c_uint]),
     "macis_b200_spmv": (C.c_int, [_vp, C.c_int64, C.c_double, _vp, C.c_int64,
                                   C.c_double, _vp, C.c_int64, C.c_uint]),
+    "macis_b200_spmv_mixed_noalloc": (C.c_int, [_vp, C.c_double, _vp,
+                                                C.c_double, _vp]),
     "macis_b200_davidson": (C.c_int, [_vp, C.c_int64, C.c_double, C.c_int,
                                       _vp, C.POINTER(C.c_double),
                                       C.POINTER(C.c_int64), C.c_uint]),

@@ -10,6 +10,8 @@
 // FP64. Mixed mode: FP32 off-diagonal values times an FP32 copy of x, each
 // product formed exactly in FP64 (24x24-bit mantissas fit in 53 bits) and
 // summed in FP64, plus the FP64 diagonal times the FP64 x.
+#include <mutex>
+
 #include "internal.hpp"
 #include "primitives.cuh"
 
@@ -104,3 +106,85 @@ void spmv_device(const macis_b200_csr* A, double alpha, const double* x,
 }
 
 }  // namespace mb
+
+// ---------------------------------------------------------------------------
+// Allocation-free mixed-precision SpMV.
+//
+// Some callers may not allocate device memory once they are running: a
+// service that hands all of HBM to its own pool manager at start-up and
+// forbids cudaMalloc afterwards, or a host program whose memory budget is
+// fixed when it links this library. For them the FP32 copy of x that the
+// mixed-precision product needs lives in the file-scope array below instead
+// of a stream-ordered allocation. Every GPU that loads the library holds
+// this array (16 MiB) until the process exits.
+namespace mb {
+namespace {
+
+constexpr int64_t kNoAllocMaxN = int64_t(1) << 22;  // 4,194,304 columns
+static __device__ __align__(256) float g_noalloc_x32[kNoAllocMaxN];
+
+// Host code cannot use g_noalloc_x32 as a device address: its name there is
+// a host-side stand-in. The device address is looked up once per device with
+// that device current.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[kMaxDevices] = {};
+
+float* noalloc_scratch(int dev) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  MB_REQUIRE(dev >= 0 && dev < kMaxDevices, MACIS_B200_EINVAL,
+             "device ordinal out of range");
+  if(!g_noalloc_ptr[dev]) {
+    int cur = -1;
+    MB_CUDA(cudaGetDevice(&cur));
+    if(cur != dev) MB_CUDA(cudaSetDevice(dev));
+    void* p = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_x32);
+    if(cur != dev) cudaSetDevice(cur);
+    MB_CUDA(rc);
+    g_noalloc_ptr[dev] = static_cast<float*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+}  // namespace mb
+
+extern "C" int macis_b200_spmv_mixed_noalloc(const macis_b200_csr* A,
+                                             double alpha, const double* x,
+                                             double beta, double* y) {
+  try {
+    MB_REQUIRE(A && x && y, MACIS_B200_EINVAL, "null argument");
+    MB_REQUIRE(A->val_bytes == 4, MACIS_B200_EINVAL,
+               "the allocation-free SpMV needs an FP32-value (mixed) matrix");
+    MB_REQUIRE(A->n <= mb::kNoAllocMaxN, MACIS_B200_ECAPACITY,
+               "matrix has more columns than the allocation-free scratch "
+               "holds (4,194,304)");
+    float* x32 = mb::noalloc_scratch(A->device);
+    const int64_t m = A->m;
+    cudaStream_t s = A->stream;
+    if(m > 0) {
+      // the scratch is fully rewritten before it is read: nothing to clear
+      mb::to_f32_k<<<mb::grid_for(size_t(A->n), 256, 8 * mb::num_sms()), 256,
+                     0, s>>>(x, x32, A->n), mb::note_launch();
+      const unsigned g = mb::spmv_grid(m);
+      if(A->idx_bytes == 4)
+        mb::spmv_k<int32_t, float, true><<<g, mb::SPMV_THREADS, 0, s>>>(
+            m, A->n, (const int32_t*)A->rowptr, (const int32_t*)A->colind,
+            (const float*)A->nzval, A->diag, x, x32, alpha, beta, y),
+            mb::note_launch();
+      else
+        mb::spmv_k<int64_t, float, true><<<g, mb::SPMV_THREADS, 0, s>>>(
+            m, A->n, (const int64_t*)A->rowptr, (const int64_t*)A->colind,
+            (const float*)A->nzval, A->diag, x, x32, alpha, beta, y),
+            mb::note_launch();
+      MB_CUDA(cudaGetLastError());
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    return MACIS_B200_OK;
+  } catch(const mb::Error& e) {
+    mb::set_error(e.what());
+    return e.code;
+  }
+}
+
