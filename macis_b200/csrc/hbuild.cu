@@ -88,11 +88,27 @@ __global__ void split_spins_k(const uint64_t* dets, size_t n, uint64_t* a,
 template <int NBITS>
 __global__ void first_alpha_change_k(const uint64_t* dets, size_t n,
                                      unsigned long long* first) {
+  // block-wide minimum first, one atomic per block
   using D = DetTraits<NBITS>;
+  __shared__ unsigned long long wmin[32];
   const auto a0 = D::alpha(dets);
+  unsigned long long best = ~0ull;
   for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
       i += size_t(gridDim.x) * blockDim.x)
-    if(!(D::alpha(dets + i * D::NW) == a0)) atomicMin(first, (unsigned long long)i);
+    if(!(D::alpha(dets + i * D::NW) == a0)) {
+      best = i;
+      break;  // later i of this thread are larger
+    }
+  for(int o = 16; o; o >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, best, o);
+    best = y < best ? y : best;
+  }
+  if((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    for(int w = 1; w < int(blockDim.x >> 5); ++w) best = wmin[w] < best ? wmin[w] : best;
+    if(best != ~0ull) atomicMin(first, best);
+  }
 }
 
 // Flags any determinant that breaks the (A = i/UB, B = i%UB) product layout,
