@@ -70,7 +70,34 @@ typedef struct {
   uint64_t kept_pairs;    /* after dropping core dets and zero scores */
   uint64_t batches;       /* core-det batches used */
   double pairs_ms, sort_ms, keep_ms, topk_ms, total_ms;
+  uint64_t units_total;   /* work units of the search (see asci_screen) */
+  uint64_t units_kept;    /* units scored exactly */
+  uint64_t samples;       /* training samples recorded into the network */
+  double screen_ms;       /* prediction + selection + recording */
 } macis_b200_asci_stats;
+
+/* Learned screening (no MACIS counterpart). A "unit" of the ASCI search is
+ * one core determinant with one excitation class and, for doubles, one outer
+ * (occupied, virtual) pair: the singles of a spin, or the inner loop of
+ * append_ss_doubles / append_os_doubles_asci_contributions
+ * (determinant_contributions.hpp:68-160) for fixed (i, a). The network
+ * predicts each unit's largest log |score|; with use_net the search scores
+ * exactly only the top keep_frac of the units (plus a random explore_frac)
+ * and drops the rest before any contribution is generated. With
+ * max_samples > 0 the search records up to that many (unit input, exact
+ * target) pairs of the units it scored into the network, for
+ * macis_b200_mlp_train with X == NULL. Target = (ln max|rv| + 20) / 5 with
+ * max|rv| floored at 1e-12. */
+typedef struct macis_b200_mlp macis_b200_mlp;
+typedef struct {
+  macis_b200_mlp* net;   /* may be NULL: exact search, nothing recorded */
+  int32_t use_net;       /* 1: prune units by prediction */
+  int32_t pad_;
+  double keep_frac;      /* fraction of units kept by prediction, (0, 1] */
+  double explore_frac;   /* extra random fraction kept, [0, 1] */
+  uint64_t max_samples;  /* samples recorded (0: none) */
+  uint64_t seed;
+} macis_b200_asci_screen;
 
 const char* macis_b200_last_error(void);
 int macis_b200_version(void);
@@ -216,6 +243,55 @@ int macis_b200_asci_pairs(macis_b200_ham* h, const macis_b200_asci_settings* s,
                           size_t* npairs);
 int macis_b200_asci_last_stats(const macis_b200_ham* h,
                                macis_b200_asci_stats* out);
+
+/* --- Learned screening network (no MACIS counterpart) ---------------------
+ * din -> 256 -> 256 -> 1 with GELU, BF16 tcgen05 GEMMs with FP32
+ * accumulation, FP32 master weights and Adam. Parameters are one FP32 array:
+ * W1 [256][din] row-major, b1 [256], W2 [256][256], b2 [256], w3 [256],
+ * b3 [1]. BF16 inputs are passed as their uint16 bit patterns. */
+int macis_b200_mlp_create(int din, uint64_t seed, macis_b200_mlp** out);
+int macis_b200_mlp_destroy(macis_b200_mlp* m);
+int macis_b200_mlp_num_params(const macis_b200_mlp* m, size_t* n);
+int macis_b200_mlp_get_params(const macis_b200_mlp* m, float* P);
+/* Sets the master weights and resets the Adam state. */
+int macis_b200_mlp_set_params(macis_b200_mlp* m, const float* P);
+/* y[i] = network(X[i]) for X [n][din]. */
+int macis_b200_mlp_forward(macis_b200_mlp* m, const uint16_t* X, size_t n,
+                           float* y, unsigned flags);
+/* Gradient of L = sum_i (y_i - t_i)^2 / (2 n) over all n rows (host grad,
+ * num_params floats); *loss = L. No update. */
+int macis_b200_mlp_gradients(macis_b200_mlp* m, const uint16_t* X,
+                             const float* t, size_t n, float* grad,
+                             double* loss, unsigned flags);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) over shuffled minibatches; X == NULL
+ * trains on the samples the last screened search recorded. *loss = mean
+ * loss of the last epoch (may be NULL). */
+int macis_b200_mlp_train(macis_b200_mlp* m, const uint16_t* X, const float* t,
+                         size_t n, int epochs, int batch, double lr,
+                         uint64_t seed, double* loss, unsigned flags);
+/* Raise the recorded targets below their q-quantile to that value (the
+ * ranking below it does not matter to a search that keeps the top units);
+ * *floor = the value (may be NULL). */
+int macis_b200_mlp_clamp_samples(macis_b200_mlp* m, double q, float* floor);
+/* Recorded samples (host copies; X may be NULL to query *n). */
+int macis_b200_mlp_samples(const macis_b200_mlp* m, size_t* n, uint16_t* X,
+                           float* t);
+/* Network input width of the ASCI units of nbits-wide determinants. */
+int macis_b200_asci_unit_width(int nbits);
+/* macis_b200_asci_search with learned screening / sample recording. */
+int macis_b200_asci_search_screened(macis_b200_ham* h,
+                                    const macis_b200_asci_settings* s,
+                                    const macis_b200_asci_screen* scr,
+                                    size_t ndets_max, const uint64_t* cdets,
+                                    size_t ncdets, double E0, const double* C,
+                                    uint64_t* out_dets, size_t* nout,
+                                    unsigned flags);
+/* Network input rows of units [first, first + n) of the search over the
+ * core dets (X [n][width], host); *nunits = the search's unit count. */
+int macis_b200_asci_unit_features(macis_b200_ham* h, const uint64_t* cdets,
+                                  size_t ncdets, double E0, const double* C,
+                                  size_t first, size_t n, uint16_t* X,
+                                  size_t* nunits);
 
 #ifdef __cplusplus
 }

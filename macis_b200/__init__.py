@@ -9,6 +9,9 @@ as the host side mirroring MACIS's own API:
     ASCISettings, MCSCFSettings, asci_search, asci_iter, asci_grow,
     asci_refine
 
+plus the learned screening of the ASCI search (ScreeningNetwork,
+ScreenSettings), which has no MACIS counterpart.
+
 Importing the package loads the native library and fails if it is missing.
 """
 from ._lib import MacisError  # noqa: F401  (loads libmacis_b200.so)
@@ -19,6 +22,8 @@ from .hamiltonian import (DeviceCSR, HamiltonianGenerator,  # noqa: F401
                           make_csr_hamiltonian, make_csr_hamiltonian_block,
                           row_bounds)
 from .integrals import fcidump_fill, synthetic_integrals  # noqa: F401
+from .screening import (ScreeningNetwork, ScreenSettings,  # noqa: F401
+                        unit_features, unit_width)
 from .sd import (canonical_hf_determinant, from_canonical_string,  # noqa
                  generate_cisd_hilbert_space, generate_hilbert_space,
                  to_canonical_string)

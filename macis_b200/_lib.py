@@ -34,7 +34,16 @@ class AsciStatsC(C.Structure):
                 ("kept_pairs", C.c_uint64), ("batches", C.c_uint64),
                 ("pairs_ms", C.c_double), ("sort_ms", C.c_double),
                 ("keep_ms", C.c_double), ("topk_ms", C.c_double),
-                ("total_ms", C.c_double)]
+                ("total_ms", C.c_double), ("units_total", C.c_uint64),
+                ("units_kept", C.c_uint64), ("samples", C.c_uint64),
+                ("screen_ms", C.c_double)]
+
+
+class AsciScreenC(C.Structure):
+    _fields_ = [("net", C.c_void_p), ("use_net", C.c_int32),
+                ("pad_", C.c_int32), ("keep_frac", C.c_double),
+                ("explore_frac", C.c_double), ("max_samples", C.c_uint64),
+                ("seed", C.c_uint64)]
 
 
 class DavidsonOptsC(C.Structure):
@@ -93,6 +102,27 @@ _SIGS = {
                                         _sz, C.c_double, _vp, _vp, _vp,
                                         C.POINTER(_sz)]),
     "macis_b200_asci_last_stats": (C.c_int, [_vp, C.POINTER(AsciStatsC)]),
+    "macis_b200_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    "macis_b200_mlp_destroy": (C.c_int, [_vp]),
+    "macis_b200_mlp_num_params": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "macis_b200_mlp_get_params": (C.c_int, [_vp, _vp]),
+    "macis_b200_mlp_set_params": (C.c_int, [_vp, _vp]),
+    "macis_b200_mlp_forward": (C.c_int, [_vp, _vp, _sz, _vp, C.c_uint]),
+    "macis_b200_mlp_gradients": (C.c_int, [_vp, _vp, _vp, _sz, _vp,
+                                           C.POINTER(C.c_double), C.c_uint]),
+    "macis_b200_mlp_train": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, C.c_int,
+                                       C.c_double, C.c_uint64,
+                                       C.POINTER(C.c_double), C.c_uint]),
+    "macis_b200_mlp_samples": (C.c_int, [_vp, C.POINTER(_sz), _vp, _vp]),
+    "macis_b200_mlp_clamp_samples": (C.c_int, [_vp, C.c_double,
+                                               C.POINTER(C.c_float)]),
+    "macis_b200_asci_unit_width": (C.c_int, [C.c_int]),
+    "macis_b200_asci_search_screened": (C.c_int, [
+        _vp, C.POINTER(AsciSettingsC), C.POINTER(AsciScreenC), _sz, _vp, _sz,
+        C.c_double, _vp, _vp, C.POINTER(_sz), C.c_uint]),
+    "macis_b200_asci_unit_features": (C.c_int, [_vp, _vp, _sz, C.c_double, _vp,
+                                                _sz, _sz, _vp,
+                                                C.POINTER(_sz)]),
 }
 
 EXPORTS = tuple(_SIGS)

@@ -75,9 +75,14 @@ def _dets(d, nbits):
     return np.ascontiguousarray(d, dtype=np.uint64).reshape(-1, nbits // 64)
 
 
-def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen):
+def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen,
+                screen=None, use_net=False):
     """New determinant list: top-(ndets_max - ncdets) contributions then the
-    core determinants (determinant_search.hpp:395-663)."""
+    core determinants (determinant_search.hpp:395-663).
+
+    screen: optional ScreenSettings (macis_b200.screening). Its network
+    records (unit input, exact log score) samples of the units this search
+    scores; with use_net it also prunes units by prediction first."""
     log = logging.getLogger("asci_search")
     cdets = _dets(cdets, ham_gen.nbits)
     C = np.ascontiguousarray(C, dtype=np.float64)[:len(cdets)]
@@ -85,10 +90,19 @@ def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen):
     out = np.empty((int(ndets_max) + len(cdets), ham_gen.nbits // 64),
                    dtype=np.uint64)
     nout = ct.c_size_t()
-    check(LIB.macis_b200_asci_search(ham_gen.handle, ct.byref(s),
-                                     int(ndets_max), cdets.ctypes.data,
-                                     len(cdets), float(E_ASCI), C.ctypes.data,
-                                     out.ctypes.data, ct.byref(nout), 0))
+    if screen is not None and screen.network is not None:
+        sc = screen.c_struct(use_net)
+        check(LIB.macis_b200_asci_search_screened(
+            ham_gen.handle, ct.byref(s), ct.byref(sc), int(ndets_max),
+            cdets.ctypes.data, len(cdets), float(E_ASCI), C.ctypes.data,
+            out.ctypes.data, ct.byref(nout), 0))
+        screen.searches += 1
+    else:
+        check(LIB.macis_b200_asci_search(ham_gen.handle, ct.byref(s),
+                                         int(ndets_max), cdets.ctypes.data,
+                                         len(cdets), float(E_ASCI),
+                                         C.ctypes.data, out.ctypes.data,
+                                         ct.byref(nout), 0))
     st = last_search_stats(ham_gen)
     log.info("  * ASCI Kept %d Pairs; %d unique; PAIR_DUR = %.2e s, "
              "SORT_ACC_DUR = %.2e s, ASCI_SEARCH DUR = %.2e s",
@@ -123,19 +137,45 @@ def last_search_stats(ham_gen):
     return {k: getattr(st, k) for k, _ in st._fields_}
 
 
+def _screened(screen):
+    """Whether the next search prunes by prediction."""
+    return (screen is not None and screen.network is not None and
+            screen.network.trained_steps > 0 and
+            screen.searches >= screen.warmup_searches)
+
+
 def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
-              norb):
+              norb, screen=None):
     """One ASCI iteration: reorder, search on the ncdets_max largest, then
-    rediagonalise without guess reuse (iteration.hpp:17-68)."""
+    rediagonalise without guess reuse (iteration.hpp:17-68). With a
+    ScreenSettings the search records samples / prunes units and the
+    network is retrained on the recorded samples afterwards."""
     wfn = _dets(wfn, ham_gen.nbits)
     X = np.asarray(X, dtype=np.float64)
     if len(wfn) > 1:
         wfn, X = reorder_ci_on_coeff(wfn, X)
     nkeep = min(int(asci_settings.ncdets_max), len(wfn))
     t0 = time.perf_counter()
+    use_net = _screened(screen)
+    if use_net and screen.min_units:
+        # small searches run exact: the network cannot save time there
+        from .screening import unit_features
+        _, nunits = unit_features(ham_gen, wfn[:nkeep], E0, X[:nkeep], 0, 0)
+        use_net = nunits >= screen.min_units
     wfn = asci_search(asci_settings, ndets_max, wfn[:nkeep], E0, X[:nkeep],
-                      norb, ham_gen)
+                      norb, ham_gen, screen=screen, use_net=use_net)
+    st = last_search_stats(ham_gen)
     t1 = time.perf_counter()
+    train_ms = 0.0
+    if screen is not None and screen.network is not None and screen.train \
+            and st["samples"] > 0:
+        tt = time.perf_counter()
+        if screen.clamp_quantile:
+            screen.network.clamp_samples(screen.clamp_quantile)
+        screen.network.train(None, None, screen.epochs, screen.batch,
+                             screen.lr, screen.seed + screen.searches)
+        train_ms = (time.perf_counter() - tt) * 1e3
+    t1b = time.perf_counter()
     tim = {}
     E, X = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,
                             mcscf_settings.ci_max_subspace,
@@ -145,12 +185,15 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
                             max_iter=mcscf_settings.davidson_max_iter)
     t2 = time.perf_counter()
     mcscf_settings.iteration_log.append(dict(
-        ndets=len(wfn), E=E, search_ms=(t1 - t0) * 1e3,
-        diag_ms=(t2 - t1) * 1e3, **tim))
+        ndets=len(wfn), E=E, search_ms=(t1 - t0) * 1e3, train_ms=train_ms,
+        diag_ms=(t2 - t1b) * 1e3, screened=bool(use_net),
+        units_total=st["units_total"], units_kept=st["units_kept"],
+        raw_pairs=st["raw_pairs"], **tim))
     return E, wfn, X
 
 
-def asci_grow(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb):
+def asci_grow(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb,
+              screen=None):
     log = logging.getLogger("asci_grow")
     wfn = _dets(wfn, ham_gen.nbits)
     if asci_settings.grow_with_rot:
@@ -161,7 +204,7 @@ def asci_grow(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb):
                             len(wfn) * asci_settings.grow_factor),
                         asci_settings.ntdets_max)
         E, wfn, X = asci_iter(asci_settings, mcscf_settings, ndets_new, E0,
-                              wfn, X, ham_gen, norb)
+                              wfn, X, ham_gen, norb, screen)
         if ndets_new > len(wfn):
             raise RuntimeError("Wavefunction didn't grow enough...")
         log.info("iter = %4d, E0 = %20.12e, dE = %14.6e, WFN_SIZE = %d", it, E,
@@ -171,12 +214,13 @@ def asci_grow(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb):
     return E0, wfn, X
 
 
-def asci_refine(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb):
+def asci_refine(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb,
+                screen=None):
     log = logging.getLogger("asci_refine")
     ndets = len(wfn)
     for it in range(asci_settings.max_refine_iter):
         E, wfn, X = asci_iter(asci_settings, mcscf_settings, ndets, E0, wfn, X,
-                              ham_gen, norb)
+                              ham_gen, norb, screen)
         if len(wfn) != ndets:
             raise RuntimeError("Wavefunction size can't change in refinement")
         dE = E - E0

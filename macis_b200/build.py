@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmacis_b200.so")
-SOURCES = ["ham.cu", "hbuild.cu", "spmv.cu", "davidson.cu", "asci.cu",
+SOURCES = ["ham.cu", "hbuild.cu", "spmv.cu", "davidson.cu", "asci.cu", "mlp.cu",
            "capi.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -23,6 +23,7 @@
 #include <cstdlib>
 
 #include "internal.hpp"
+#include "mlp.cuh"
 #include "primitives.cuh"
 
 namespace mb {
@@ -40,7 +41,33 @@ struct CoreData {
   double* eps;    // ncdets x 2 x n
   double* hd;     // ncdets
   int64_t* uoff;  // ncdets+1 unit offsets
+  const double* pairmax;  // 2 n^2 outer-pair integral bounds (screening)
 };
+
+// Outer-pair integral bounds (macis_b200_ham::pairmax). G rows are
+// contiguous (warp per pair); V is read with one thread per pair so that a
+// warp's loads are consecutive.
+__global__ void pairmax_g_k(const double* G, int n, double* out) {
+  const int lane = threadIdx.x & 31;
+  const size_t n2 = size_t(n) * n;
+  for(size_t p = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      p < n2; p += size_t(gridDim.x) * (blockDim.x >> 5)) {
+    double m = 0.0;
+    for(size_t q = lane; q < n2; q += 32) m = fmax(m, fabs(G[p * n2 + q]));
+    for(int o = 16; o > 0; o >>= 1)
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if(lane == 0) out[p] = m;
+  }
+}
+__global__ void pairmax_v_k(const double* V, int n, double* out) {
+  const size_t n2 = size_t(n) * n;
+  for(size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n2;
+      p += size_t(gridDim.x) * blockDim.x) {
+    double m = 0.0;
+    for(size_t q = 0; q < n2; ++q) m = fmax(m, fabs(V[p + q * n2]));
+    out[p] = m;
+  }
+}
 
 // Per core det precompute; one warp per det (bitset_to_occ_vir,
 // sd_operations.hpp:82-97; single_orbital_ens; matrix_element diag).
@@ -117,11 +144,49 @@ __device__ __forceinline__ void det_flip(uint64_t* d, int spin, int orb) {
 #define G2R(p, q) __ldg(I.G2_red + (p) + size_t(q) * n)
 #define V2R(p, q) __ldg(I.V2_red + (p) + size_t(q) * n)
 
+// A unit of core det c: t = 0 / 1 alpha / beta singles; then the (ii, aa)
+// outer pairs of the same-spin alpha doubles, of the same-spin beta doubles
+// and of the opposite-spin doubles (alpha outer, beta inner).
+struct UnitDesc {
+  int kind, ii, aa;
+  int64_t ninner;
+};
+__device__ __forceinline__ UnitDesc decode_unit(int nA, int nB, int nvA,
+                                                int nvB, int64_t t) {
+  UnitDesc d{0, 0, 0, 0};
+  if(t == 0) {
+    d.kind = 0;
+    d.ninner = int64_t(nA) * nvA;
+  } else if(t == 1) {
+    d.kind = 1;
+    d.ninner = int64_t(nB) * nvB;
+  } else if(t < 2 + int64_t(nA) * nvA) {
+    d.kind = 2;
+    d.ii = int((t - 2) / nvA);
+    d.aa = int((t - 2) % nvA);
+    d.ninner = int64_t(nA - 1 - d.ii) * (nvA - 1 - d.aa);
+  } else if(t < 2 + int64_t(nA) * nvA + int64_t(nB) * nvB) {
+    d.kind = 3;
+    const int64_t u = t - 2 - int64_t(nA) * nvA;
+    d.ii = int(u / nvB);
+    d.aa = int(u % nvB);
+    d.ninner = int64_t(nB - 1 - d.ii) * (nvB - 1 - d.aa);
+  } else {
+    d.kind = 4;
+    const int64_t u = t - 2 - int64_t(nA) * nvA - int64_t(nB) * nvB;
+    d.ii = int(u / nvA);
+    d.aa = int(u % nvA);
+    d.ninner = int64_t(nB) * nvB;
+  }
+  return d;
+}
+
 // One unit of contributions; MODE 0 counts, MODE 1 writes. Warp-synchronous.
 template <int NBITS, int MODE>
 __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                          double E0, double tol, int64_t* count_out,
-                         int64_t out0, uint64_t* keys, double* rv) {
+                         int64_t out0, uint64_t* keys, double* rv,
+                         float* umax) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
   const int lane = threadIdx.x & 31;
@@ -138,34 +203,11 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
   const uint64_t* det = cd.dets + c * D::NW;
   const Spin<NSW> sA = D::alpha(det), sB = D::beta(det);
 
-  // decode the unit
-  int kind, ii = 0, aa = 0;
-  int64_t ninner;
-  if(t == 0) {
-    kind = 0;
-    ninner = int64_t(nA) * nvA;
-  } else if(t == 1) {
-    kind = 1;
-    ninner = int64_t(nB) * nvB;
-  } else if(t < 2 + int64_t(nA) * nvA) {
-    kind = 2;
-    ii = int((t - 2) / nvA);
-    aa = int((t - 2) % nvA);
-    ninner = int64_t(nA - 1 - ii) * (nvA - 1 - aa);
-  } else if(t < 2 + int64_t(nA) * nvA + int64_t(nB) * nvB) {
-    kind = 3;
-    const int64_t u = t - 2 - int64_t(nA) * nvA;
-    ii = int(u / nvB);
-    aa = int(u % nvB);
-    ninner = int64_t(nB - 1 - ii) * (nvB - 1 - aa);
-  } else {
-    kind = 4;
-    const int64_t u = t - 2 - int64_t(nA) * nvA - int64_t(nB) * nvB;
-    ii = int(u / nvA);
-    aa = int(u % nvA);
-    ninner = int64_t(nB) * nvB;
-  }
+  const UnitDesc ud = decode_unit(nA, nB, nvA, nvB, t);
+  const int kind = ud.kind, ii = ud.ii, aa = ud.aa;
+  const int64_t ninner = ud.ninner;
   int64_t done = 0;
+  float mx = 0.f;  // largest |rv| of this lane (MODE 1)
   for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
     const int64_t q = q0 + lane;
     bool keep = false;
@@ -258,10 +300,17 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
 #pragma unroll
       for(int w = 0; w < D::NW; ++w) keys[pos * D::NW + w] = ex[w];
       rv[pos] = r;
+      mx = fmaxf(mx, float(fabs(r)));
     }
     done += __popc(m);
   }
   if(MODE == 0 && lane == 0) *count_out = done;
+  if(MODE == 1 && umax) {
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+      mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if(lane == 0) *umax = mx;
+  }
 }
 #undef G2R
 #undef V2R
@@ -271,10 +320,14 @@ template <int NBITS, int MODE>
 __global__ void __launch_bounds__(256)
     units_k(Ints I, CoreData cd, int64_t u0, int64_t u1, size_t c0, size_t c1,
             double E0, double tol, int64_t* counts, const int64_t* outoff,
-            uint64_t* keys, double* rv) {
+            uint64_t* keys, double* rv, const uint8_t* umask, float* umax) {
   const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
   for(int64_t u = u0 + int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
       u < u1; u += int64_t(nwarp)) {
+    if(umask && !umask[u]) {  // screened out: no contributions
+      if(MODE == 0 && (threadIdx.x & 31) == 0) counts[u - u0] = 0;
+      continue;
+    }
     // det owning unit u: last c in [c0, c1) with uoff[c] <= u
     size_t lo = c0, hi = c1;
     while(hi - lo > 1) {
@@ -286,8 +339,231 @@ __global__ void __launch_bounds__(256)
     }
     const int64_t t = u - cd.uoff[lo];
     unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
-                          MODE ? outoff[u - u0] : 0, keys, rv);
+                          MODE ? outoff[u - u0] : 0, keys, rv,
+                          umax ? umax + u : nullptr);
   }
+}
+
+// ------------------------------------------------------ learned screening
+// Network input of a unit (width 2 * 64 NSW + 64):
+//   occupation bits of the core det after the unit's outer excitation
+//   (alpha orbitals in columns [0, 64 NSW), beta in [64 NSW, 128 NSW)), then
+//   64 features: 1, ln|C_c| / 10, one-hot kind (5), eps of the outer hole and
+//   particle and their difference, E0 - H_cc, ln(1 + inner count) / 10, the
+//   outer orbitals scaled to (0, 1], ln of the outer pair's integral bound
+//   (macis_b200_ham::pairmax) / 10, a crude ln score estimate
+//   (ln|C| + ln bound - ln|E0 - H_cc - (eps_a - eps_i)|) / 10, and the
+//   eps-weighted occupations of orbitals 0..47 of the excited det (eps =
+//   the core det's single-orbital energies of the spin).
+constexpr int UNIT_EPS_ORBS = 48;
+
+template <int NBITS>
+__host__ __device__ constexpr int unit_din() {
+  return 2 * 64 * DetTraits<NBITS>::NSW + MLP_NFEAT;
+}
+
+__device__ __forceinline__ size_t unit_owner(const CoreData& cd, int64_t u) {
+  size_t lo = 0, hi = cd.ncdets;
+  while(hi - lo > 1) {
+    const size_t mid = (lo + hi) >> 1;
+    if(cd.uoff[mid] <= u)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t bf16_bits(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+
+// put(k, v): 16-byte piece k (columns [8k, 8k+8)) of the unit's row.
+template <int NBITS, class Put>
+__device__ void unit_features(const CoreData& cd, double E0, int64_t u,
+                              Put&& put) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  const size_t c = unit_owner(cd, u);
+  const int64_t t = u - cd.uoff[c];
+  const int n = cd.n;
+  const int no[2] = {cd.cnt[c * 4], cd.cnt[c * 4 + 1]};
+  const int nv[2] = {cd.cnt[c * 4 + 2], cd.cnt[c * 4 + 3]};
+  const UnitDesc ud = decode_unit(no[0], no[1], nv[0], nv[1], t);
+  const uint64_t* det = cd.dets + c * D::NW;
+  Spin<NSW> sp[2] = {D::alpha(det), D::beta(det)};
+  const double* eps[2] = {cd.eps + (c * 2) * n, cd.eps + (c * 2 + 1) * n};
+  int S = 0, hole = -1, part = -1;
+  if(ud.kind >= 2) {
+    S = ud.kind == 3 ? 1 : 0;
+    hole = cd.occ[(c * 2 + S) * MAXORB + ud.ii];
+    part = cd.vir[(c * 2 + S) * MAXORB + ud.aa];
+    sp[S] = sp_flip(sp_flip(sp[S], hole), part);
+  }
+  // occupation bits, one byte per piece
+#pragma unroll
+  for(int s = 0; s < 2; ++s)
+#pragma unroll
+    for(int b = 0; b < NSW * 8; ++b) {
+      const uint32_t byte = uint32_t(sp[s].w[b >> 3] >> ((b & 7) * 8)) & 0xFFu;
+      uint32_t w[4];
+#pragma unroll
+      for(int q = 0; q < 4; ++q)
+        w[q] = (((byte >> (2 * q)) & 1u) ? 0x3F80u : 0u) |
+               (((byte >> (2 * q + 1)) & 1u) ? 0x3F800000u : 0u);
+      put(s * NSW * 8 + b, make_uint4(w[0], w[1], w[2], w[3]));
+    }
+  // scalar features
+  const double eh = hole >= 0 ? eps[S][hole] : 0.0;
+  const double ep = part >= 0 ? eps[S][part] : 0.0;
+  float f[16];
+  f[0] = 1.f;
+  f[1] = float(log(fabs(cd.C[c]) + 1e-300) / 10.0);
+#pragma unroll
+  for(int k = 0; k < 5; ++k) f[2 + k] = ud.kind == k ? 1.f : 0.f;
+  f[7] = float(eh);
+  f[8] = float(ep);
+  f[9] = float(ep - eh);
+  f[10] = float(E0 - cd.hd[c]);
+  f[11] = float(log(1.0 + double(ud.ninner)) / 10.0);
+  f[12] = hole >= 0 ? float(hole + 1) / float(n) : 0.f;
+  f[13] = part >= 0 ? float(part + 1) / float(n) : 0.f;
+  // outer-pair integral bound and a crude log-score estimate
+  const double lnc = log(fabs(cd.C[c]) + 1e-300);
+  if(ud.kind >= 2) {
+    const size_t pr = size_t(part) + size_t(hole) * n;
+    const double bound =
+        cd.pairmax[(ud.kind == 4 ? size_t(n) * n : 0) + pr];
+    const double lb = log(bound + 1e-300);
+    f[14] = float(lb / 10.0);
+    f[15] = float((lnc + lb - log(fabs(E0 - cd.hd[c] - (ep - eh)) + 1e-3)) /
+                  10.0);
+  } else {
+    f[14] = 0.f;
+    f[15] = float((lnc - log(fabs(E0 - cd.hd[c]) + 1e-3)) / 10.0);
+  }
+  const int base = 2 * NSW * 8;
+#pragma unroll
+  for(int q = 0; q < 2; ++q) {
+    uint32_t w[4];
+#pragma unroll
+    for(int k = 0; k < 4; ++k)
+      w[k] = bf16_bits(f[8 * q + 2 * k]) | (bf16_bits(f[8 * q + 2 * k + 1]) << 16);
+    put(base + q, make_uint4(w[0], w[1], w[2], w[3]));
+  }
+  // eps-weighted occupations
+  for(int q = 0; q < UNIT_EPS_ORBS / 8; ++q) {
+    uint32_t w[4];
+#pragma unroll
+    for(int k = 0; k < 4; ++k) {
+      float v2[2];
+#pragma unroll
+      for(int h = 0; h < 2; ++h) {
+        const int p = 8 * q + 2 * k + h;
+        double e = 0.0;
+        if(p < n) {
+          if(sp_test(sp[0], p)) e += eps[0][p];
+          if(sp_test(sp[1], p)) e += eps[1][p];
+        }
+        v2[h] = float(e);
+      }
+      w[k] = bf16_bits(v2[0]) | (bf16_bits(v2[1]) << 16);
+    }
+    put(base + 2 + q, make_uint4(w[0], w[1], w[2], w[3]));
+  }
+}
+
+// Row source of the fused forward: tile row r = unit row0 + r.
+template <int NBITS>
+struct UnitRows {
+  CoreData cd;
+  double E0;
+  __device__ void fill(int64_t row0, int nvalid, uint8_t* xs, int tid) const {
+    uint8_t* base = xs + tid * 16;
+    if(tid < nvalid) {
+      unit_features<NBITS>(cd, E0, row0 + tid, [&](int k, uint4 v) {
+        *reinterpret_cast<uint4*>(base + size_t(k) * (MLP_TM * 16)) = v;
+      });
+    } else {
+      for(int k = 0; k < unit_din<NBITS>() / 8; ++k)
+        *reinterpret_cast<uint4*>(base + size_t(k) * (MLP_TM * 16)) =
+            make_uint4(0, 0, 0, 0);
+    }
+  }
+};
+
+// Rows of the listed units into X [n][din] (row-major BF16), and targets
+// t = (ln max(umax, 1e-12) + 20) / 5 when umax is given.
+template <int NBITS>
+__global__ void unit_rows_k(CoreData cd, double E0, const int64_t* units,
+                            int64_t first, size_t n, uint16_t* X,
+                            const float* umax, float* t) {
+  constexpr int DIN = unit_din<NBITS>();
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const int64_t u = units ? units[i] : first + int64_t(i);
+    uint4* row = reinterpret_cast<uint4*>(X + i * DIN);
+    unit_features<NBITS>(cd, E0, u, [&](int k, uint4 v) { row[k] = v; });
+    if(t) t[i] = (logf(fmaxf(umax[u], 1e-12f)) + 20.f) / 5.f;
+  }
+}
+
+__device__ __forceinline__ uint32_t pred_key(float x) {
+  const uint32_t b = __float_as_uint(x);
+  if(x != x) return 0u;  // NaN ranks last
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__global__ void pred_hist_k(const float* y, size_t n, uint32_t prefix,
+                            uint32_t mask, int shift,
+                            unsigned long long* hist) {
+  __shared__ unsigned int h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t k = pred_key(y[i]);
+    if((k & mask) == prefix) atomicAdd(&h[(k >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  if(h[threadIdx.x])
+    atomicAdd(&hist[threadIdx.x], (unsigned long long)h[threadIdx.x]);
+}
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// keep units predicted at or above the threshold key, plus a hashed random
+// fraction (explore / 2^64) of the others
+__global__ void unit_mask_k(const float* y, size_t n, uint32_t T,
+                            uint64_t explore, uint64_t seed, uint8_t* mask,
+                            unsigned long long* nkept) {
+  unsigned int c = 0;
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const bool k = pred_key(y[i]) >= T ||
+                   mix64(seed + 0x9E3779B97F4A7C15ull * (i + 1)) < explore;
+    mask[i] = k ? 1 : 0;
+    c += k;
+  }
+  for(int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if((threadIdx.x & 31) == 0 && c) atomicAdd(nkept, (unsigned long long)c);
+}
+// sample flags over the units that ran (mask or all)
+__global__ void sample_flags_k(const uint8_t* mask, size_t n, uint64_t p,
+                               uint64_t seed, uint32_t* f) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    f[i] = ((!mask || mask[i]) &&
+            mix64(seed ^ (0xD1B54A32D192ED03ull * (i + 1))) <= p)
+               ? 1u
+               : 0u;
+}
+__global__ void sample_list_k(const uint32_t* f, const uint32_t* fx, size_t n,
+                              size_t cap, int64_t* list) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    if(f[i] && fx[i] < cap) list[fx[i]] = int64_t(i);
 }
 
 // --------------------------------------------------- accumulate / merge
@@ -440,23 +716,15 @@ double ms_since(std::chrono::steady_clock::time_point t) {
 }
 }  // namespace
 
+// Core-det precompute and unit offsets; returns the unit count.
 template <int NBITS>
-static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
-                      size_t ndets_max, const uint64_t* cdets, size_t ncdets,
-                      double E0, const double* C, uint64_t* out_dets,
-                      size_t* nout, std::vector<uint64_t>* ps,
-                      std::vector<double>* pr, bool pairs_only) {
-  constexpr int NW = DetTraits<NBITS>::NW;
+static int64_t core_setup(macis_b200_ham* h, Arena& A, const uint64_t* cdets,
+                          size_t ncdets, const double* C, int just_singles,
+                          CoreData& cd) {
   cudaStream_t s = h->stream;
-  Arena A(s);
-  const Ints I = h->ints();
   const int n = h->norb;
   const int sms = num_sms();
-  auto t_all = std::chrono::steady_clock::now();
-  macis_b200_asci_stats stats{};
-
-  // ------------------------------------------------ core precompute
-  CoreData cd{};
+  cd = CoreData{};
   cd.n = n;
   cd.dets = cdets;
   cd.C = C;
@@ -468,20 +736,121 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   cd.hd = A.get<double>(ncdets + 1);
   int64_t* units = A.get<int64_t>(ncdets + 1);
   cd.uoff = A.get<int64_t>(ncdets + 1);
+  if(!h->pairmax) {
+    const size_t n2 = size_t(n) * n;
+    MB_CUDA(cudaMalloc(&h->pairmax, 2 * n2 * sizeof(double)));
+    pairmax_g_k<<<grid_for(n2 * 32, 256, 16 * sms), 256, 0, s>>>(
+        h->G, n, h->pairmax), note_launch();
+    pairmax_v_k<<<grid_for(n2, 128, 4 * sms), 128, 0, s>>>(
+        h->V, n, h->pairmax + n2), note_launch();
+    MB_CUDA(cudaGetLastError());
+  }
+  cd.pairmax = h->pairmax;
   if(ncdets) {
     core_prep_k<NBITS><<<grid_for(ncdets * 32, 256, 16 * sms), 256, 0, s>>>(
-        I, cd, st.just_singles, units), note_launch();
+        h->ints(), cd, just_singles, units), note_launch();
     MB_CUDA(cudaGetLastError());
   }
   exclusive_scan<int64_t, int64_t>(units, cd.uoff, ncdets, cd.uoff + ncdets, A);
-  const int64_t U = ncdets ? to_host(cd.uoff + ncdets, s) : 0;
+  return ncdets ? to_host(cd.uoff + ncdets, s) : 0;
+}
+
+static void check_net(const macis_b200_mlp* net, cudaStream_t s) {
+  int e = 0;
+  MB_CUDA(cudaMemcpyAsync(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  MB_REQUIRE(e == 0, MACIS_B200_ETIMEOUT,
+             "screening network kernel timed out waiting on a barrier");
+}
+
+template <int NBITS>
+static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
+                      const macis_b200_asci_screen* scr, size_t ndets_max,
+                      const uint64_t* cdets, size_t ncdets, double E0,
+                      const double* C, uint64_t* out_dets, size_t* nout,
+                      std::vector<uint64_t>* ps, std::vector<double>* pr,
+                      bool pairs_only) {
+  constexpr int NW = DetTraits<NBITS>::NW;
+  cudaStream_t s = h->stream;
+  Arena A(s);
+  const Ints I = h->ints();
+  const int sms = num_sms();
+  auto t_all = std::chrono::steady_clock::now();
+  macis_b200_asci_stats stats{};
+
+  // ------------------------------------------------ core precompute
+  CoreData cd{};
+  const int64_t U = core_setup<NBITS>(h, A, cdets, ncdets, C, st.just_singles, cd);
+
+  // ------------------------------------------------ learned screening
+  macis_b200_mlp* net = scr ? scr->net : nullptr;
+  const bool screen = net && scr->use_net && U > 0;
+  const bool record = net && scr->max_samples > 0 && U > 0;
+  if(net)
+    MB_REQUIRE(net->din == unit_din<NBITS>(), MACIS_B200_EINVAL,
+               "screening network input width does not match the determinant width");
+  stats.units_total = uint64_t(U);
+  stats.units_kept = uint64_t(U);
+  auto t_scr = std::chrono::steady_clock::now();
+  uint8_t* umask = nullptr;
+  float* umax = nullptr;
+  if(record) {
+    umax = A.get<float>(size_t(U));
+    MB_CUDA(cudaMemsetAsync(umax, 0, size_t(U) * 4, s));
+  }
+  if(screen) {
+    MB_REQUIRE(scr->keep_frac > 0 && scr->keep_frac <= 1 &&
+                   scr->explore_frac >= 0 && scr->explore_frac <= 1,
+               MACIS_B200_EINVAL, "keep_frac in (0,1], explore_frac in [0,1]");
+    float* pred = A.get<float>(size_t(U));
+    const size_t smem = mlp_fwd_smem_bytes(net->din);
+    auto kern = mlp_fwd_k<UnitRows<NBITS>, false>;
+    MB_CUDA(cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const int64_t tiles = (U + MLP_TM - 1) / MLP_TM;
+    kern<<<unsigned(std::min<int64_t>(tiles, sms)), MLP_TM, smem, s>>>(
+        mlp_weights(net), UnitRows<NBITS>{cd, E0}, U, pred, MlpTaps{},
+        net->err), note_launch();
+    MB_CUDA(cudaGetLastError());
+    // threshold key of the keep-th largest prediction (MSD radix select)
+    uint64_t need = uint64_t(std::ceil(scr->keep_frac * double(U)));
+    need = std::min<uint64_t>(std::max<uint64_t>(need, 1), uint64_t(U));
+    auto* hist = A.get<unsigned long long>(256);
+    uint32_t prefix = 0, msk = 0;
+    for(int shift = 24; shift >= 0; shift -= 8) {
+      MB_CUDA(cudaMemsetAsync(hist, 0, 256 * 8, s));
+      pred_hist_k<<<grid_for(size_t(U), 256, 8 * sms), 256, 0, s>>>(
+          pred, size_t(U), prefix, msk, shift, hist), note_launch();
+      unsigned long long hh[256];
+      MB_CUDA(cudaMemcpyAsync(hh, hist, sizeof(hh), cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaStreamSynchronize(s));
+      int d = 255;
+      for(; d > 0; --d) {
+        if(hh[d] >= need) break;
+        need -= hh[d];
+      }
+      prefix |= uint32_t(d) << shift;
+      msk |= 255u << shift;
+    }
+    umask = A.get<uint8_t>(size_t(U));
+    auto* nk = A.get<unsigned long long>(1);
+    MB_CUDA(cudaMemsetAsync(nk, 0, 8, s));
+    const double ex = scr->explore_frac * 18446744073709551616.0;
+    const uint64_t explore =
+        ex >= 18446744073709551615.0 ? ~uint64_t(0) : uint64_t(ex);
+    unit_mask_k<<<grid_for(size_t(U), 256, 8 * sms), 256, 0, s>>>(
+        pred, size_t(U), prefix, explore, scr->seed, umask, nk), note_launch();
+    stats.units_kept = to_host(nk, s);
+    check_net(net, s);
+  }
+  stats.screen_ms = ms_since(t_scr);
 
   // unit counts of the whole search (count pass over all units at once)
   int64_t* ucnt = A.get<int64_t>(U + 1);
   if(U)
     units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
         I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt, nullptr, nullptr,
-        nullptr), note_launch();
+        nullptr, umask, nullptr), note_launch();
   int64_t* uout = A.get<int64_t>(U + 1);
   exclusive_scan<int64_t, int64_t>(ucnt, uout, size_t(U), uout + U, A);
   const int64_t Ptot = U ? to_host(uout + U, s) : 0;
@@ -533,7 +902,8 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
                                        nullptr, B);
       units_k<NBITS, 1><<<grid_for(size_t(u1 - u0) * 32, 256, 32 * sms), 256,
                           0, s>>>(I, cd, u0, u1, c0, c1, E0, st.h_el_tol,
-                                  ucnt + u0, boff, keys, rv), note_launch();
+                                  ucnt + u0, boff, keys, rv, umask, umax),
+          note_launch();
       MB_CUDA(cudaGetLastError());
     }
     MB_CUDA(cudaStreamSynchronize(s));
@@ -628,6 +998,35 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   stats.unique_pairs = acc.n;
   stats.pairs_ms += pair_ms;
   stats.sort_ms = sort_ms;
+
+  // ---------------------------- (unit features, exact log score) samples
+  if(record) {
+    t_scr = std::chrono::steady_clock::now();
+    const size_t cap = size_t(scr->max_samples);
+    const double cand = double(stats.units_kept);
+    const double frac = double(cap) / std::max(cand, 1.0);
+    const uint64_t p =
+        frac >= 1.0 ? ~uint64_t(0) : uint64_t(frac * 18446744073709551616.0);
+    uint32_t* f = A.get<uint32_t>(size_t(U) + 1);
+    uint32_t* fx = A.get<uint32_t>(size_t(U) + 1);
+    sample_flags_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
+        umask, size_t(U), p, scr->seed + 1, f), note_launch();
+    exclusive_scan<uint32_t, uint32_t>(f, fx, size_t(U), fx + U, A);
+    const size_t nrec = std::min<size_t>(to_host(fx + U, s), cap);
+    int64_t* list = A.get<int64_t>(nrec + 1);
+    sample_list_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
+        f, fx, size_t(U), nrec, list), note_launch();
+    MB_CUDA(cudaStreamSynchronize(s));
+    mlp_reserve_samples(net, cap);
+    if(nrec)
+      unit_rows_k<NBITS><<<grid_for(nrec, 128, 16 * sms), 128, 0, s>>>(
+          cd, E0, list, 0, nrec, net->xs, umax, net->ts), note_launch();
+    MB_CUDA(cudaGetLastError());
+    MB_CUDA(cudaStreamSynchronize(s));
+    net->ns = nrec;
+    stats.samples = nrec;
+    stats.screen_ms += ms_since(t_scr);
+  }
 
   if(pairs_only) {
     ps->resize(acc.n * NW);
@@ -732,20 +1131,54 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
 }
 
 void asci_search_device(macis_b200_ham* h, const macis_b200_asci_settings& s,
-                        size_t ndets_max, const uint64_t* cdets, size_t ncdets,
-                        double E0, const double* C, uint64_t* out_dets,
-                        size_t* nout, std::vector<uint64_t>* ps,
-                        std::vector<double>* pr, bool pairs_only) {
+                        const macis_b200_asci_screen* scr, size_t ndets_max,
+                        const uint64_t* cdets, size_t ncdets, double E0,
+                        const double* C, uint64_t* out_dets, size_t* nout,
+                        std::vector<uint64_t>* ps, std::vector<double>* pr,
+                        bool pairs_only) {
   MB_REQUIRE(h->norb <= MAXORB, MACIS_B200_EINVAL, "norb too large for ASCI");
   if(h->nbits == 64)
-    asci_impl<64>(h, s, ndets_max, cdets, ncdets, E0, C, out_dets, nout, ps,
-                  pr, pairs_only);
+    asci_impl<64>(h, s, scr, ndets_max, cdets, ncdets, E0, C, out_dets, nout,
+                  ps, pr, pairs_only);
   else if(h->nbits == 128)
-    asci_impl<128>(h, s, ndets_max, cdets, ncdets, E0, C, out_dets, nout, ps,
-                   pr, pairs_only);
+    asci_impl<128>(h, s, scr, ndets_max, cdets, ncdets, E0, C, out_dets, nout,
+                   ps, pr, pairs_only);
   else
-    asci_impl<256>(h, s, ndets_max, cdets, ncdets, E0, C, out_dets, nout, ps,
-                   pr, pairs_only);
+    asci_impl<256>(h, s, scr, ndets_max, cdets, ncdets, E0, C, out_dets, nout,
+                   ps, pr, pairs_only);
+}
+
+template <int NBITS>
+static int64_t unit_features_impl(macis_b200_ham* h, const uint64_t* cdets,
+                                  size_t ncdets, double E0, const double* C,
+                                  size_t first, size_t n, uint16_t* X) {
+  Arena A(h->stream);
+  CoreData cd{};
+  const int64_t U = core_setup<NBITS>(h, A, cdets, ncdets, C, 0, cd);
+  if(X && n) {
+    MB_REQUIRE(first + n <= size_t(U), MACIS_B200_EINVAL,
+               "unit range outside the search's units");
+    unit_rows_k<NBITS><<<grid_for(n, 128, 16 * num_sms()), 128, 0, h->stream>>>(
+        cd, E0, nullptr, int64_t(first), n, X, nullptr, nullptr), note_launch();
+    MB_CUDA(cudaGetLastError());
+  }
+  MB_CUDA(cudaStreamSynchronize(h->stream));
+  return U;
+}
+
+int64_t asci_unit_features_device(macis_b200_ham* h, const uint64_t* cdets,
+                                  size_t ncdets, double E0, const double* C,
+                                  size_t first, size_t n, uint16_t* X) {
+  MB_REQUIRE(h->norb <= MAXORB, MACIS_B200_EINVAL, "norb too large for ASCI");
+  if(h->nbits == 64)
+    return unit_features_impl<64>(h, cdets, ncdets, E0, C, first, n, X);
+  if(h->nbits == 128)
+    return unit_features_impl<128>(h, cdets, ncdets, E0, C, first, n, X);
+  return unit_features_impl<256>(h, cdets, ncdets, E0, C, first, n, X);
+}
+
+int asci_unit_din(int nbits) {
+  return nbits == 256 ? unit_din<256>() : unit_din<64>();
 }
 
 }  // namespace mb

@@ -303,6 +303,17 @@ int macis_b200_asci_search(macis_b200_ham* h,
                            size_t ndets_max, const uint64_t* cdets,
                            size_t ncdets, double E0, const double* C,
                            uint64_t* out_dets, size_t* nout, unsigned flags) {
+  return macis_b200_asci_search_screened(h, s, nullptr, ndets_max, cdets,
+                                         ncdets, E0, C, out_dets, nout, flags);
+}
+
+int macis_b200_asci_search_screened(macis_b200_ham* h,
+                                    const macis_b200_asci_settings* s,
+                                    const macis_b200_asci_screen* scr,
+                                    size_t ndets_max, const uint64_t* cdets,
+                                    size_t ncdets, double E0, const double* C,
+                                    uint64_t* out_dets, size_t* nout,
+                                    unsigned flags) {
   return guarded([&] {
     MB_REQUIRE(h && s && out_dets && nout, MACIS_B200_EINVAL, "null argument");
     require_dets(cdets, ncdets, flags);
@@ -315,8 +326,8 @@ int macis_b200_asci_search(macis_b200_ham* h,
     if(!(flags & MACIS_B200_DEVICE_PTRS))
       MB_CUDA(cudaMallocAsync(&od, cap * nw * 8 + 32, h->stream));
     try {
-      asci_search_device(h, *s, ndets_max, cd.d, ncdets, E0, cc.d, od, nout,
-                         nullptr, nullptr, false);
+      asci_search_device(h, *s, scr, ndets_max, cd.d, ncdets, E0, cc.d, od,
+                         nout, nullptr, nullptr, false);
     } catch(...) {
       if(!(flags & MACIS_B200_DEVICE_PTRS)) cudaFreeAsync(od, h->stream);
       throw;
@@ -343,8 +354,8 @@ int macis_b200_asci_pairs(macis_b200_ham* h, const macis_b200_asci_settings* s,
     std::vector<uint64_t> ps;
     std::vector<double> pr;
     size_t dummy = 0;
-    asci_search_device(h, *s, 0, cd.d, ncdets, E0, cc.d, nullptr, &dummy, &ps,
-                       &pr, true);
+    asci_search_device(h, *s, nullptr, 0, cd.d, ncdets, E0, cc.d, nullptr,
+                       &dummy, &ps, &pr, true);
     *npairs = pr.size();
     if(states) {
       std::memcpy(states, ps.data(), ps.size() * 8);
@@ -358,6 +369,145 @@ int macis_b200_asci_last_stats(const macis_b200_ham* h,
   return guarded([&] {
     MB_REQUIRE(h && out, MACIS_B200_EINVAL, "null argument");
     *out = h->last_asci;
+  });
+}
+
+int macis_b200_asci_unit_width(int nbits) { return asci_unit_din(nbits); }
+
+int macis_b200_asci_unit_features(macis_b200_ham* h, const uint64_t* cdets,
+                                  size_t ncdets, double E0, const double* C,
+                                  size_t first, size_t n, uint16_t* X,
+                                  size_t* nunits) {
+  return guarded([&] {
+    MB_REQUIRE(h && nunits, MACIS_B200_EINVAL, "null argument");
+    require_dets(cdets, ncdets);
+    const size_t nw = h->nbits / 64, din = size_t(asci_unit_din(h->nbits));
+    DevBuf<uint64_t> cd(cdets, ncdets * nw, 0, h->stream);
+    DevBuf<double> cc(C, ncdets, 0, h->stream);
+    DevBuf<uint16_t> xd(nullptr, X ? n * din : 0, 0, h->stream);
+    *nunits = size_t(asci_unit_features_device(h, cd.d, ncdets, E0, cc.d,
+                                               first, X ? n : 0, xd.d));
+    if(X && n) {
+      MB_CUDA(cudaMemcpyAsync(X, xd.d, n * din * 2, cudaMemcpyDeviceToHost,
+                              h->stream));
+      MB_CUDA(cudaStreamSynchronize(h->stream));
+    }
+  });
+}
+
+// ------------------------------------------------------ screening network
+int macis_b200_mlp_create(int din, uint64_t seed, macis_b200_mlp** out) {
+  return guarded([&] {
+    MB_REQUIRE(out, MACIS_B200_EINVAL, "null argument");
+    *out = mlp_create(din, seed);
+  });
+}
+
+int macis_b200_mlp_destroy(macis_b200_mlp* m) {
+  return guarded([&] { mlp_destroy(m); });
+}
+
+int macis_b200_mlp_num_params(const macis_b200_mlp* m, size_t* n) {
+  return guarded([&] {
+    MB_REQUIRE(m && n, MACIS_B200_EINVAL, "null argument");
+    *n = m->nparams;
+  });
+}
+
+int macis_b200_mlp_get_params(const macis_b200_mlp* m, float* P) {
+  return guarded([&] {
+    MB_REQUIRE(m && P, MACIS_B200_EINVAL, "null argument");
+    mlp_get_params(m, P);
+  });
+}
+
+int macis_b200_mlp_set_params(macis_b200_mlp* m, const float* P) {
+  return guarded([&] {
+    MB_REQUIRE(m && P, MACIS_B200_EINVAL, "null argument");
+    mlp_set_params(m, P);
+  });
+}
+
+int macis_b200_mlp_forward(macis_b200_mlp* m, const uint16_t* X, size_t n,
+                           float* y, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(m && (n == 0 || (X && y)), MACIS_B200_EINVAL, "null argument");
+    const size_t din = size_t(m->din);
+    DevBuf<uint16_t> xd(X, n * din, flags, m->stream);
+    DevBuf<float> yd(nullptr, (flags & MACIS_B200_DEVICE_PTRS) ? 0 : n, 0,
+                     m->stream);
+    float* yp = (flags & MACIS_B200_DEVICE_PTRS) ? y : yd.d;
+    mlp_forward_device(m, xd.d, int64_t(n), yp, m->stream);
+    if(!(flags & MACIS_B200_DEVICE_PTRS) && n) {
+      MB_CUDA(cudaMemcpyAsync(y, yp, n * 4, cudaMemcpyDeviceToHost, m->stream));
+      MB_CUDA(cudaStreamSynchronize(m->stream));
+    }
+  });
+}
+
+int macis_b200_mlp_gradients(macis_b200_mlp* m, const uint16_t* X,
+                             const float* t, size_t n, float* grad,
+                             double* loss, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(m && X && t && grad && n > 0, MACIS_B200_EINVAL,
+               "null argument or empty batch");
+    const size_t din = size_t(m->din);
+    DevBuf<uint16_t> xd(X, n * din, flags, m->stream);
+    DevBuf<float> td(t, n, flags, m->stream);
+    DevBuf<float> gd(nullptr, m->nparams, 0, m->stream);
+    const double l = mlp_gradients_device(m, xd.d, td.d, int64_t(n), gd.d);
+    MB_CUDA(cudaMemcpyAsync(grad, gd.d, m->nparams * 4,
+                            (flags & MACIS_B200_DEVICE_PTRS)
+                                ? cudaMemcpyDeviceToDevice
+                                : cudaMemcpyDeviceToHost,
+                            m->stream));
+    MB_CUDA(cudaStreamSynchronize(m->stream));
+    if(loss) *loss = l;
+  });
+}
+
+int macis_b200_mlp_train(macis_b200_mlp* m, const uint16_t* X, const float* t,
+                         size_t n, int epochs, int batch, double lr,
+                         uint64_t seed, double* loss, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(m, MACIS_B200_EINVAL, "null argument");
+    double l = 0;
+    if(X == nullptr) {
+      MB_REQUIRE(m->ns > 0, MACIS_B200_EINVAL, "no recorded samples");
+      l = mlp_train_device(m, m->xs, m->ts, int64_t(m->ns), epochs, batch, lr,
+                           seed);
+    } else {
+      MB_REQUIRE(t && n > 0, MACIS_B200_EINVAL, "null targets or no samples");
+      const size_t din = size_t(m->din);
+      DevBuf<uint16_t> xd(X, n * din, flags, m->stream);
+      DevBuf<float> td(t, n, flags, m->stream);
+      l = mlp_train_device(m, xd.d, td.d, int64_t(n), epochs, batch, lr, seed);
+    }
+    if(loss) *loss = l;
+  });
+}
+
+int macis_b200_mlp_clamp_samples(macis_b200_mlp* m, double q, float* floor) {
+  return guarded([&] {
+    MB_REQUIRE(m, MACIS_B200_EINVAL, "null argument");
+    const float f = mlp_clamp_samples(m, q);
+    if(floor) *floor = f;
+  });
+}
+
+int macis_b200_mlp_samples(const macis_b200_mlp* m, size_t* n, uint16_t* X,
+                           float* t) {
+  return guarded([&] {
+    MB_REQUIRE(m && n, MACIS_B200_EINVAL, "null argument");
+    *n = m->ns;
+    if(X && m->ns) {
+      MB_CUDA(cudaMemcpyAsync(X, m->xs, m->ns * size_t(m->din) * 2,
+                              cudaMemcpyDeviceToHost, m->stream));
+      if(t)
+        MB_CUDA(cudaMemcpyAsync(t, m->ts, m->ns * 4, cudaMemcpyDeviceToHost,
+                                m->stream));
+      MB_CUDA(cudaStreamSynchronize(m->stream));
+    }
   });
 }
 

@@ -118,6 +118,7 @@ void ham_destroy(macis_b200_ham* h) {
   cudaFree(h->G2_red);
   cudaFree(h->V2_red);
   cudaFree(h->VT);
+  cudaFree(h->pairmax);
   if(h->stream) cudaStreamDestroy(h->stream);
 }
 

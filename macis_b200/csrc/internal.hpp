@@ -19,6 +19,11 @@ struct macis_b200_ham {
   // V[(p + q n) + (r + s n) n^2]; built on first use by the direct-product
   // fill so that one alpha pair's row of V is contiguous
   double* VT = nullptr;
+  // Per outer pair (i, a), p = a + i n: pairmax[p] = max_{b,j} |G(b,j,a,i)|
+  // and pairmax[n^2 + p] = max_{b,j} |V(a,i,b,j)| -- upper bounds of the
+  // same-spin / opposite-spin double elements of the ASCI units; built on
+  // first use by the screened search
+  double* pairmax = nullptr;
   macis_b200_asci_stats last_asci{};
   mb::Ints ints() const {
     return mb::Ints{norb, T, V, G, G_red, V_red, G2_red, V2_red};
@@ -43,7 +48,54 @@ struct macis_b200_csr {
   float fill_ms = 0.f;
 };
 
+// Screening network (mlp.cu). BF16 buffers are held as uint16_t.
+struct macis_b200_mlp {
+  int din = 192;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t off_w1 = 0, off_b1 = 0, off_w2 = 0, off_b2 = 0, off_w3 = 0,
+         off_b3 = 0, nparams = 0;
+  float *P = nullptr, *G = nullptr, *Mo = nullptr, *Ve = nullptr;
+  uint16_t *w1t = nullptr, *w2t = nullptr, *w2T = nullptr;
+  int* err = nullptr;
+  int64_t step = 0;  // Adam steps taken
+  // training scratch for batches of B rows
+  int64_t B = 0;
+  std::vector<void*> scratch;
+  uint16_t *xb = nullptr, *xbt = nullptr, *h1t = nullptr, *dz2t_b = nullptr,
+           *dz2_b = nullptr, *dz1t_b = nullptr;
+  float *tb = nullptr, *yb = nullptr, *z1t = nullptr, *z2t = nullptr,
+        *dy = nullptr, *dz2t = nullptr, *p3t = nullptr, *dz1t = nullptr;
+  int64_t* idx = nullptr;
+  // (features, target) samples recorded by the last ASCI search
+  uint16_t* xs = nullptr;
+  float* ts = nullptr;
+  size_t ns = 0, cap = 0;
+  double last_loss = 0;
+  double train_ms = 0;
+};
+
 namespace mb {
+
+struct MlpWeights;
+macis_b200_mlp* mlp_create(int din, uint64_t seed);
+void mlp_destroy(macis_b200_mlp* m);
+void mlp_set_params(macis_b200_mlp* m, const float* host);
+void mlp_get_params(const macis_b200_mlp* m, float* host);
+MlpWeights mlp_weights(const macis_b200_mlp* m);
+// y[0..n) = network(X) for device X [n][din] BF16; synchronizes s.
+void mlp_forward_device(macis_b200_mlp* m, const uint16_t* X, int64_t n,
+                        float* y, cudaStream_t s);
+// One forward + backward over all n rows; device gradient (nparams) -> grad.
+double mlp_gradients_device(macis_b200_mlp* m, const uint16_t* X,
+                            const float* t, int64_t n, float* grad);
+// Adam on (X, t) device samples; returns the mean loss of the last epoch.
+double mlp_train_device(macis_b200_mlp* m, const uint16_t* X, const float* t,
+                        int64_t S, int epochs, int batch, double lr,
+                        uint64_t seed);
+void mlp_reserve_samples(macis_b200_mlp* m, size_t cap);
+// Raise the recorded targets below their q-quantile to it; returns the floor.
+float mlp_clamp_samples(macis_b200_mlp* m, double q);
 
 // Build the CSR block of H for device-resident bra/ket determinant arrays.
 macis_b200_csr* build_csr_device(macis_b200_ham* h, const uint64_t* bra,
@@ -68,11 +120,19 @@ void small_syev_lowest(int k, const double* lower, int nwant, double* W,
                        double* Vec);
 
 // ASCI search on device-resident core dets (see macis_b200_asci_search).
+// scr may be null (exact search, nothing recorded).
 void asci_search_device(macis_b200_ham* h, const macis_b200_asci_settings& s,
-                        size_t ndets_max, const uint64_t* cdets, size_t ncdets,
-                        double E0, const double* C, uint64_t* out_dets,
-                        size_t* nout, std::vector<uint64_t>* pairs_states,
+                        const macis_b200_asci_screen* scr, size_t ndets_max,
+                        const uint64_t* cdets, size_t ncdets, double E0,
+                        const double* C, uint64_t* out_dets, size_t* nout,
+                        std::vector<uint64_t>* pairs_states,
                         std::vector<double>* pairs_rv, bool pairs_only);
+// Network input rows of units [first, first + n) of the search over the core
+// dets (device X [n][din]); returns the unit count.
+int64_t asci_unit_features_device(macis_b200_ham* h, const uint64_t* cdets,
+                                  size_t ncdets, double E0, const double* C,
+                                  size_t first, size_t n, uint16_t* X);
+int asci_unit_din(int nbits);
 
 void set_error(const std::string& s);
 

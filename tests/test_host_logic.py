@@ -30,10 +30,11 @@ def test_struct_layouts_match_header(tmp_path):
     import subprocess
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include "macis_b200.h"\nint main(){'
-                   'printf("%zu %zu %zu %zu", sizeof(macis_b200_asci_settings),'
+                   'printf("%zu %zu %zu %zu %zu", sizeof(macis_b200_asci_settings),'
                    'sizeof(macis_b200_asci_stats),'
                    'sizeof(macis_b200_davidson_opts),'
-                   'sizeof(macis_b200_build_stats));return 0;}')
+                   'sizeof(macis_b200_build_stats),'
+                   'sizeof(macis_b200_asci_screen));return 0;}')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src),
                     "-o", str(exe)], check=True)
@@ -42,7 +43,8 @@ def test_struct_layouts_match_header(tmp_path):
     assert got == [ctypes.sizeof(_lib.AsciSettingsC),
                    ctypes.sizeof(_lib.AsciStatsC),
                    ctypes.sizeof(_lib.DavidsonOptsC),
-                   ctypes.sizeof(_lib.BuildStatsC)]
+                   ctypes.sizeof(_lib.BuildStatsC),
+                   ctypes.sizeof(_lib.AsciScreenC)]
     assert ctypes.sizeof(_lib.AsciSettingsC) == ctypes.sizeof(
         oracle.AsciSettings)
 
