@@ -418,13 +418,17 @@ def extras(mb, H, dets, torch):
         out["asci_search_n48"] = asci_extra(mb)
     except Exception as e:  # noqa: BLE001
         out["asci_search_n48"] = {"error": str(e)}
+    try:
+        out["asci_screened_n48"] = screen_extra(mb)
+    except Exception as e:  # noqa: BLE001
+        out["asci_screened_n48"] = {"error": str(e)}
     return out
 
 
-def asci_extra(mb, ncore=10000, ndets_max=1000000, seed=0):
-    """One asci_search on n = 48 orbitals, 12 alpha / 12 beta, bitset<128>:
-    HF plus its lowest singles / doubles as the core set with decaying
-    coefficients (C3-shaped, exact FP64 search)."""
+def _n48_core(mb, ncore, seed=0):
+    """n = 48 orbitals, 12 alpha / 12 beta, bitset<128>: HF plus its lowest
+    singles / doubles as the core set with decaying coefficients
+    (C3-shaped)."""
     n, k = 48, 12
     T, V = mb.synthetic_integrals(n, seed)
     H = mb.HamiltonianGenerator(T, V, 128)
@@ -447,9 +451,17 @@ def asci_extra(mb, ncore=10000, ndets_max=1000000, seed=0):
     C = np.exp(-0.5 * np.arange(len(core)) / 100.0)
     C /= np.linalg.norm(C)
     hd = H.matrix_element(core[:1], core[:1])
+    return n, H, core, C, hd - 0.5
+
+
+def asci_extra(mb, ncore=10000, ndets_max=1000000, seed=0):
+    """One exact FP64 asci_search on the n = 48 core set."""
+    n, H, core, C, E0 = _n48_core(mb, ncore, seed)
     s = mb.ASCISettings()
+    # a warm-up search sizes the memory pool, as in a multi-iteration run
+    mb.asci_search(s, ndets_max, core[:ncore // 4], E0, C[:ncore // 4], n, H)
     t = time.perf_counter()
-    out = mb.asci_search(s, ndets_max, core, hd - 0.5, C, n, H)
+    out = mb.asci_search(s, ndets_max, core, E0, C, n, H)
     dt = time.perf_counter() - t
     st = mb.last_search_stats(H)
     return {"seconds": dt, "ncdets": len(core), "ndets_max": ndets_max,
@@ -458,6 +470,58 @@ def asci_extra(mb, ncore=10000, ndets_max=1000000, seed=0):
             "raw_pairs_per_s": st["raw_pairs"] / dt,
             "phase_ms": {k2: st[k2] for k2 in ("pairs_ms", "sort_ms",
                                                "keep_ms", "topk_ms")}}
+
+
+def screen_extra(mb, ncore=10000, ndets_max=1000000, seed=0, keep=0.2,
+                 batch=None, lr=None, epochs=None):
+    """Learned screening on the n = 48 core set: the network is trained on
+    the exact search over the leading ncore/4 core dets (the previous
+    iteration's data), then the search over all ncore dets runs exact and
+    screened (top `keep` of the units). Reports both times, the training
+    time, top-k recall of the screened selection and the network forward
+    throughput (tensor-pipe work)."""
+    n, H, core, C, E0 = _n48_core(mb, ncore, seed)
+    s = mb.ASCISettings()
+    net = mb.ScreeningNetwork(nbits=128, seed=seed)
+    scr = mb.ScreenSettings(network=net, max_samples=1000000)
+    scr.batch = batch or scr.batch
+    scr.lr = lr or scr.lr
+    scr.epochs = epochs or scr.epochs
+    nprev = max(1, ncore // 4)
+    mb.asci_search(s, ndets_max // 4, core[:nprev], E0, C[:nprev], n, H,
+                   screen=scr)
+    st_p = mb.last_search_stats(H)
+    t = time.perf_counter()
+    net.clamp_samples(scr.clamp_quantile)
+    loss = net.train(None, None, scr.epochs, scr.batch, scr.lr, seed)
+    t_train = time.perf_counter() - t
+    t = time.perf_counter()
+    exact = mb.asci_search(s, ndets_max, core, E0, C, n, H)
+    t_exact = time.perf_counter() - t
+    st_e = mb.last_search_stats(H)
+    sc = mb.ScreenSettings(network=net, keep_frac=keep, explore_frac=0.0,
+                           train=False)
+    mb.asci_search(s, ndets_max, core, E0, C, n, H, screen=sc, use_net=True)
+    t = time.perf_counter()
+    scrd = mb.asci_search(s, ndets_max, core, E0, C, n, H, screen=sc,
+                          use_net=True)
+    t_scr = time.perf_counter() - t
+    st_s = mb.last_search_stats(H)
+    ea = set(map(bytes, exact))
+    recall = sum(1 for d in scrd if bytes(d) in ea) / max(len(exact), 1)
+    din = mb.unit_width(128)
+    flop = 2.0 * (din * 256 + 256 * 256 + 256) * st_s["units_total"]
+    return {"ncdets": len(core), "ndets_max": ndets_max, "keep_frac": keep,
+            "batch": scr.batch, "lr": scr.lr, "epochs": scr.epochs,
+            "train_samples": st_p["samples"],
+            "exact_s": t_exact, "screened_s": t_scr, "train_s": t_train,
+            "train_loss": loss, "speedup_search": t_exact / t_scr,
+            "topk_recall": recall,
+            "units": [st_s["units_kept"], st_s["units_total"]],
+            "raw_pairs": [st_s["raw_pairs"], st_e["raw_pairs"]],
+            "predict_ms": st_s["predict_ms"],
+            "predict_tflops": flop / (st_s["predict_ms"] * 1e-3) / 1e12,
+            "screen_ms": st_s["screen_ms"]}
 
 
 def main():

@@ -74,6 +74,7 @@ typedef struct {
   uint64_t units_kept;    /* units scored exactly */
   uint64_t samples;       /* training samples recorded into the network */
   double screen_ms;       /* prediction + selection + recording */
+  double predict_ms;      /* network forward over all units (device time) */
 } macis_b200_asci_stats;
 
 /* Learned screening (no MACIS counterpart). A "unit" of the ASCI search is

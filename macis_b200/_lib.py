@@ -36,7 +36,7 @@ class AsciStatsC(C.Structure):
                 ("keep_ms", C.c_double), ("topk_ms", C.c_double),
                 ("total_ms", C.c_double), ("units_total", C.c_uint64),
                 ("units_kept", C.c_uint64), ("samples", C.c_uint64),
-                ("screen_ms", C.c_double)]
+                ("screen_ms", C.c_double), ("predict_ms", C.c_double)]
 
 
 class AsciScreenC(C.Structure):

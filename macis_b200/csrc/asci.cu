@@ -808,10 +808,21 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     MB_CUDA(cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int64_t tiles = (U + MLP_TM - 1) / MLP_TM;
+    cudaEvent_t ev[2];
+    MB_CUDA(cudaEventCreate(&ev[0]));
+    MB_CUDA(cudaEventCreate(&ev[1]));
+    MB_CUDA(cudaEventRecord(ev[0], s));
     kern<<<unsigned(std::min<int64_t>(tiles, sms)), MLP_TM, smem, s>>>(
         mlp_weights(net), UnitRows<NBITS>{cd, E0}, U, pred, MlpTaps{},
         net->err), note_launch();
     MB_CUDA(cudaGetLastError());
+    MB_CUDA(cudaEventRecord(ev[1], s));
+    MB_CUDA(cudaEventSynchronize(ev[1]));
+    float pms = 0.f;
+    MB_CUDA(cudaEventElapsedTime(&pms, ev[0], ev[1]));
+    stats.predict_ms = pms;
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
     // threshold key of the keep-th largest prediction (MSD radix select)
     uint64_t need = uint64_t(std::ceil(scr->keep_frac * double(U)));
     need = std::min<uint64_t>(std::max<uint64_t>(need, 1), uint64_t(U));

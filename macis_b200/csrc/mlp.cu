@@ -130,12 +130,16 @@ __global__ void __launch_bounds__(128)
                              __uint_as_float(v[4 * q + 2]),
                              __uint_as_float(v[4 * q + 3]));
       } else {
+        // all 16 pre-activations first: independent loads, one latency
+        float z[16];
+#pragma unroll
+        for(int q = 0; q < 16; ++q)
+          z[q] = m < o.mvalid ? __ldg(o.z1t + (n0 + c0 + q) * o.ldo + m) : 0.f;
 #pragma unroll
         for(int q = 0; q < 16; ++q) {
           const int64_t n = n0 + c0 + q;
-          float g = 0.f;
-          if(m < o.mvalid)
-            g = __uint_as_float(v[q]) * gelu_grad_f(o.z1t[n * o.ldo + m]);
+          const float g =
+              m < o.mvalid ? __uint_as_float(v[q]) * gelu_grad_f(z[q]) : 0.f;
           o.of32t[n * o.ldo + m] = g;
           o.obf16t[n * o.ldo + m] = __float2bfloat16_rn(g);
         }
@@ -182,6 +186,29 @@ __global__ void mlp_loss_k(const float* y, const float* t, int64_t nvalid,
 }
 
 // out[r] = sum_{m < n} in[r * ld + m] in a fixed order (deterministic).
+// Rows [0, r1) come from (in, out), rows [r1, r2) from (in2, out2), and so
+// on, so that several small reductions share one launch.
+struct RowSums {
+  const float* in[3];
+  float* out[3];
+  int rows[3];
+};
+__global__ void rowsums_k(RowSums R, int64_t ld, int64_t n) {
+  __shared__ float sh[256];
+  int r = blockIdx.x, g = 0;
+  while(g < 2 && r >= R.rows[g]) r -= R.rows[g++];
+  const float* row = R.in[g] + int64_t(r) * ld;
+  float a = 0.f;
+  for(int64_t m = threadIdx.x; m < n; m += blockDim.x) a += row[m];
+  sh[threadIdx.x] = a;
+  __syncthreads();
+  for(int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if(int(threadIdx.x) < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if(threadIdx.x == 0) R.out[g][r] = sh[0];
+}
+
 __global__ void rowsum_k(const float* in, int64_t ld, int64_t n, float* out) {
   __shared__ float sh[256];
   const float* row = in + int64_t(blockIdx.x) * ld;
@@ -373,9 +400,10 @@ void fwd_bwd(macis_b200_mlp* m, const uint16_t* X, const float* t,
       reinterpret_cast<__nv_bfloat16*>(m->dz2t_b),
       reinterpret_cast<__nv_bfloat16*>(m->dz2_b), m->p3t, loss_acc), note_launch();
   float* G = m->G;
-  rowsum_k<<<MLP_H, 256, 0, s>>>(m->dz2t, B, B, G + m->off_b2), note_launch();
-  rowsum_k<<<MLP_H, 256, 0, s>>>(m->p3t, B, B, G + m->off_w3), note_launch();
-  rowsum_k<<<1, 256, 0, s>>>(m->dy, B, B, G + m->off_b3), note_launch();
+  RowSums rs{{m->dz2t, m->p3t, m->dy},
+             {G + m->off_b2, G + m->off_w3, G + m->off_b3},
+             {MLP_H, MLP_H, 1}};
+  rowsums_k<<<2 * MLP_H + 1, 256, 0, s>>>(rs, B, B), note_launch();
   // dW2[o][i] = sum_m dZ2[m][o] H1[m][i]
   GemmOut o2;
   o2.c = G + m->off_w2;

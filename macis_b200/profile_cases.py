@@ -5,6 +5,9 @@
     python -m macis_b200.profile_cases spmv_c1     # FP64 SpMV on CAS(10e,10o)
     python -m macis_b200.profile_cases hbuild_sel  # selected (shuffled) space
     python -m macis_b200.profile_cases asci_n48    # one ASCI search, n = 48
+    python -m macis_b200.profile_cases mlp_fwd     # network forward, 2M rows
+    python -m macis_b200.profile_cases mlp_train   # one training epoch
+    python -m macis_b200.profile_cases screen_n48  # screened search, n = 48
 
 Each case runs its hot call a few times (--reps) and prints one timing line.
 """
@@ -61,6 +64,50 @@ def asci_n48(reps, ncore=2000):
               f"unique={r['unique_pairs']}")
 
 
+def _rand_rows(n, din, seed=0):
+    rng = np.random.default_rng(seed)
+    X = np.zeros((n, din), dtype=np.float32)
+    X[:, :din - 64] = rng.integers(0, 2, (n, din - 64))
+    X[:, din - 64:] = rng.normal(0, 1, (n, 64))
+    u = X.view(np.uint32).astype(np.uint64)
+    return (((u + 0x7FFF + ((u >> 16) & 1)) >> 16)).astype(np.uint16)
+
+
+def mlp_fwd(reps, n=1 << 21):
+    net = mb.ScreeningNetwork(din=192, seed=0)
+    X = _rand_rows(n, 192)
+    for _ in range(reps):
+        t = time.perf_counter()
+        net.forward(X)
+        dt = time.perf_counter() - t
+        print(f"mlp forward {n} rows {dt * 1e3:.3f} ms (host-staged)")
+
+
+def mlp_train(reps, n=1 << 18, batch=256):
+    net = mb.ScreeningNetwork(din=192, seed=0)
+    X = _rand_rows(n, 192)
+    t = np.random.default_rng(1).normal(0, 1, n).astype(np.float32)
+    for _ in range(reps):
+        tt = time.perf_counter()
+        loss = net.train(X, t, epochs=1, batch=batch)
+        dt = time.perf_counter() - tt
+        print(f"mlp train 1 epoch {n} rows batch {batch}: {dt * 1e3:.1f} ms "
+              f"({dt * 1e6 / (n / batch):.1f} us/step) loss {loss:.4f}")
+
+
+def screen_n48(reps, ncore=10000):
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "bench", os.path.join(os.path.dirname(os.path.dirname(
+            os.path.abspath(__file__))), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for _ in range(reps):
+        r = bench.screen_extra(mb, ncore=ncore, ndets_max=200000)
+        print(r)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case")
@@ -76,6 +123,12 @@ def main():
         spmv(10, 5, a.reps)
     elif a.case == "asci_n48":
         asci_n48(a.reps)
+    elif a.case == "mlp_fwd":
+        mlp_fwd(a.reps)
+    elif a.case == "mlp_train":
+        mlp_train(a.reps)
+    elif a.case == "screen_n48":
+        screen_n48(a.reps)
     else:
         raise SystemExit(f"unknown case {a.case}")
 

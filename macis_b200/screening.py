@@ -134,7 +134,7 @@ class ScreenSettings:
     max_samples: int = 1_000_000  # samples recorded per search
     epochs: int = 2
     lr: float = 1e-3
-    batch: int = 256
+    batch: int = 1024
     clamp_quantile: float = 0.6   # recorded targets below it are raised to it
     min_units: int = 20000        # searches with fewer units run exact
     warmup_searches: int = 1      # exact (recording) searches before pruning
