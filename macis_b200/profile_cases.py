@@ -50,7 +50,7 @@ def spmv(norb, k, reps):
         print(f"spmv host-staged {1e3 * (time.perf_counter() - t):.3f} ms")
 
 
-def asci_n48(reps, ncore=2000):
+def asci_n48(reps, ncore=10000):
     import importlib.util
     import os
     spec = importlib.util.spec_from_file_location(
@@ -61,7 +61,8 @@ def asci_n48(reps, ncore=2000):
     for _ in range(reps):
         r = bench.asci_extra(mb, ncore=ncore, ndets_max=200000)
         print(f"asci {r['seconds']:.3f} s raw={r['raw_pairs']} "
-              f"unique={r['unique_pairs']}")
+              f"unique={r['unique_pairs']} batches={r['batches']} "
+              f"phases={r['phase_ms']}")
 
 
 def _rand_rows(n, din, seed=0):
