@@ -229,7 +229,20 @@ __global__ void key_vary_k(const uint64_t* keys, size_t n, uint64_t* vary) {
 
 template <int NW>
 __device__ __forceinline__ unsigned digit_of(const Key<NW>& k, int shift) {
-  return unsigned(k.w[shift >> 6] >> (shift & 63)) & 255u;
+  // select the word with predicated moves, not a dynamic index (which
+  // would place the key in local memory)
+  const int sel = shift >> 6;
+  uint64_t w;
+  if constexpr(NW == 1) {
+    w = k.w[0];
+  } else if constexpr(NW == 2) {
+    w = sel ? k.w[1] : k.w[0];
+  } else {
+    const uint64_t lo = (sel & 1) ? k.w[1] : k.w[0];
+    const uint64_t hi = (sel & 1) ? k.w[3] : k.w[2];
+    w = (sel & 2) ? hi : lo;
+  }
+  return unsigned(w >> (shift & 63)) & 255u;
 }
 
 template <int NW>
@@ -249,28 +262,50 @@ __global__ void __launch_bounds__(RS_THREADS)
   counts[size_t(threadIdx.x) * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
+// Bytes of shared memory the scatter stages a tile in.
+template <int NW, typename P>
+constexpr size_t rs_stage_bytes() {
+  return size_t(RS_TILE) * (8 * NW + sizeof(P));
+}
+
+// One digit pass. Every warp ranks its 512 items (__match_any_sync, input
+// order), the block turns the per-warp counts into each item's position in
+// a bucket-ordered copy of the tile in shared memory, and then consecutive
+// threads write consecutive items of a bucket to consecutive addresses, so
+// the stores of a bucket run (16 items per bucket on average) coalesce.
+// Stable: within a bucket items keep warp, round and lane order, which is
+// the input order. Keys are read twice (the second time from L2) so that no
+// per-thread key array is needed.
 template <int NW, typename P>
 __global__ void __launch_bounds__(RS_THREADS)
     radix_scatter_k(const uint64_t* keys, const P* vals, size_t n, int shift,
                     const uint64_t* offsets, unsigned nblocks,
                     uint64_t* keys_out, P* vals_out) {
+  extern __shared__ __align__(16) uint8_t rs_smem[];
+  uint64_t* skeys = reinterpret_cast<uint64_t*>(rs_smem);
+  P* svals = reinterpret_cast<P*>(skeys + size_t(RS_TILE) * NW);
   __shared__ uint32_t wcount[RS_WARPS][256];
+  __shared__ uint32_t bstart[256];
   __shared__ uint64_t boff[256];
+  __shared__ uint32_t scan_sh[RS_WARPS + 1];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for(int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS)
     (&wcount[0][0])[d] = 0;
   boff[threadIdx.x] = offsets[size_t(threadIdx.x) * nblocks + blockIdx.x];
   __syncthreads();
-  const size_t wbase = size_t(blockIdx.x) * RS_TILE + size_t(wid) * RS_WARP_ITEMS;
-  Key<NW> k[RS_IPT];
+  const size_t tile0 = size_t(blockIdx.x) * RS_TILE;
+  const size_t wbase = tile0 + size_t(wid) * RS_WARP_ITEMS;
   uint32_t rank[RS_IPT];
   unsigned dig[RS_IPT];
+  // all loads first (16 in flight per thread), then the dependent ranking
 #pragma unroll
   for(int r = 0; r < RS_IPT; ++r) {
     const size_t i = wbase + size_t(r) * 32 + lane;
-    const bool ok = i < n;
-    if(ok) k[r] = load_key<NW>(keys, i);
-    dig[r] = ok ? digit_of<NW>(k[r], shift) : 256u;
+    dig[r] = i < n ? digit_of<NW>(load_key<NW>(keys, i), shift) : 256u;
+  }
+#pragma unroll
+  for(int r = 0; r < RS_IPT; ++r) {
+    const bool ok = dig[r] < 256u;
     const unsigned peers = __match_any_sync(0xffffffffu, dig[r]);
     const unsigned before = __popc(peers & lanemask_lt());
     const int leader = __ffs(peers) - 1;
@@ -282,27 +317,37 @@ __global__ void __launch_bounds__(RS_THREADS)
     __syncwarp();
   }
   __syncthreads();
-  // exclusive prefix over warps, per digit
   {
+    // per digit: exclusive prefix over warps, then over digits (bucket
+    // starts inside the tile)
     const int d = threadIdx.x;
     uint32_t acc = 0;
 #pragma unroll
     for(int w = 0; w < RS_WARPS; ++w) {
-      uint32_t c = wcount[w][d];
+      const uint32_t c = wcount[w][d];
       wcount[w][d] = acc;
       acc += c;
     }
+    bstart[d] = block_excl_scan<uint32_t>(acc, scan_sh, nullptr);
   }
   __syncthreads();
 #pragma unroll
   for(int r = 0; r < RS_IPT; ++r) {
-    const size_t i = wbase + size_t(r) * 32 + lane;
-    if(i < n) {
-      const unsigned d = dig[r];
-      const size_t dst = boff[d] + wcount[wid][d] + rank[r];
-      store_key<NW>(keys_out, dst, k[r]);
-      if(vals) vals_out[dst] = vals[i];
+    if(dig[r] < 256u) {
+      const size_t i = wbase + size_t(r) * 32 + lane;
+      const uint32_t pos = bstart[dig[r]] + wcount[wid][dig[r]] + rank[r];
+      store_key<NW>(skeys, pos, load_key<NW>(keys, i));
+      if(vals) svals[pos] = vals[i];
     }
+  }
+  __syncthreads();
+  const int cnt = int(n - tile0 < size_t(RS_TILE) ? n - tile0 : size_t(RS_TILE));
+  for(int j = threadIdx.x; j < cnt; j += RS_THREADS) {
+    const Key<NW> kk = load_key<NW>(skeys, j);
+    const unsigned d = digit_of<NW>(kk, shift);
+    const size_t dst = boff[d] + uint32_t(j - bstart[d]);
+    store_key<NW>(keys_out, dst, kk);
+    if(vals) vals_out[dst] = svals[j];
   }
 }
 
@@ -321,6 +366,10 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
   MB_CUDA(cudaMemcpyAsync(vary, d_vary, NW * 8, cudaMemcpyDeviceToHost, A.s));
   MB_CUDA(cudaStreamSynchronize(A.s));
   const unsigned nblocks = unsigned((n + RS_TILE - 1) / RS_TILE);
+  constexpr size_t stage = rs_stage_bytes<NW, P>();
+  MB_CUDA(cudaFuncSetAttribute(radix_scatter_k<NW, P>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(stage)));
   uint32_t* counts = A.get<uint32_t>(size_t(256) * nblocks);
   uint64_t* offs = A.get<uint64_t>(size_t(256) * nblocks);
   int passes = 0;
@@ -334,7 +383,7 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
                                                         nblocks), note_launch();
       exclusive_scan<uint32_t, uint64_t>(counts, offs, size_t(256) * nblocks,
                                          nullptr, A);
-      radix_scatter_k<NW, P><<<nblocks, RS_THREADS, 0, A.s>>>(
+      radix_scatter_k<NW, P><<<nblocks, RS_THREADS, stage, A.s>>>(
           kin, vin, n, shift, offs, nblocks, kout, vout), note_launch();
       std::swap(kin, kout);
       std::swap(vin, vout);
