@@ -315,7 +315,8 @@ __device__ __forceinline__ void dp_store(CI* colind, VT* nzval, int64_t pos,
 // Packed list words of the fill (y of a uint2 whose x is the partner
 // string index): bits 0..27 an integral offset, bits 29..30 the excitation
 // class (0 none, 1 single, 2 double), bit 31 the fermionic sign.
-//   alpha list:  single -> pair index a = v1 + o1 n (row a of VT)
+//   alpha list:  single -> pair index a = v1 + o1 n (row a of VT) in bits
+//                0..13, singles-table index v1 n + o1 in bits 14..27
 //                double -> G offset of (v1,o1,v2,o2)
 //   beta L2:     single -> pair index b = v1 + o1 n (column b of VT)
 //   beta L4:     single -> singles-table index n^2 + v1 n + o1
@@ -331,8 +332,10 @@ __global__ void dp_encode_k(uint32_t* info, int64_t m, int n, int which) {
     const uint32_t o1 = ex_o1(e), v1 = ex_v1(e), o2 = ex_o2(e), v2 = ex_v2(e);
     if(p == 2) {
       cls = 1;
-      if(which == 0 || which == 1)
-        off = v1 + o1 * n;  // pair index: row of VT (alpha) / column (beta)
+      if(which == 0)  // pair index (row of VT) | singles-table index << 14
+        off = (v1 + o1 * n) | ((v1 * n + o1) << 14);
+      else if(which == 1)
+        off = v1 + o1 * n;  // pair index: column of VT
       else
         off = n2 + v1 * n + o1;
     } else if(p == 4) {
@@ -447,14 +450,35 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
     {
       const int nsa = no[0] * nv[0], nsb = no[1] * nv[1];
       for(int t = lane; t < nsa + nsb; t += 32) {
+        // selects instead of no[S] / nv[S]: a dynamic index would put the
+        // arrays in local memory
         const int S = t < nsa ? 0 : 1;
         const int u = S ? t - nsa : t;
-        const int v = occl[S * 128 + u / nv[S]], o = virl[S * 128 + u % nv[S]];
+        const int nvS = S ? nv[1] : nv[0];
+        const int noS = S ? no[1] : no[0], noO = S ? no[0] : no[1];
+        const int v = occl[S * 128 + u / nvS], o = virl[S * 128 + u % nvS];
         double h = sT[v + o * n];
         const double* Gov = sG + v * n + o * n2;
         const double* Vov = sV + v * n + o * n2;
-        for(int p = 0; p < no[S]; ++p) h += Gov[occl[S * 128 + p]];
-        for(int p = 0; p < no[1 - S]; ++p) h += Vov[occl[(1 - S) * 128 + p]];
+        // loads 8 at a time, additions in the reference order
+        for(int p0 = 0; p0 < noS; p0 += 8) {
+          double g[8];
+#pragma unroll
+          for(int k = 0; k < 8; ++k)
+            g[k] = p0 + k < noS ? Gov[occl[S * 128 + p0 + k]] : 0.0;
+#pragma unroll
+          for(int k = 0; k < 8; ++k)
+            if(p0 + k < noS) h += g[k];
+        }
+        for(int p0 = 0; p0 < noO; p0 += 8) {
+          double g[8];
+#pragma unroll
+          for(int k = 0; k < 8; ++k)
+            g[k] = p0 + k < noO ? Vov[occl[(1 - S) * 128 + p0 + k]] : 0.0;
+#pragma unroll
+          for(int k = 0; k < 8; ++k)
+            if(p0 + k < noO) h += g[k];
+        }
         F[S * n2 + v * n + o] = h;
       }
     }
@@ -463,36 +487,59 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
     const int64_t out0 = rowptr[row];
     CI* __restrict__ rc = colind + out0;
     VT* __restrict__ rv = nzval + out0;
-    int32_t pos = 0, dropped = 0;
+    int32_t pos = 0, dropped = 0;  // dropped: this lane's count
     uint2 el = make_uint2(0u, 0u);  // this lane's entry of the beta L2 list
     if(lane < n2l)
       el = s2 ? sl2[lane]
               : make_uint2(uint32_t(__ldg(d.l2col + l2b + lane)),
                            __ldg(d.l2info + l2b + lane));
+    using CS = typename std::conditional<sizeof(CI) == 4, int, long long>::type;
+    CS* __restrict__ rcs = reinterpret_cast<CS*>(rc);
+    // entries whose column differs from the row (every phase but the
+    // same-alpha segment): no diagonal test
     auto put = [&](bool act, int32_t p, int32_t col, double h) {
-      const bool keep = act && fabs(h) > thresh;
-      dropped += __popc(__ballot_sync(0xffffffffu, act && !keep));
       if(act) {
+        const bool keep = fabs(h) > thresh;
+        dropped += !keep;
+        __stcs(rcs + p, CS(keep ? col : -1));
+        __stcs(rv + p, store_val<VT>(h, false));
+      }
+    };
+    auto put_d = [&](bool act, int32_t p, int32_t col, double h) {
+      if(act) {
+        const bool keep = fabs(h) > thresh;
+        dropped += !keep;
         const bool isd = keep && col == row;
-        __stcs(reinterpret_cast<typename std::conditional<
-                   sizeof(CI) == 4, int, long long>::type*>(rc) + p,
-               (typename std::conditional<sizeof(CI) == 4, int, long long>::type)(
-                   keep ? col : -1));
+        __stcs(rcs + p, CS(keep ? col : -1));
         __stcs(rv + p, store_val<VT>(h, isd));
         if(isd) diag[row] = h;
       }
     };
     const int64_t c1 = d.aoff[A + 1];
+    // the next chunk of the alpha list is loaded while this one is emitted
+    int32_t nx_col = 0;
+    uint32_t nx_ai = 0;
+    {
+      const int64_t j = d.aoff[A] + lane;
+      if(j < c1) {
+        nx_col = __ldg(d.acol + j);
+        nx_ai = __ldg(d.ainfo + j);
+      }
+    }
     for(int64_t c = d.aoff[A]; c < c1; c += 32) {
       const int64_t j = c + lane;
       int32_t colA = 0;
       uint32_t ai = 0;
       int cls = 3, cnt = 0;
       if(j < c1) {
-        colA = __ldg(d.acol + j) * UB;
-        ai = __ldg(d.ainfo + j);
+        colA = nx_col * UB;
+        ai = nx_ai;
         cls = int((ai >> 29) & 3u);
         cnt = cls == 0 ? n4l : cls == 1 ? n2l : 1;
+      }
+      if(j + 32 < c1) {
+        nx_col = __ldg(d.acol + j + 32);
+        nx_ai = __ldg(d.ainfo + j + 32);
       }
       const int incl = warp_incl_scan(cnt);
       const int32_t spos = pos + incl - cnt;
@@ -526,7 +573,7 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
             col = cA + int32_t(ent.x);
             h = cb == 0 ? hd : sgnd(ent.y, v);
           }
-          put(act, sp0 + t, col, h);
+          put_d(act, sp0 + t, col, h);
         }
       }
       // (3) alpha singles: one segment of n2l entries (beta within one
@@ -539,20 +586,29 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
         seg_col[wid][rk] = colA;
         const uint32_t pa_ = ai & 0x3FFFu;  // v1 + o1 n
         seg_a[wid][rk] = (ai & 0x80000000u) | (pa_ * uint32_t(n2));
-        seg_single[wid][rk] =
-            sgnd(ai, F[(pa_ % uint32_t(n)) * n + pa_ / uint32_t(n)]);
+        seg_single[wid][rk] = sgnd(ai, F[(ai >> 14) & 0x3FFFu]);
       }
       __syncwarp();
       const int k2 = __popc(m2);
-      {
-        const bool act = lane < n2l;
+      if(lane < n2l) {
+        // branch-free body: the same-beta entry (offset 0) also loads from
+        // its VT row and then selects the alpha-single value
         const bool bsame = ((el.y >> 29) & 3u) == 0;
         const uint32_t boff = el.y & 0x0FFFFFFFu, bsg = el.y & 0x80000000u;
+        const int32_t elx = int32_t(el.x);
+        CS* __restrict__ rcl = rcs + lane;
+        VT* __restrict__ rvl = rv + lane;
         for(int q = 0; q < k2; ++q) {
           const uint32_t sa = seg_a[wid][q];
+          const int32_t p = seg_pos[wid][q];
+          const int32_t cb = seg_col[wid][q];
+          const double sgl = seg_single[wid][q];
           const double v = __ldg(gVT + ((sa & 0x7FFFFFFFu) + boff));
-          const double h = bsame ? seg_single[wid][q] : sgnd(sa ^ bsg, v);
-          put(act, seg_pos[wid][q] + lane, seg_col[wid][q] + int32_t(el.x), h);
+          const double h = bsame ? sgl : sgnd(sa ^ bsg, v);
+          const bool keep = fabs(h) > thresh;
+          dropped += !keep;
+          __stcs(rcl + p, CS(keep ? cb + elx : -1));
+          __stcs(rvl + p, store_val<VT>(h, false));
         }
       }
       if(n2l > 32) {  // list entries 32.. of every segment, flattened
@@ -583,6 +639,9 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
       }
       __syncwarp();
     }
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+      dropped += __shfl_xor_sync(0xffffffffu, dropped, o);
     if(lane == 0) rowcnt[row] = int64_t(pos) - dropped;
   }
 }

@@ -43,6 +43,19 @@ def test_fci_direct_product_exact(ref, nbits):
         assert np.array_equal(A32.diagonal(), A.diagonal())
 
 
+@pytest.mark.parametrize("norb,na,nb", [(9, 3, 0), (8, 2, 8), (7, 1, 6),
+                                         (12, 6, 1)])
+def test_direct_product_edge_occupations(ref, norb, na, nb):
+    """Empty / full / single-electron beta strings: beta lists of one entry
+    (no beta excitation) and short lists."""
+    T, V, dets = fci(norb, na, nb, 64, seed=5)
+    H = mb.HamiltonianGenerator(T, V, 64)
+    A = mb.make_csr_hamiltonian(dets, H, np.finfo(float).eps)
+    assert A.build_stats()["direct_product"] == 1
+    assert_csr_equal(A.to_host(), ref.build_csr(
+        ref.ham(64, norb, T, V), dets, dets, np.finfo(float).eps, nthreads=4))
+
+
 def test_c1_fci_exact(ref):
     # CAS(10e,10o): 63,504 determinants
     T, V, dets = fci(10, 5, 5, 64, seed=0)
