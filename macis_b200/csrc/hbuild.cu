@@ -368,9 +368,9 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
               int64_t nrows) {
   constexpr int NSW = DetTraits<NBITS>::NSW;
   extern __shared__ __align__(16) unsigned char dsm[];
-  __shared__ int32_t seg_pos[DP_WARPS][32];
-  __shared__ int32_t seg_col[DP_WARPS][32];
-  __shared__ uint32_t seg_a[DP_WARPS][32];  // sign bit | VT row offset
+  // alpha-single segments of the current chunk: (row position, column
+  // base, sign bit | VT row offset, unused) and the alpha-single value
+  __shared__ int4 seg_d[DP_WARPS][32];
   __shared__ double seg_single[DP_WARPS][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int n = L.n;
@@ -567,11 +567,13 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
                                  : make_uint2(uint32_t(__ldg(d.l4col + l4b + t)),
                                               __ldg(d.l4info + l4b + t));
             const uint32_t cb = (ent.y >> 29) & 3u, off = ent.y & 0x0FFFFFFFu;
-            // one generic load: singles table (shared) or G (global)
-            const double* src = cb == 1 ? F + off : gG + off;
-            const double v = *src;
+            // singles from this row's table (shared), doubles from G: both
+            // loads issued, the class selects (offsets are in range for
+            // either array: singles < 2 n^2 <= n^4, doubles clamped)
+            const double vf = F[off < uint32_t(2 * n2) ? off : 0u];
+            const double vg = __ldg(gG + off);
             col = cA + int32_t(ent.x);
-            h = cb == 0 ? hd : sgnd(ent.y, v);
+            h = cb == 0 ? hd : sgnd(ent.y, cb == 1 ? vf : vg);
           }
           put_d(act, sp0 + t, col, h);
         }
@@ -582,10 +584,9 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
       const unsigned m2 = __ballot_sync(0xffffffffu, cls == 1);
       if(cls == 1) {
         const int rk = __popc(m2 & lanemask_lt());
-        seg_pos[wid][rk] = spos;
-        seg_col[wid][rk] = colA;
         const uint32_t pa_ = ai & 0x3FFFu;  // v1 + o1 n
-        seg_a[wid][rk] = (ai & 0x80000000u) | (pa_ * uint32_t(n2));
+        seg_d[wid][rk] = make_int4(spos, colA,
+                                   int((ai & 0x80000000u) | (pa_ * uint32_t(n2))), 0);
         seg_single[wid][rk] = sgnd(ai, F[(ai >> 14) & 0x3FFFu]);
       }
       __syncwarp();
@@ -599,9 +600,9 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
         CS* __restrict__ rcl = rcs + lane;
         VT* __restrict__ rvl = rv + lane;
         for(int q = 0; q < k2; ++q) {
-          const uint32_t sa = seg_a[wid][q];
-          const int32_t p = seg_pos[wid][q];
-          const int32_t cb = seg_col[wid][q];
+          const int4 sd = seg_d[wid][q];
+          const int32_t p = sd.x, cb = sd.y;
+          const uint32_t sa = uint32_t(sd.z);
           const double sgl = seg_single[wid][q];
           const double v = __ldg(gVT + ((sa & 0x7FFFFFFFu) + boff));
           const double h = bsame ? sgl : sgnd(sa ^ bsg, v);
@@ -615,26 +616,26 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
         const int32_t w2 = n2l - 32;
         const int32_t tot2 = k2 * w2;
         const float invw = 1.0f / float(w2);
-        for(int32_t e = lane; e - lane < tot2; e += 32) {
-          const bool act = e < tot2;
-          double h = 0;
-          int32_t col = 0, p = 0;
-          if(act) {
-            int sg = int(float(e) * invw);
-            if(sg * w2 > e) --sg;
-            if((sg + 1) * w2 <= e) ++sg;
-            const int32_t t = 32 + e - sg * w2;
-            const uint2 ent = s2 ? sl2[t]
-                                 : make_uint2(uint32_t(__ldg(d.l2col + l2b + t)),
-                                              __ldg(d.l2info + l2b + t));
-            const uint32_t sa = seg_a[wid][sg];
-            const double v = __ldg(gVT + ((sa & 0x7FFFFFFFu) + (ent.y & 0x0FFFFFFFu)));
-            h = ((ent.y >> 29) & 3u) == 0 ? seg_single[wid][sg]
-                                           : sgnd(sa ^ (ent.y & 0x80000000u), v);
-            col = seg_col[wid][sg] + int32_t(ent.x);
-            p = seg_pos[wid][sg] + t;
-          }
-          put(act, p, col, h);
+        for(int32_t e = lane; e < tot2; e += 32) {
+          int sg = int(float(e) * invw);
+          if(sg * w2 > e) --sg;
+          if((sg + 1) * w2 <= e) ++sg;
+          const int32_t t = 32 + e - sg * w2;
+          const uint2 ent = s2 ? sl2[t]
+                               : make_uint2(uint32_t(__ldg(d.l2col + l2b + t)),
+                                            __ldg(d.l2info + l2b + t));
+          const int4 sd = seg_d[wid][sg];
+          const uint32_t sa = uint32_t(sd.z);
+          const double sgl = seg_single[wid][sg];
+          const double v =
+              __ldg(gVT + ((sa & 0x7FFFFFFFu) + (ent.y & 0x0FFFFFFFu)));
+          const double h = ((ent.y >> 29) & 3u) == 0
+                               ? sgl
+                               : sgnd(sa ^ (ent.y & 0x80000000u), v);
+          const bool keep = fabs(h) > thresh;
+          dropped += !keep;
+          __stcs(rcs + sd.x + t, CS(keep ? sd.y + int32_t(ent.x) : -1));
+          __stcs(rv + sd.x + t, store_val<VT>(h, false));
         }
       }
       __syncwarp();
