@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
   constexpr int NSW = DetTraits<NBITS>::NSW;
   extern __shared__ __align__(16) unsigned char dsm[];
   // alpha-single segments of the current chunk: (row position, column
-  // base, sign bit | VT row offset, unused) and the alpha-single value
+  // base, VT row offset, sign bit) and the alpha-single value
   __shared__ int4 seg_d[DP_WARPS][32];
   __shared__ double seg_single[DP_WARPS][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -585,8 +585,8 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
       if(cls == 1) {
         const int rk = __popc(m2 & lanemask_lt());
         const uint32_t pa_ = ai & 0x3FFFu;  // v1 + o1 n
-        seg_d[wid][rk] = make_int4(spos, colA,
-                                   int((ai & 0x80000000u) | (pa_ * uint32_t(n2))), 0);
+        seg_d[wid][rk] = make_int4(spos, colA, int(pa_ * uint32_t(n2)),
+                                   int(ai & 0x80000000u));
         seg_single[wid][rk] = sgnd(ai, F[(ai >> 14) & 0x3FFFu]);
       }
       __syncwarp();
@@ -599,16 +599,19 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
         const int32_t elx = int32_t(el.x);
         CS* __restrict__ rcl = rcs + lane;
         VT* __restrict__ rvl = rv + lane;
+#pragma unroll 2
         for(int q = 0; q < k2; ++q) {
           const int4 sd = seg_d[wid][q];
-          const int32_t p = sd.x, cb = sd.y;
-          const uint32_t sa = uint32_t(sd.z);
           const double sgl = seg_single[wid][q];
-          const double v = __ldg(gVT + ((sa & 0x7FFFFFFFu) + boff));
-          const double h = bsame ? sgl : sgnd(sa ^ bsg, v);
+          const double v = __ldg(gVT + uint32_t(sd.z + int(boff)));
+          // sign of the element: one XOR on the high word
+          const double hv = __hiloint2double(
+              __double2hiint(v) ^ (sd.w ^ int(bsg)), __double2loint(v));
+          const double h = bsame ? sgl : hv;
           const bool keep = fabs(h) > thresh;
-          dropped += !keep;
-          __stcs(rcl + p, CS(keep ? cb + elx : -1));
+          dropped += keep ? 0 : 1;
+          const uint32_t p = uint32_t(sd.x);
+          __stcs(rcl + p, CS(keep ? sd.y + elx : -1));
           __stcs(rvl + p, store_val<VT>(h, false));
         }
       }
@@ -625,17 +628,17 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
                                : make_uint2(uint32_t(__ldg(d.l2col + l2b + t)),
                                             __ldg(d.l2info + l2b + t));
           const int4 sd = seg_d[wid][sg];
-          const uint32_t sa = uint32_t(sd.z);
           const double sgl = seg_single[wid][sg];
-          const double v =
-              __ldg(gVT + ((sa & 0x7FFFFFFFu) + (ent.y & 0x0FFFFFFFu)));
-          const double h = ((ent.y >> 29) & 3u) == 0
-                               ? sgl
-                               : sgnd(sa ^ (ent.y & 0x80000000u), v);
+          const double v = __ldg(gVT + uint32_t(sd.z + int(ent.y & 0x0FFFFFFFu)));
+          const double hv = __hiloint2double(
+              __double2hiint(v) ^ (sd.w ^ int(ent.y & 0x80000000u)),
+              __double2loint(v));
+          const double h = ((ent.y >> 29) & 3u) == 0 ? sgl : hv;
           const bool keep = fabs(h) > thresh;
-          dropped += !keep;
-          __stcs(rcs + sd.x + t, CS(keep ? sd.y + int32_t(ent.x) : -1));
-          __stcs(rv + sd.x + t, store_val<VT>(h, false));
+          dropped += keep ? 0 : 1;
+          const uint32_t p = uint32_t(sd.x + t);
+          __stcs(rcs + p, CS(keep ? sd.y + int32_t(ent.x) : -1));
+          __stcs(rv + p, store_val<VT>(h, false));
         }
       }
       __syncwarp();
