@@ -16,8 +16,10 @@
 //     resolved towards smaller determinants (determinant_search.hpp:622-626
 //     leaves them unspecified)
 //
-// Core dets are processed in batches sized to the free HBM; batch results are
-// merged into the running unique list by a merge-path style rank merge.
+// When the raw contributions do not fit in HBM at once, the candidate
+// determinants are split into ranges by a hash of the determinant; each
+// range is generated, sorted and accumulated on its own (its sums are
+// complete) and merged into a running top-k.
 #include <algorithm>
 #include <chrono>
 #include <cstdlib>
@@ -141,6 +143,22 @@ __device__ __forceinline__ void det_flip(uint64_t* d, int spin, int orb) {
   }
 }
 
+// Range of a candidate determinant when the search is partitioned into nr
+// ranges: a hash of its words scaled to [0, nr). Every contribution to one
+// determinant falls into the same range.
+template <int NW>
+__device__ __forceinline__ uint32_t det_range(const uint64_t* w, uint32_t nr) {
+  uint64_t h = 0x9E3779B97F4A7C15ull;
+#pragma unroll
+  for(int j = 0; j < NW; ++j) {
+    h ^= w[j];
+    h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
+    h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
+    h ^= h >> 31;
+  }
+  return uint32_t((uint64_t(uint32_t(h >> 32)) * nr) >> 32);
+}
+
 #define G2R(p, q) __ldg(I.G2_red + (p) + size_t(q) * n)
 #define V2R(p, q) __ldg(I.V2_red + (p) + size_t(q) * n)
 
@@ -186,7 +204,7 @@ template <int NBITS, int MODE>
 __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                          double E0, double tol, int64_t* count_out,
                          int64_t out0, uint64_t* keys, double* rv,
-                         float* umax) {
+                         float* umax, uint32_t nr, uint32_t rr) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
   const int lane = threadIdx.x & 31;
@@ -229,7 +247,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         for(int p = 0; p < nS; ++p) h += __ldg(Gov + occS[p]);
         for(int p = 0; p < nO; ++p) h += __ldg(Vov + occO[p]);
         keep = !(fabs(h) < tol);
-        if(MODE == 1 && keep) {
+        if((MODE == 1 || nr > 1) && keep) {
           const double* eps = S ? epsB : epsA;
           h *= ex_sign(S ? sB : sA, a, i);
           const double hd = hii + eps[a] - eps[i] - G2R(a, i) - G2R(i, a);
@@ -252,7 +270,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int i = occS[ii], a = virS[aa], j = occS[jj], b = virS[bb];
         const double Gv = __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
         keep = !(fabs(Gv) < tol);
-        if(MODE == 1 && keep) {
+        if((MODE == 1 || nr > 1) && keep) {
           const Spin<NSW> st = S ? sB : sA;
           Spin<NSW> fx = sp_flip(sp_flip(sp_flip(sp_flip(sp_zero<NSW>(), i), j), a), b);
           const uint32_t e = double_ex(st, st ^ fx);
@@ -277,7 +295,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int j = occB[q / nvB], b = virB[q % nvB];
         const double Vv = __ldg(I.V + a + size_t(i) * n + size_t(b + size_t(j) * n) * n * n);
         keep = !(fabs(Vv) < tol);
-        if(MODE == 1 && keep) {
+        if((MODE == 1 || nr > 1) && keep) {
           const double sign = ex_sign(sA, a, i) * ex_sign(sB, b, j);
           double h = sign * Vv;
           const double hd = hii + epsA[a] + epsB[b] - epsA[i] - epsB[j] +
@@ -294,6 +312,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         }
       }
     }
+    if(nr > 1 && keep) keep = det_range<D::NW>(ex, nr) == rr;
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     if(MODE == 1 && keep) {
       const int64_t pos = out0 + done + __popc(m & lanemask_lt());
@@ -309,7 +328,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1)
       mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if(lane == 0) *umax = mx;
+    if(lane == 0) *umax = fmaxf(*umax, mx);  // running max over ranges
   }
 }
 #undef G2R
@@ -320,7 +339,8 @@ template <int NBITS, int MODE>
 __global__ void __launch_bounds__(256)
     units_k(Ints I, CoreData cd, int64_t u0, int64_t u1, size_t c0, size_t c1,
             double E0, double tol, int64_t* counts, const int64_t* outoff,
-            uint64_t* keys, double* rv, const uint8_t* umask, float* umax) {
+            uint64_t* keys, double* rv, const uint8_t* umask, float* umax,
+            uint32_t nr, uint32_t rr) {
   const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
   for(int64_t u = u0 + int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
       u < u1; u += int64_t(nwarp)) {
@@ -340,7 +360,7 @@ __global__ void __launch_bounds__(256)
     const int64_t t = u - cd.uoff[lo];
     unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
                           MODE ? outoff[u - u0] : 0, keys, rv,
-                          umax ? umax + u : nullptr);
+                          umax ? umax + u : nullptr, nr, rr);
   }
 }
 
@@ -598,36 +618,6 @@ __global__ void seg_sum_k(const int64_t* start, size_t nseg, size_t n,
   }
 }
 
-// Rank of every key of X among Y (lower bound if before_ties, else upper).
-template <int NW>
-__global__ void merge_rank_k(const uint64_t* X, size_t nx, const uint64_t* Y,
-                             size_t ny, int upper, int64_t* pos) {
-  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nx;
-      i += size_t(gridDim.x) * blockDim.x) {
-    const Key<NW> k = load_key<NW>(X, i);
-    size_t lo = 0, hi = ny;
-    while(lo < hi) {
-      const size_t mid = (lo + hi) >> 1;
-      const int c = key_cmp<NW>(load_key<NW>(Y, mid), k);
-      if(c < 0 || (upper && c == 0))
-        lo = mid + 1;
-      else
-        hi = mid;
-    }
-    pos[i] = int64_t(i + lo);
-  }
-}
-template <int NW>
-__global__ void merge_scatter_k(const uint64_t* X, const double* xv, size_t nx,
-                                const int64_t* pos, uint64_t* out,
-                                double* ov) {
-  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nx;
-      i += size_t(gridDim.x) * blockDim.x) {
-    store_key<NW>(out, pos[i], load_key<NW>(X, i));
-    ov[pos[i]] = xv[i];
-  }
-}
-
 // --------------------------------------------------------- core / top-k
 template <int NW>
 __global__ void keep_flags_k(const uint64_t* keys, const double* rv, size_t n,
@@ -694,12 +684,23 @@ __global__ void select_flags_k(const double* rv, size_t n, uint64_t T,
     eq[i] = k == T;
   }
 }
-__global__ void select_final_k(const uint32_t* gt, const uint32_t* eq,
-                               const uint32_t* eqx, size_t n, uint64_t need,
-                               uint32_t* f) {
+// |rv| at or above the threshold bits T (candidates that stay in the running
+// top-k, ties included)
+__global__ void ge_flags_k(const double* rv, size_t n, uint64_t T,
+                           uint32_t* f) {
   for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
       i += size_t(gridDim.x) * blockDim.x)
-    f[i] = gt[i] || (eq[i] && eqx[i] < need);
+    f[i] = uint64_t(__double_as_longlong(fabs(rv[i]))) >= T ? 1u : 0u;
+}
+// final selection: everything above the threshold, and the ties whose
+// determinant is not above Kmax (the need-th smallest tied determinant)
+template <int NW>
+__global__ void tie_select_k(const uint64_t* keys, const uint32_t* gt,
+                             const uint32_t* eq, size_t n, Key<NW> Kmax,
+                             uint32_t* f) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x)
+    f[i] = gt[i] || (eq[i] && key_cmp<NW>(load_key<NW>(keys, i), Kmax) <= 0);
 }
 
 // ----------------------------------------------------------------- driver
@@ -709,6 +710,25 @@ struct Pairs {
   double* rv = nullptr;
   size_t n = 0;
 };
+// Device bytes that allocations can still obtain: free memory plus what the
+// default stream-ordered pool holds without using it.
+size_t device_bytes_available() {
+  size_t freeb = 0, totb = 0;
+  MB_CUDA(cudaMemGetInfo(&freeb, &totb));
+  int dev = 0;
+  MB_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  if(cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long res = 0, used = 0;  // the attributes are 64-bit
+    if(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res) ==
+           cudaSuccess &&
+       cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) ==
+           cudaSuccess &&
+       res > used)
+      freeb += size_t(res - used);
+  }
+  return freeb;
+}
 double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(
              std::chrono::steady_clock::now() - t)
@@ -861,237 +881,59 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   if(U)
     units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
         I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt, nullptr, nullptr,
-        nullptr, umask, nullptr), note_launch();
+        nullptr, umask, nullptr, 1u, 0u), note_launch();
   int64_t* uout = A.get<int64_t>(U + 1);
   exclusive_scan<int64_t, int64_t>(ucnt, uout, size_t(U), uout + U, A);
   const int64_t Ptot = U ? to_host(uout + U, s) : 0;
   stats.raw_pairs = uint64_t(Ptot);
 
-  // per-det raw counts on the host to form batches
-  std::vector<int64_t> h_uoff(ncdets + 1), h_uout;
-  if(ncdets) {
-    MB_CUDA(cudaMemcpyAsync(h_uoff.data(), cd.uoff, (ncdets + 1) * 8,
-                            cudaMemcpyDeviceToHost, s));
-    h_uout.resize(U + 1);
-    MB_CUDA(cudaMemcpyAsync(h_uout.data(), uout, (U + 1) * 8,
-                            cudaMemcpyDeviceToHost, s));
-    MB_CUDA(cudaStreamSynchronize(s));
-  }
-  size_t freeb = 0, totb = 0;
-  MB_CUDA(cudaMemGetInfo(&freeb, &totb));
-  // raw record + sort scratch + flags ~ 2.6 x (NW*8 + 8) + 16 bytes
-  const size_t rec = size_t(2.6 * (NW * 8 + 8)) + 16;
-  int64_t cap = int64_t(double(freeb) * 0.45 / double(rec));
-  cap = std::max<int64_t>(cap, int64_t(1) << 20);
-  cap = std::min<int64_t>(cap, int64_t(1) << 31);
-  // MACIS_B200_ASCI_BATCH_PAIRS caps the raw pairs per batch (exercises the
-  // batch merge on small problems).
-  if(const char* e = getenv("MACIS_B200_ASCI_BATCH_PAIRS"))
+  // The candidate determinants are split into nr ranges by a hash of the
+  // determinant, sized so that one range's raw contributions fit in memory.
+  // Every contribution to a determinant lands in its range, so each range's
+  // accumulated scores are complete (summed in generation order, as in the
+  // unpartitioned search) and the range can go straight into the running
+  // top-k: memory stays bounded by one range plus ~ndets_max candidates.
+  const double rs = double(NW * 8 + 8);
+  const double per_pair = 3.0 * rs + 20.0;  // record, sort copy, flags, sums
+  const size_t topk = ndets_max - ncdets;   // size_t arithmetic (:547)
+  const double keep_reserve =
+      6.0 * rs * double(std::min<uint64_t>(topk, uint64_t(Ptot)));
+  // MACIS_B200_ASCI_BATCH_PAIRS caps the raw pairs per range (exercises the
+  // partitioned path on small problems).
+  int64_t cap = 0;
+  if(const char* e = getenv("MACIS_B200_ASCI_BATCH_PAIRS")) {
     cap = std::max<int64_t>(1, atoll(e));
+  } else {
+    cap = int64_t((0.8 * double(device_bytes_available()) - keep_reserve) /
+                  per_pair);
+    cap = std::min<int64_t>(std::max<int64_t>(cap, int64_t(1) << 20),
+                            int64_t(1) << 31);
+  }
+  uint32_t nr = uint32_t(std::max<int64_t>(1, (Ptot + cap - 1) / cap));
+  if(pairs_only) nr = 1;  // the full accumulated list is the result
+  stats.batches = nr;
   stats.pairs_ms = ms_since(t_all);
 
-  Pairs acc;  // running unique list (sorted)
-  double sort_ms = 0, pair_ms = 0;
-  size_t c0 = 0;
-  while(c0 < ncdets) {
-    // grow the batch while its raw count fits
-    size_t c1 = c0 + 1;
-    while(c1 < ncdets &&
-          h_uout[h_uoff[c1 + 1]] - h_uout[h_uoff[c0]] <= cap)
-      ++c1;
-    const int64_t u0 = h_uoff[c0], u1 = h_uoff[c1];
-    const int64_t p0 = h_uout[u0], P = h_uout[u1] - p0;
-    stats.batches++;
-    auto tb = std::chrono::steady_clock::now();
-    Arena B(s);
-    uint64_t* keys = B.get<uint64_t>(size_t(P) * NW + NW);
-    double* rv = B.get<double>(size_t(P) + 1);
-    if(P) {
-      // offsets relative to the batch
-      int64_t* boff = B.get<int64_t>(size_t(u1 - u0) + 1);
-      exclusive_scan<int64_t, int64_t>(ucnt + u0, boff, size_t(u1 - u0),
-                                       nullptr, B);
-      units_k<NBITS, 1><<<grid_for(size_t(u1 - u0) * 32, 256, 32 * sms), 256,
-                          0, s>>>(I, cd, u0, u1, c0, c1, E0, st.h_el_tol,
-                                  ucnt + u0, boff, keys, rv, umask, umax),
-          note_launch();
-      MB_CUDA(cudaGetLastError());
-    }
-    MB_CUDA(cudaStreamSynchronize(s));
-    pair_ms += ms_since(tb);
-    tb = std::chrono::steady_clock::now();
-    Pairs bat;
-    if(P) {
-      uint64_t* k2 = B.get<uint64_t>(size_t(P) * NW + NW);
-      double* r2 = B.get<double>(size_t(P) + 1);
-      radix_sort<NW, double>(keys, rv, k2, r2, size_t(P), B);
-      uint32_t* f = B.get<uint32_t>(size_t(P) + 1);
-      uint32_t* fx = B.get<uint32_t>(size_t(P) + 1);
-      seg_flags_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
-          keys, size_t(P), f), note_launch();
-      exclusive_scan<uint32_t, uint32_t>(f, fx, size_t(P), fx + P, B);
-      const uint32_t nu = to_host(fx + P, s);
-      int64_t* start = B.get<int64_t>(nu + 1);
-      // unique keys reuse k2, sums reuse r2
-      seg_starts_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
-          f, fx, size_t(P), start, keys, k2), note_launch();
-      seg_sum_k<<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(start, nu,
-                                                            size_t(P), rv, r2), note_launch();
-      // move into A-owned storage
-      bat.n = nu;
-      bat.keys = A.get<uint64_t>(size_t(nu) * NW + NW);
-      bat.rv = A.get<double>(size_t(nu) + 1);
-      MB_CUDA(cudaMemcpyAsync(bat.keys, k2, size_t(nu) * NW * 8,
-                              cudaMemcpyDeviceToDevice, s));
-      MB_CUDA(cudaMemcpyAsync(bat.rv, r2, size_t(nu) * 8,
-                              cudaMemcpyDeviceToDevice, s));
-    }
-    if(acc.n == 0) {
-      acc = bat;
-    } else if(bat.n) {
-      // merge two sorted unique lists, then add equal neighbours (acc first)
-      const size_t nm = acc.n + bat.n;
-      int64_t* pa = B.get<int64_t>(acc.n);
-      int64_t* pb = B.get<int64_t>(bat.n);
-      merge_rank_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
-          acc.keys, acc.n, bat.keys, bat.n, 0, pa), note_launch();
-      merge_rank_k<NW><<<grid_for(bat.n, 256, 16 * sms), 256, 0, s>>>(
-          bat.keys, bat.n, acc.keys, acc.n, 1, pb), note_launch();
-      uint64_t* mk = B.get<uint64_t>(nm * NW + NW);
-      double* mr = B.get<double>(nm + 1);
-      merge_scatter_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
-          acc.keys, acc.rv, acc.n, pa, mk, mr), note_launch();
-      merge_scatter_k<NW><<<grid_for(bat.n, 256, 16 * sms), 256, 0, s>>>(
-          bat.keys, bat.rv, bat.n, pb, mk, mr), note_launch();
-      uint32_t* f = B.get<uint32_t>(nm + 1);
-      uint32_t* fx = B.get<uint32_t>(nm + 1);
-      seg_flags_k<NW><<<grid_for(nm, 256, 16 * sms), 256, 0, s>>>(mk, nm, f), note_launch();
-      exclusive_scan<uint32_t, uint32_t>(f, fx, nm, fx + nm, B);
-      const uint32_t nu = to_host(fx + nm, s);
-      int64_t* start = B.get<int64_t>(nu + 1);
-      Pairs m2;
-      m2.n = nu;
-      m2.keys = A.get<uint64_t>(size_t(nu) * NW + NW);
-      m2.rv = A.get<double>(size_t(nu) + 1);
-      seg_starts_k<NW><<<grid_for(nm, 256, 16 * sms), 256, 0, s>>>(
-          f, fx, nm, start, mk, m2.keys), note_launch();
-      seg_sum_k<<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(start, nu, nm, mr,
-                                                           m2.rv), note_launch();
-      A.release(acc.keys);
-      A.release(acc.rv);
-      A.release(bat.keys);
-      A.release(bat.rv);
-      acc = m2;
-    }
-    // pruning when the list outgrows pair_size_max (determinant_search.hpp:
-    // 121-137), applied to the running sums
-    if(acc.n > st.pair_size_max) {
-      uint32_t* f = B.get<uint32_t>(acc.n + 1);
-      uint32_t* fx = B.get<uint32_t>(acc.n + 1);
-      prune_flags_k<<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
-          acc.rv, acc.n, st.rv_prune_tol, f), note_launch();
-      exclusive_scan<uint32_t, uint32_t>(f, fx, acc.n, fx + acc.n, B);
-      const uint32_t nk = to_host(fx + acc.n, s);
-      Pairs p2;
-      p2.n = nk;
-      p2.keys = A.get<uint64_t>(size_t(nk) * NW + NW);
-      p2.rv = A.get<double>(size_t(nk) + 1);
-      compact_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
-          acc.keys, acc.rv, acc.n, f, fx, p2.keys, p2.rv), note_launch();
-      A.release(acc.keys);
-      A.release(acc.rv);
-      acc = p2;
-    }
-    MB_CUDA(cudaStreamSynchronize(s));
-    sort_ms += ms_since(tb);
-    c0 = c1;
-  }
-  stats.unique_pairs = acc.n;
-  stats.pairs_ms += pair_ms;
-  stats.sort_ms = sort_ms;
-
-  // ---------------------------- (unit features, exact log score) samples
-  if(record) {
-    t_scr = std::chrono::steady_clock::now();
-    const size_t cap = size_t(scr->max_samples);
-    const double cand = double(stats.units_kept);
-    const double frac = double(cap) / std::max(cand, 1.0);
-    const uint64_t p =
-        frac >= 1.0 ? ~uint64_t(0) : uint64_t(frac * 18446744073709551616.0);
-    uint32_t* f = A.get<uint32_t>(size_t(U) + 1);
-    uint32_t* fx = A.get<uint32_t>(size_t(U) + 1);
-    sample_flags_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
-        umask, size_t(U), p, scr->seed + 1, f), note_launch();
-    exclusive_scan<uint32_t, uint32_t>(f, fx, size_t(U), fx + U, A);
-    const size_t nrec = std::min<size_t>(to_host(fx + U, s), cap);
-    int64_t* list = A.get<int64_t>(nrec + 1);
-    sample_list_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
-        f, fx, size_t(U), nrec, list), note_launch();
-    MB_CUDA(cudaStreamSynchronize(s));
-    mlp_reserve_samples(net, cap);
-    if(nrec)
-      unit_rows_k<NBITS><<<grid_for(nrec, 128, 16 * sms), 128, 0, s>>>(
-          cd, E0, list, 0, nrec, net->xs, umax, net->ts), note_launch();
-    MB_CUDA(cudaGetLastError());
-    MB_CUDA(cudaStreamSynchronize(s));
-    net->ns = nrec;
-    stats.samples = nrec;
-    stats.screen_ms += ms_since(t_scr);
-  }
-
-  if(pairs_only) {
-    ps->resize(acc.n * NW);
-    pr->resize(acc.n);
-    if(acc.n) {
-      MB_CUDA(cudaMemcpyAsync(ps->data(), acc.keys, acc.n * NW * 8,
-                              cudaMemcpyDeviceToHost, s));
-      MB_CUDA(cudaMemcpyAsync(pr->data(), acc.rv, acc.n * 8,
-                              cudaMemcpyDeviceToHost, s));
-    }
-    MB_CUDA(cudaStreamSynchronize(s));
-    h->last_asci = stats;
-    return;
-  }
-
-  // ------------------------------------------- drop core dets, zero scores
-  auto tk = std::chrono::steady_clock::now();
+  // sorted core dets (dropped from the candidates)
   uint64_t* core = A.get<uint64_t>(ncdets * NW + NW);
   if(ncdets) {
     uint64_t* ct = A.get<uint64_t>(ncdets * NW + NW);
     MB_CUDA(cudaMemcpyAsync(core, cdets, ncdets * NW * 8,
                             cudaMemcpyDeviceToDevice, s));
     radix_sort<NW, uint32_t>(core, nullptr, ct, nullptr, ncdets, A);
+    A.release(ct);
   }
-  Pairs kept;
-  if(acc.n) {
-    uint32_t* f = A.get<uint32_t>(acc.n + 1);
-    uint32_t* fx = A.get<uint32_t>(acc.n + 1);
-    keep_flags_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
-        acc.keys, acc.rv, acc.n, core, ncdets, f), note_launch();
-    exclusive_scan<uint32_t, uint32_t>(f, fx, acc.n, fx + acc.n, A);
-    kept.n = to_host(fx + acc.n, s);
-    kept.keys = A.get<uint64_t>(kept.n * NW + NW);
-    kept.rv = A.get<double>(kept.n + 1);
-    compact_k<NW><<<grid_for(acc.n, 256, 16 * sms), 256, 0, s>>>(
-        acc.keys, acc.rv, acc.n, f, fx, kept.keys, kept.rv), note_launch();
-  }
-  stats.kept_pairs = kept.n;
-  stats.keep_ms = ms_since(tk);
 
-  // ------------------------------------------------------------- top-k
-  auto tt = std::chrono::steady_clock::now();
-  const size_t topk = ndets_max - ncdets;  // size_t arithmetic (:547)
-  size_t nsel = kept.n;
-  uint32_t* sel = nullptr;
-  uint32_t* selx = nullptr;
-  if(kept.n > topk) {
+  // MSD radix select on |rv| bits: the bits T of the topk-th largest score
+  // and how many entries equal to T still belong to the top-k.
+  auto kth_bits = [&](const double* rv, size_t n, uint64_t want,
+                      uint64_t* need_out) {
     auto* hist = A.get<unsigned long long>(256);
-    uint64_t prefix = 0, mask = 0;
-    uint64_t need = topk;  // still to take from the current prefix bucket
+    uint64_t prefix = 0, mask = 0, need = want;
     for(int shift = 56; shift >= 0; shift -= 8) {
       MB_CUDA(cudaMemsetAsync(hist, 0, 256 * 8, s));
-      select_hist_k<<<grid_for(kept.n, 256, 8 * sms), 256, 0, s>>>(
-          kept.rv, kept.n, prefix, mask, shift, hist), note_launch();
+      select_hist_k<<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(
+          rv, n, prefix, mask, shift, hist), note_launch();
       unsigned long long hh[256];
       MB_CUDA(cudaMemcpyAsync(hh, hist, sizeof(hh), cudaMemcpyDeviceToHost, s));
       MB_CUDA(cudaStreamSynchronize(s));
@@ -1103,32 +945,243 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       prefix |= uint64_t(d) << shift;
       mask |= uint64_t(255) << shift;
     }
-    // prefix = k-th largest |rv| bits; take all > T and the first `need`
-    // equal ones in ascending determinant order
-    uint32_t* gt = A.get<uint32_t>(kept.n + 1);
-    uint32_t* eq = A.get<uint32_t>(kept.n + 1);
-    uint32_t* eqx = A.get<uint32_t>(kept.n + 1);
-    select_flags_k<<<grid_for(kept.n, 256, 16 * sms), 256, 0, s>>>(
-        kept.rv, kept.n, prefix, gt, eq), note_launch();
-    exclusive_scan<uint32_t, uint32_t>(eq, eqx, kept.n, eqx + kept.n, A);
-    sel = A.get<uint32_t>(kept.n + 1);
-    selx = A.get<uint32_t>(kept.n + 1);
-    select_final_k<<<grid_for(kept.n, 256, 16 * sms), 256, 0, s>>>(
-        gt, eq, eqx, kept.n, need, sel), note_launch();
-    exclusive_scan<uint32_t, uint32_t>(sel, selx, kept.n, selx + kept.n, A);
-    nsel = to_host(selx + kept.n, s);
+    A.release(hist);
+    *need_out = need;
+    return prefix;
+  };
+  // keep the flagged entries of (keys, rv, n) in new A-owned arrays
+  auto compact_to = [&](Arena& W, const uint64_t* keys, const double* rv,
+                        size_t n, const uint32_t* f) {
+    uint32_t* fx = W.get<uint32_t>(n + 1);
+    exclusive_scan<uint32_t, uint32_t>(f, fx, n, fx + n, W);
+    Pairs o;
+    o.n = to_host(fx + n, s);
+    o.keys = A.get<uint64_t>(o.n * NW + NW);
+    o.rv = A.get<double>(o.n + 1);
+    if(n)
+      compact_k<NW><<<grid_for(n, 256, 16 * sms), 256, 0, s>>>(
+          keys, rv, n, f, fx, o.keys, o.rv), note_launch();
+    W.release(fx);
+    return o;
+  };
+
+  Pairs surv;  // running top-k candidates (ties at the threshold included)
+  uint64_t uniq_total = 0, kept_total = 0;
+  double sort_ms = 0, pair_ms = 0, keep_ms = 0;
+  for(uint32_t rr = 0; rr < nr; ++rr) {
+    auto tb = std::chrono::steady_clock::now();
+    Arena B(s);
+    int64_t* rc = ucnt;
+    int64_t* off = uout;
+    int64_t P = Ptot;
+    if(nr > 1) {
+      rc = B.get<int64_t>(U + 1);
+      off = B.get<int64_t>(U + 1);
+      units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
+          I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, nullptr, nullptr,
+          nullptr, umask, nullptr, nr, rr), note_launch();
+      exclusive_scan<int64_t, int64_t>(rc, off, size_t(U), off + U, B);
+      P = to_host(off + U, s);
+    }
+    uint64_t* keys = B.get<uint64_t>(size_t(P) * NW + NW);
+    double* rv = B.get<double>(size_t(P) + 1);
+    if(P) {
+      units_k<NBITS, 1><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
+          I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, off, keys, rv, umask,
+          umax, nr, rr), note_launch();
+      MB_CUDA(cudaGetLastError());
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    pair_ms += ms_since(tb);
+    tb = std::chrono::steady_clock::now();
+    // sort + accumulate (stable: duplicates summed in generation order)
+    Pairs uq;
+    uint64_t* k2 = nullptr;
+    double* r2 = nullptr;
+    if(P) {
+      k2 = B.get<uint64_t>(size_t(P) * NW + NW);
+      r2 = B.get<double>(size_t(P) + 1);
+      radix_sort<NW, double>(keys, rv, k2, r2, size_t(P), B);
+      uint32_t* f = B.get<uint32_t>(size_t(P) + 1);
+      uint32_t* fx = B.get<uint32_t>(size_t(P) + 1);
+      seg_flags_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
+          keys, size_t(P), f), note_launch();
+      exclusive_scan<uint32_t, uint32_t>(f, fx, size_t(P), fx + P, B);
+      const uint32_t nu = to_host(fx + P, s);
+      int64_t* start = B.get<int64_t>(nu + 1);
+      // unique keys into k2, sums into r2
+      seg_starts_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
+          f, fx, size_t(P), start, keys, k2), note_launch();
+      seg_sum_k<<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(
+          start, nu, size_t(P), rv, r2), note_launch();
+      for(void* q : {static_cast<void*>(f), static_cast<void*>(fx),
+                     static_cast<void*>(start)})
+        B.release(q);
+      uq.keys = k2;
+      uq.rv = r2;
+      uq.n = nu;
+    }
+    uniq_total += uq.n;
+    // pruning when the accumulated lists outgrow pair_size_max
+    // (determinant_search.hpp:121-137)
+    if(uq.n && uniq_total > st.pair_size_max) {
+      uint32_t* f = B.get<uint32_t>(uq.n + 1);
+      prune_flags_k<<<grid_for(uq.n, 256, 16 * sms), 256, 0, s>>>(
+          uq.rv, uq.n, st.rv_prune_tol, f), note_launch();
+      Pairs p2 = compact_to(B, uq.keys, uq.rv, uq.n, f);
+      uq = p2;  // A-owned now
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    sort_ms += ms_since(tb);
+
+    if(pairs_only) {  // nr == 1: the accumulated list is the answer
+      ps->resize(uq.n * NW);
+      pr->resize(uq.n);
+      if(uq.n) {
+        MB_CUDA(cudaMemcpyAsync(ps->data(), uq.keys, uq.n * NW * 8,
+                                cudaMemcpyDeviceToHost, s));
+        MB_CUDA(cudaMemcpyAsync(pr->data(), uq.rv, uq.n * 8,
+                                cudaMemcpyDeviceToHost, s));
+      }
+      MB_CUDA(cudaStreamSynchronize(s));
+      continue;
+    }
+    // drop core dets and zero scores (keep_only_largest_copy_asci_pairs +
+    // partition, determinant_sort.hpp:86-120, determinant_search.hpp:528-544)
+    tb = std::chrono::steady_clock::now();
+    Pairs kept;
+    if(uq.n) {
+      uint32_t* f = B.get<uint32_t>(uq.n + 1);
+      keep_flags_k<NW><<<grid_for(uq.n, 256, 16 * sms), 256, 0, s>>>(
+          uq.keys, uq.rv, uq.n, core, ncdets, f), note_launch();
+      kept = compact_to(B, uq.keys, uq.rv, uq.n, f);
+    }
+    kept_total += kept.n;
+    // running top-k: survivors + this range, cut at the topk-th score (all
+    // entries tied with it stay)
+    Pairs cat;
+    cat.n = surv.n + kept.n;
+    cat.keys = A.get<uint64_t>(cat.n * NW + NW);
+    cat.rv = A.get<double>(cat.n + 1);
+    if(surv.n) {
+      MB_CUDA(cudaMemcpyAsync(cat.keys, surv.keys, surv.n * NW * 8,
+                              cudaMemcpyDeviceToDevice, s));
+      MB_CUDA(cudaMemcpyAsync(cat.rv, surv.rv, surv.n * 8,
+                              cudaMemcpyDeviceToDevice, s));
+      A.release(surv.keys);
+      A.release(surv.rv);
+    }
+    if(kept.n) {
+      MB_CUDA(cudaMemcpyAsync(cat.keys + surv.n * NW, kept.keys,
+                              kept.n * NW * 8, cudaMemcpyDeviceToDevice, s));
+      MB_CUDA(cudaMemcpyAsync(cat.rv + surv.n, kept.rv, kept.n * 8,
+                              cudaMemcpyDeviceToDevice, s));
+      A.release(kept.keys);
+      A.release(kept.rv);
+    }
+    if(uq.keys != k2) {  // pruned copy lives in A
+      A.release(uq.keys);
+      A.release(uq.rv);
+    }
+    if(cat.n > topk) {
+      uint64_t need = 0;
+      const uint64_t T = kth_bits(cat.rv, cat.n, topk, &need);
+      uint32_t* f = B.get<uint32_t>(cat.n + 1);
+      ge_flags_k<<<grid_for(cat.n, 256, 16 * sms), 256, 0, s>>>(
+          cat.rv, cat.n, T, f), note_launch();
+      surv = compact_to(B, cat.keys, cat.rv, cat.n, f);
+      A.release(cat.keys);
+      A.release(cat.rv);
+    } else {
+      surv = cat;
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    keep_ms += ms_since(tb);
   }
+  stats.unique_pairs = uniq_total;
+  stats.kept_pairs = kept_total;
+  stats.pairs_ms += pair_ms;
+  stats.sort_ms = sort_ms;
+  stats.keep_ms = keep_ms;
+
+  // ---------------------------- (unit features, exact log score) samples
+  if(record) {
+    t_scr = std::chrono::steady_clock::now();
+    const size_t rcap = size_t(scr->max_samples);
+    const double cand = double(stats.units_kept);
+    const double frac = double(rcap) / std::max(cand, 1.0);
+    const uint64_t p =
+        frac >= 1.0 ? ~uint64_t(0) : uint64_t(frac * 18446744073709551616.0);
+    uint32_t* f = A.get<uint32_t>(size_t(U) + 1);
+    uint32_t* fx = A.get<uint32_t>(size_t(U) + 1);
+    sample_flags_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
+        umask, size_t(U), p, scr->seed + 1, f), note_launch();
+    exclusive_scan<uint32_t, uint32_t>(f, fx, size_t(U), fx + U, A);
+    const size_t nrec = std::min<size_t>(to_host(fx + U, s), rcap);
+    int64_t* list = A.get<int64_t>(nrec + 1);
+    sample_list_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
+        f, fx, size_t(U), nrec, list), note_launch();
+    MB_CUDA(cudaStreamSynchronize(s));
+    mlp_reserve_samples(net, rcap);
+    if(nrec)
+      unit_rows_k<NBITS><<<grid_for(nrec, 128, 16 * sms), 128, 0, s>>>(
+          cd, E0, list, 0, nrec, net->xs, umax, net->ts), note_launch();
+    MB_CUDA(cudaGetLastError());
+    MB_CUDA(cudaStreamSynchronize(s));
+    net->ns = nrec;
+    stats.samples = nrec;
+    stats.screen_ms += ms_since(t_scr);
+  }
+
+  if(pairs_only) {
+    h->last_asci = stats;
+    return;
+  }
+
+  // ------------------------------------------------------------- top-k
+  // Ties at the topk-th score go to the smaller determinants
+  // (determinant_search.hpp:622-626 leaves them unspecified); the result is
+  // returned in ascending determinant order.
+  auto tt = std::chrono::steady_clock::now();
+  Pairs selp = surv;
+  if(surv.n > topk) {
+    uint64_t need = 0;
+    const uint64_t T = kth_bits(surv.rv, surv.n, topk, &need);
+    uint32_t* gt = A.get<uint32_t>(surv.n + 1);
+    uint32_t* eq = A.get<uint32_t>(surv.n + 1);
+    select_flags_k<<<grid_for(surv.n, 256, 16 * sms), 256, 0, s>>>(
+        surv.rv, surv.n, T, gt, eq), note_launch();
+    // the need-th smallest tied determinant
+    uint32_t* eqx = A.get<uint32_t>(surv.n + 1);
+    exclusive_scan<uint32_t, uint32_t>(eq, eqx, surv.n, eqx + surv.n, A);
+    const uint32_t neq = to_host(eqx + surv.n, s);
+    Key<NW> kmax;
+    {
+      uint64_t* ek = A.get<uint64_t>(size_t(neq) * NW + NW);
+      uint64_t* ek2 = A.get<uint64_t>(size_t(neq) * NW + NW);
+      double* dummy = A.get<double>(neq + 1);
+      compact_k<NW><<<grid_for(surv.n, 256, 16 * sms), 256, 0, s>>>(
+          surv.keys, surv.rv, surv.n, eq, eqx, ek, dummy), note_launch();
+      radix_sort<NW, uint32_t>(ek, nullptr, ek2, nullptr, neq, A);
+      MB_REQUIRE(need >= 1 && need <= neq, MACIS_B200_EINVAL,
+                 "internal: tie count out of range in the top-k selection");
+      MB_CUDA(cudaMemcpyAsync(kmax.w, ek + (need - 1) * NW, NW * 8,
+                              cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaStreamSynchronize(s));
+    }
+    uint32_t* sel = A.get<uint32_t>(surv.n + 1);
+    tie_select_k<NW><<<grid_for(surv.n, 256, 16 * sms), 256, 0, s>>>(
+        surv.keys, gt, eq, surv.n, kmax, sel), note_launch();
+    selp = compact_to(A, surv.keys, surv.rv, surv.n, sel);
+  }
+  const size_t nsel = selp.n;
   MB_REQUIRE(nsel <= ndets_max, MACIS_B200_ECAPACITY,
              "ASCI search result exceeds ndets_max + ncdets determinants");
   if(nsel) {
-    if(sel) {
-      double* tmp = A.get<double>(nsel + 1);
-      compact_k<NW><<<grid_for(kept.n, 256, 16 * sms), 256, 0, s>>>(
-          kept.keys, kept.rv, kept.n, sel, selx, out_dets, tmp), note_launch();
-    } else {
-      MB_CUDA(cudaMemcpyAsync(out_dets, kept.keys, nsel * NW * 8,
-                              cudaMemcpyDeviceToDevice, s));
-    }
+    uint64_t* k2 = A.get<uint64_t>(nsel * NW + NW);
+    radix_sort<NW, uint32_t>(selp.keys, nullptr, k2, nullptr, nsel, A);
+    MB_CUDA(cudaMemcpyAsync(out_dets, selp.keys, nsel * NW * 8,
+                            cudaMemcpyDeviceToDevice, s));
   }
   if(ncdets)
     MB_CUDA(cudaMemcpyAsync(out_dets + nsel * NW, cdets, ncdets * NW * 8,

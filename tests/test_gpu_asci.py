@@ -122,18 +122,34 @@ def test_search_edge_cases(port, wcase):
     assert len(got) == 0
 
 
-def test_search_batched_merge(port, wcase, monkeypatch):
+def test_search_partitioned_ranges(port, wcase, monkeypatch):
+    """Splitting the candidates into hash ranges (forced small here) gives
+    the unpartitioned result exactly: each range holds complete sums and the
+    running top-k keeps every tie until the end."""
     norb, T, V, hp, cd, cc, E = wcase
-    monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", "50000")
     H = mb.HamiltonianGenerator(T, V, 64, norb)
-    st, rv = mb.asci_pairs(_settings(), cd, E, cc, H)
-    assert mb.last_search_stats(H)["batches"] > 1
-    so, ro = port.asci_pairs(hp, oracle.AsciSettings.default(), cd, E, cc)
-    assert np.array_equal(st, so)
-    np.testing.assert_allclose(rv, ro, rtol=1e-12, atol=1e-15 * np.abs(ro).max())
+    one = mb.asci_search(_settings(), 5000, cd, E, cc, norb, H)
+    assert mb.last_search_stats(H)["batches"] == 1
+    net = mb.ScreeningNetwork(nbits=64, seed=0)
+    rec = mb.ScreenSettings(network=net, max_samples=10 ** 6)
+    mb.asci_search(_settings(), 5000, cd, E, cc, norb, H, screen=rec)
+    X1, t1 = net.samples()
+    monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", "50000")
     got = mb.asci_search(_settings(), 5000, cd, E, cc, norb, H)
+    st = mb.last_search_stats(H)
+    assert st["batches"] > 1
+    assert np.array_equal(got, one)
     exp = port.asci_search(hp, oracle.AsciSettings.default(), 5000, cd, E, cc)
-    assert len(_tuples(got) ^ _tuples(exp)) <= 2
+    assert np.array_equal(got, exp)
+    # per-unit recorded targets are the maximum over all ranges
+    mb.asci_search(_settings(), 5000, cd, E, cc, norb, H, screen=rec)
+    X2, t2 = net.samples()
+    assert np.array_equal(X1, X2) and np.array_equal(t1, t2)
+    # tiny top-k: ties resolved towards smaller determinants in both modes
+    got_small = mb.asci_search(_settings(), len(cd) + 7, cd, E, cc, norb, H)
+    monkeypatch.delenv("MACIS_B200_ASCI_BATCH_PAIRS")
+    one_small = mb.asci_search(_settings(), len(cd) + 7, cd, E, cc, norb, H)
+    assert np.array_equal(got_small, one_small)
 
 
 def test_water_grow_refine_golden():
