@@ -339,7 +339,7 @@ int davidson_device(const macis_b200_csr* A, int64_t max_m, double tol,
   double* tmp = restart_keep ? Ar.get<double>(size_t(N) * restart_keep) : nullptr;
   DavCtx ctx(s, N, Ar);
   MB_CUDA(cudaMemcpyAsync(V, X, N * 8, cudaMemcpyDeviceToDevice, s));
-  spmv_device(A, 1.0, V, 0.0, AV, s);
+  spmv_device_x64(A, 1.0, V, 0.0, AV, s);
   MB_CUDA(cudaMemcpyAsync(V + N, AV, N * 8, cudaMemcpyDeviceToDevice, s));
   ctx.cgs2(V, 1, V + N);
 
@@ -358,7 +358,7 @@ int davidson_device(const macis_b200_csr* A, int64_t max_m, double tol,
   int64_t i = 1;  // index of the newest basis vector (AV_i not yet formed)
   for(;; ++iter) {
     const int k = int(i + 1);
-    spmv_device(A, 1.0, V + i * N, 0.0, AV + i * N, s);
+    spmv_device_x64(A, 1.0, V + i * N, 0.0, AV + i * N, s);
     // new row of V^T AV: V_i . AV_c for c <= i (lower triangle)
     ctx.multidot(AV, N, k, V + i * N, ctx.dots);
     MB_CUDA(cudaMemcpyAsync(rowdots.data(), ctx.dots, k * 8,

@@ -107,6 +107,10 @@ void matrix_elements_device(macis_b200_ham* h, const uint64_t* bra,
                             const uint64_t* ket, size_t n, double* out);
 
 // y = alpha*A*x + beta*y on device vectors (one column).
+// Davidson's product: on a mixed matrix, FP32 values times the FP64 x with
+// FP64 sums (one fixed linear operator); FP64 matrices as spmv_device.
+void spmv_device_x64(const macis_b200_csr* A, double alpha, const double* x,
+                     double beta, double* y, cudaStream_t s);
 void spmv_device(const macis_b200_csr* A, double alpha, const double* x,
                  double beta, double* y, cudaStream_t s);
 

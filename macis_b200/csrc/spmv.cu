@@ -9,7 +9,8 @@
 // evict-first hint so that x keeps the cache. Row sums are warp trees in
 // FP64. Mixed mode: FP32 off-diagonal values times an FP32 copy of x, each
 // product formed exactly in FP64 (24x24-bit mantissas fit in 53 bits) and
-// summed in FP64, plus the FP64 diagonal times the FP64 x.
+// summed in FP64, plus the FP64 diagonal times the FP64 x. The Davidson
+// solver uses the same kernel with the FP64 x (spmv_device_x64).
 #include <mutex>
 
 #include "internal.hpp"
@@ -19,7 +20,11 @@ namespace mb {
 
 constexpr int SPMV_THREADS = 256;
 
-template <typename CI, typename VT, bool MIXED>
+// X32: the off-diagonal products use the FP32 copy x32 (the operator of
+// macis_b200_spmv on a mixed matrix); otherwise FP32 values multiply the
+// FP64 x, so that the product is one fixed linear operator of x (what the
+// Davidson residual needs to converge below FP32 resolution).
+template <typename CI, typename VT, bool MIXED, bool X32 = MIXED>
 __global__ void __launch_bounds__(SPMV_THREADS)
     spmv_k(int64_t m, int64_t n, const CI* __restrict__ rowptr,
            const CI* __restrict__ colind, const VT* __restrict__ nzval,
@@ -36,7 +41,7 @@ __global__ void __launch_bounds__(SPMV_THREADS)
     for(; j + 32 < e; j += 64) {
       const CI c0 = __ldcs(colind + j), c1 = __ldcs(colind + j + 32);
       const VT v0 = __ldcs(nzval + j), v1 = __ldcs(nzval + j + 32);
-      if constexpr(MIXED) {
+      if constexpr(X32) {
         acc0 += double(v0) * double(__ldg(x32 + c0));
         acc1 += double(v1) * double(__ldg(x32 + c1));
       } else {
@@ -47,7 +52,7 @@ __global__ void __launch_bounds__(SPMV_THREADS)
     if(j < e) {
       const CI c0 = __ldcs(colind + j);
       const VT v0 = __ldcs(nzval + j);
-      if constexpr(MIXED)
+      if constexpr(X32)
         acc0 += double(v0) * double(__ldg(x32 + c0));
       else
         acc0 += double(v0) * __ldg(x + c0);
@@ -102,6 +107,23 @@ void spmv_device(const macis_b200_csr* A, double alpha, const double* x,
           m, A->n, (const int64_t*)A->rowptr, (const int64_t*)A->colind,
           (const float*)A->nzval, A->diag, x, x32, alpha, beta, y), note_launch();
   }
+  MB_CUDA(cudaGetLastError());
+}
+
+void spmv_device_x64(const macis_b200_csr* A, double alpha, const double* x,
+                     double beta, double* y, cudaStream_t s) {
+  if(A->val_bytes == 8) return spmv_device(A, alpha, x, beta, y, s);
+  const int64_t m = A->m;
+  if(m == 0) return;
+  const unsigned g = spmv_grid(m);
+  if(A->idx_bytes == 4)
+    spmv_k<int32_t, float, true, false><<<g, SPMV_THREADS, 0, s>>>(
+        m, A->n, (const int32_t*)A->rowptr, (const int32_t*)A->colind,
+        (const float*)A->nzval, A->diag, x, nullptr, alpha, beta, y), note_launch();
+  else
+    spmv_k<int64_t, float, true, false><<<g, SPMV_THREADS, 0, s>>>(
+        m, A->n, (const int64_t*)A->rowptr, (const int64_t*)A->colind,
+        (const float*)A->nzval, A->diag, x, nullptr, alpha, beta, y), note_launch();
   MB_CUDA(cudaGetLastError());
 }
 

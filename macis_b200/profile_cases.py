@@ -8,6 +8,10 @@
     python -m macis_b200.profile_cases mlp_fwd     # network forward, 2M rows
     python -m macis_b200.profile_cases mlp_train   # one training epoch
     python -m macis_b200.profile_cases screen_n48  # screened search, n = 48
+    python -m macis_b200.profile_cases c3 --ntdets 1000000 --mode fp64
+        # ASCI n = 48, 12a/12b, bitset<128>: grow from HF (factor 8, <= 1e5
+        # core dets) then 3 refine iterations; --mode fp64 (exact search,
+        # FP64 Davidson) or learned_mixed (screened search, FP32-H Davidson)
 
 Each case runs its hot call a few times (--reps) and prints one timing line.
 """
@@ -109,10 +113,53 @@ def screen_n48(reps, ncore=10000):
         print(r)
 
 
+def c3(ntdets, mode, refine=3, ncore=100000, seed=0):
+    """One C3-shaped ASCI run; prints one JSON line with the per-iteration
+    log, the final energy and the wall time."""
+    import json
+    import logging
+    logging.basicConfig(level=logging.INFO, format="%(name)s %(message)s")
+    n, k = 48, 12
+    T, V = mb.synthetic_integrals(n, seed)
+    H = mb.HamiltonianGenerator(T, V, 128)
+    s = mb.ASCISettings(ntdets_max=int(ntdets), ntdets_min=100,
+                        ncdets_max=int(ncore), grow_factor=8, h_el_tol=1e-8,
+                        max_refine_iter=int(refine))
+    m = mb.MCSCFSettings(ci_max_subspace=40, davidson_restart_keep=8,
+                         davidson_max_iter=4000,
+                         precision=mb.MIXED if mode == "learned_mixed" else mb.FP64)
+    scr = None
+    if mode == "learned_mixed":
+        scr = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=128, seed=seed))
+    hf = mb.canonical_hf_determinant(k, k, 128)
+    E0 = float(H.matrix_element(hf, hf))
+    t0 = time.perf_counter()
+    E, dets, X = mb.asci_grow(s, m, E0, hf, [1.0], H, n, screen=scr)
+    t_grow = time.perf_counter() - t0
+    Eg = E
+    for _ in range(int(refine)):  # refine.hpp:15-66, fixed iteration count
+        E, dets, X = mb.asci_iter(s, m, len(dets), E, dets, X, H, n, scr)
+    dt = time.perf_counter() - t0
+    # variational energy of the final wavefunction with the FP64 H (the
+    # mixed mode solved with FP32 off-diagonal values)
+    A = mb.make_csr_hamiltonian(dets, H, EPS)
+    Xd = np.asarray(X, dtype=np.float64)
+    E_fp64 = float(Xd @ A.spmv(Xd)) / float(Xd @ Xd)
+    del A
+    out = {"mode": mode, "ntdets": int(ntdets), "ndets": len(dets),
+           "E_grow": Eg, "E_final": E, "E_final_fp64_H": E_fp64,
+           "seconds": dt, "grow_seconds": t_grow,
+           "iterations": m.iteration_log}
+    print(json.dumps(out, default=float))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--ntdets", type=float, default=1e6)
+    ap.add_argument("--mode", default="fp64")
     a = ap.parse_args()
     if a.case == "hbuild_c1":
         hbuild(10, 5, a.reps)
@@ -130,6 +177,8 @@ def main():
         mlp_train(a.reps)
     elif a.case == "screen_n48":
         screen_n48(a.reps)
+    elif a.case == "c3":
+        c3(a.ntdets, a.mode)
     else:
         raise SystemExit(f"unknown case {a.case}")
 
