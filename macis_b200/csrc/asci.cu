@@ -144,14 +144,17 @@ __device__ __forceinline__ void det_flip(uint64_t* d, int spin, int orb) {
 }
 
 // Range of a candidate determinant when the search is partitioned into nr
-// ranges: a hash of its words scaled to [0, nr). Every contribution to one
-// determinant falls into the same range.
-template <int NW>
-__device__ __forceinline__ uint32_t det_range(const uint64_t* w, uint32_t nr) {
+// ranges: a hash of its alpha string scaled to [0, nr). Every contribution to
+// one determinant falls into the same range, and the units whose alpha
+// string is fixed (beta singles, beta same-spin doubles, opposite-spin
+// doubles for one outer alpha pair) fall into one range as a whole.
+template <int NSW>
+__device__ __forceinline__ uint32_t alpha_range(const Spin<NSW>& a,
+                                                uint32_t nr) {
   uint64_t h = 0x9E3779B97F4A7C15ull;
 #pragma unroll
-  for(int j = 0; j < NW; ++j) {
-    h ^= w[j];
+  for(int j = 0; j < NSW; ++j) {
+    h ^= a.w[j];
     h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
     h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
     h ^= h >> 31;
@@ -226,6 +229,18 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
   const int64_t ninner = ud.ninner;
   int64_t done = 0;
   float mx = 0.f;  // largest |rv| of this lane (MODE 1)
+  // partitioned search: units with a fixed alpha string are in or out of
+  // range as a whole; the others test each contribution before evaluating it
+  bool chk = nr > 1;
+  if(chk && (kind == 1 || kind == 3 || kind == 4)) {
+    Spin<NSW> ua = sA;
+    if(kind == 4) ua = sp_flip(sp_flip(sA, int(occA[ii])), int(virA[aa]));
+    if(alpha_range<NSW>(ua, nr) != rr) {
+      if(MODE == 0 && lane == 0) *count_out = 0;
+      return;
+    }
+    chk = false;
+  }
   for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
     const int64_t q = q0 + lane;
     bool keep = false;
@@ -241,13 +256,18 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int nO = S ? nA : nB;
         const uint8_t* occO = S ? occA : occB;
         const int i = occS[q / nvS], a = virS[q % nvS];
-        double h = __ldg(I.T + a + size_t(i) * n);
-        const double* Gov = I.G_red + size_t(a) * n + size_t(i) * n * n;
-        const double* Vov = I.V_red + size_t(a) * n + size_t(i) * n * n;
-        for(int p = 0; p < nS; ++p) h += __ldg(Gov + occS[p]);
-        for(int p = 0; p < nO; ++p) h += __ldg(Vov + occO[p]);
-        keep = !(fabs(h) < tol);
-        if((MODE == 1 || nr > 1) && keep) {
+        const bool inr =
+            !chk || alpha_range<NSW>(sp_flip(sp_flip(sA, i), a), nr) == rr;
+        double h = 0;
+        if(inr) {
+          h = __ldg(I.T + a + size_t(i) * n);
+          const double* Gov = I.G_red + size_t(a) * n + size_t(i) * n * n;
+          const double* Vov = I.V_red + size_t(a) * n + size_t(i) * n * n;
+          for(int p = 0; p < nS; ++p) h += __ldg(Gov + occS[p]);
+          for(int p = 0; p < nO; ++p) h += __ldg(Vov + occO[p]);
+        }
+        keep = inr && !(fabs(h) < tol);
+        if(MODE == 1 && keep) {
           const double* eps = S ? epsB : epsA;
           h *= ex_sign(S ? sB : sA, a, i);
           const double hd = hii + eps[a] - eps[i] - G2R(a, i) - G2R(i, a);
@@ -268,9 +288,14 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int span = nvS - 1 - aa;
         const int jj = ii + 1 + int(q / span), bb = aa + 1 + int(q % span);
         const int i = occS[ii], a = virS[aa], j = occS[jj], b = virS[bb];
-        const double Gv = __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
-        keep = !(fabs(Gv) < tol);
-        if((MODE == 1 || nr > 1) && keep) {
+        const bool inr =
+            !chk || alpha_range<NSW>(sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j),
+                                                     a), b), nr) == rr;
+        const double Gv =
+            inr ? __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n)
+                : 0.0;
+        keep = inr && !(fabs(Gv) < tol);
+        if(MODE == 1 && keep) {
           const Spin<NSW> st = S ? sB : sA;
           Spin<NSW> fx = sp_flip(sp_flip(sp_flip(sp_flip(sp_zero<NSW>(), i), j), a), b);
           const uint32_t e = double_ex(st, st ^ fx);
@@ -295,7 +320,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int j = occB[q / nvB], b = virB[q % nvB];
         const double Vv = __ldg(I.V + a + size_t(i) * n + size_t(b + size_t(j) * n) * n * n);
         keep = !(fabs(Vv) < tol);
-        if((MODE == 1 || nr > 1) && keep) {
+        if(MODE == 1 && keep) {
           const double sign = ex_sign(sA, a, i) * ex_sign(sB, b, j);
           double h = sign * Vv;
           const double hd = hii + epsA[a] + epsB[b] - epsA[i] - epsB[j] +
@@ -312,7 +337,6 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         }
       }
     }
-    if(nr > 1 && keep) keep = det_range<D::NW>(ex, nr) == rr;
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     if(MODE == 1 && keep) {
       const int64_t pos = out0 + done + __popc(m & lanemask_lt());
@@ -909,7 +933,10 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     cap = std::min<int64_t>(std::max<int64_t>(cap, int64_t(1) << 20),
                             int64_t(1) << 31);
   }
-  uint32_t nr = uint32_t(std::max<int64_t>(1, (Ptot + cap - 1) / cap));
+  // ranges hash alpha strings, whose loads are uneven: 25% headroom
+  uint32_t nr = uint32_t(std::max<int64_t>(
+      1, int64_t(std::ceil(1.25 * double(Ptot) / double(cap)))));
+  if(Ptot <= cap) nr = 1;
   if(pairs_only) nr = 1;  // the full accumulated list is the result
   stats.batches = nr;
   stats.pairs_ms = ms_since(t_all);
