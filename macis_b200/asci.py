@@ -180,7 +180,8 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
     E, X = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,
                             mcscf_settings.ci_max_subspace,
                             mcscf_settings.ci_res_tol, None,
-                            precision=mcscf_settings.precision, timings=tim,
+                            precision=mcscf_settings.precision,
+                            index_t=None, timings=tim,
                             restart_keep=mcscf_settings.davidson_restart_keep,
                             max_iter=mcscf_settings.davidson_max_iter)
     t2 = time.perf_counter()

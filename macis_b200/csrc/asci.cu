@@ -143,14 +143,29 @@ __device__ __forceinline__ void det_flip(uint64_t* d, int spin, int orb) {
   }
 }
 
-// Range of a candidate determinant when the search is partitioned into nr
-// ranges: a hash of its alpha string scaled to [0, nr). Every contribution to
-// one determinant falls into the same range, and the units whose alpha
+// Candidate ranges of a partitioned search: the alpha string of a candidate
+// determinant is hashed to one of ASCI_BINS bins, and a range is an interval
+// of bins [blo, bhi) chosen from the measured bin loads. Every contribution
+// to one determinant falls into the same range, and the units whose alpha
 // string is fixed (beta singles, beta same-spin doubles, opposite-spin
-// doubles for one outer alpha pair) fall into one range as a whole.
+// doubles for one outer alpha pair) fall into one bin as a whole.
+constexpr uint32_t ASCI_BINS = 4096;
+// Second-level split of one oversized bin: a hash of the beta string.
 template <int NSW>
-__device__ __forceinline__ uint32_t alpha_range(const Spin<NSW>& a,
-                                                uint32_t nr) {
+__device__ __forceinline__ uint32_t beta_sub(const Spin<NSW>& b,
+                                             uint32_t nsub) {
+  uint64_t h = 0xD1B54A32D192ED03ull;
+#pragma unroll
+  for(int j = 0; j < NSW; ++j) {
+    h ^= b.w[j];
+    h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
+    h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
+    h ^= h >> 31;
+  }
+  return uint32_t((uint64_t(uint32_t(h >> 32)) * nsub) >> 32);
+}
+template <int NSW>
+__device__ __forceinline__ uint32_t alpha_bin(const Spin<NSW>& a) {
   uint64_t h = 0x9E3779B97F4A7C15ull;
 #pragma unroll
   for(int j = 0; j < NSW; ++j) {
@@ -159,7 +174,7 @@ __device__ __forceinline__ uint32_t alpha_range(const Spin<NSW>& a,
     h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
     h ^= h >> 31;
   }
-  return uint32_t((uint64_t(uint32_t(h >> 32)) * nr) >> 32);
+  return uint32_t(h >> 52);  // 12 bits: ASCI_BINS
 }
 
 #define G2R(p, q) __ldg(I.G2_red + (p) + size_t(q) * n)
@@ -207,7 +222,9 @@ template <int NBITS, int MODE>
 __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                          double E0, double tol, int64_t* count_out,
                          int64_t out0, uint64_t* keys, double* rv,
-                         float* umax, uint32_t nr, uint32_t rr) {
+                         float* umax, uint32_t blo, uint32_t bhi,
+                         uint32_t nsub, uint32_t sub,
+                         unsigned long long* hist) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
   const int lane = threadIdx.x & 31;
@@ -231,15 +248,29 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
   float mx = 0.f;  // largest |rv| of this lane (MODE 1)
   // partitioned search: units with a fixed alpha string are in or out of
   // range as a whole; the others test each contribution before evaluating it
-  bool chk = nr > 1;
-  if(chk && (kind == 1 || kind == 3 || kind == 4)) {
+  // A range of a split bin also selects one beta-hash class (nsub > 1): the
+  // units with a varying alpha string have a fixed beta string (tested once
+  // here), the others test each contribution's beta string.
+  const bool part = blo > 0 || bhi < ASCI_BINS;
+  const bool split = nsub > 1;
+  bool chk = part;
+  bool chkb = false;
+  const bool fixed_alpha = kind == 1 || kind == 3 || kind == 4;
+  uint32_t ubin = 0;
+  if(fixed_alpha && (part || hist)) {
     Spin<NSW> ua = sA;
     if(kind == 4) ua = sp_flip(sp_flip(sA, int(occA[ii])), int(virA[aa]));
-    if(alpha_range<NSW>(ua, nr) != rr) {
+    ubin = alpha_bin<NSW>(ua);
+    if(part && (ubin < blo || ubin >= bhi)) {
       if(MODE == 0 && lane == 0) *count_out = 0;
       return;
     }
     chk = false;
+    chkb = split;
+  }
+  if(!fixed_alpha && split && beta_sub<NSW>(sB, nsub) != sub) {
+    if(MODE == 0 && lane == 0) *count_out = 0;
+    return;
   }
   for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
     const int64_t q = q0 + lane;
@@ -256,8 +287,12 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int nO = S ? nA : nB;
         const uint8_t* occO = S ? occA : occB;
         const int i = occS[q / nvS], a = virS[q % nvS];
-        const bool inr =
-            !chk || alpha_range<NSW>(sp_flip(sp_flip(sA, i), a), nr) == rr;
+        uint32_t cbin = 0;
+        if(S == 0 && (chk || hist))
+          cbin = alpha_bin<NSW>(sp_flip(sp_flip(sA, i), a));
+        bool inr = !chk || (cbin >= blo && cbin < bhi);
+        if(chkb)  // S == 1
+          inr = beta_sub<NSW>(sp_flip(sp_flip(sB, i), a), nsub) == sub;
         double h = 0;
         if(inr) {
           h = __ldg(I.T + a + size_t(i) * n);
@@ -267,6 +302,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
           for(int p = 0; p < nO; ++p) h += __ldg(Vov + occO[p]);
         }
         keep = inr && !(fabs(h) < tol);
+        if(MODE == 0 && hist && S == 0 && keep) atomicAdd(hist + cbin, 1ull);
         if(MODE == 1 && keep) {
           const double* eps = S ? epsB : epsA;
           h *= ex_sign(S ? sB : sA, a, i);
@@ -288,13 +324,20 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int span = nvS - 1 - aa;
         const int jj = ii + 1 + int(q / span), bb = aa + 1 + int(q % span);
         const int i = occS[ii], a = virS[aa], j = occS[jj], b = virS[bb];
-        const bool inr =
-            !chk || alpha_range<NSW>(sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j),
-                                                     a), b), nr) == rr;
+        uint32_t cbin = 0;
+        if(S == 0 && (chk || hist))
+          cbin = alpha_bin<NSW>(
+              sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b));
+        bool inr = !chk || (cbin >= blo && cbin < bhi);
+        if(chkb)  // S == 1
+          inr = beta_sub<NSW>(
+                    sp_flip(sp_flip(sp_flip(sp_flip(sB, i), j), a), b), nsub) ==
+                sub;
         const double Gv =
             inr ? __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n)
                 : 0.0;
         keep = inr && !(fabs(Gv) < tol);
+        if(MODE == 0 && hist && S == 0 && keep) atomicAdd(hist + cbin, 1ull);
         if(MODE == 1 && keep) {
           const Spin<NSW> st = S ? sB : sA;
           Spin<NSW> fx = sp_flip(sp_flip(sp_flip(sp_flip(sp_zero<NSW>(), i), j), a), b);
@@ -318,8 +361,12 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         // append_os_doubles_asci_contributions (determinant_contributions.hpp:122-160)
         const int i = occA[ii], a = virA[aa];
         const int j = occB[q / nvB], b = virB[q % nvB];
-        const double Vv = __ldg(I.V + a + size_t(i) * n + size_t(b + size_t(j) * n) * n * n);
-        keep = !(fabs(Vv) < tol);
+        const bool inr =
+            !chkb || beta_sub<NSW>(sp_flip(sp_flip(sB, j), b), nsub) == sub;
+        const double Vv =
+            inr ? __ldg(I.V + a + size_t(i) * n + size_t(b + size_t(j) * n) * n * n)
+                : 0.0;
+        keep = inr && !(fabs(Vv) < tol);
         if(MODE == 1 && keep) {
           const double sign = ex_sign(sA, a, i) * ex_sign(sB, b, j);
           double h = sign * Vv;
@@ -347,7 +394,10 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
     }
     done += __popc(m);
   }
-  if(MODE == 0 && lane == 0) *count_out = done;
+  if(MODE == 0 && lane == 0) {
+    *count_out = done;
+    if(hist && fixed_alpha && done) atomicAdd(hist + ubin, (unsigned long long)done);
+  }
   if(MODE == 1 && umax) {
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1)
@@ -364,7 +414,15 @@ __global__ void __launch_bounds__(256)
     units_k(Ints I, CoreData cd, int64_t u0, int64_t u1, size_t c0, size_t c1,
             double E0, double tol, int64_t* counts, const int64_t* outoff,
             uint64_t* keys, double* rv, const uint8_t* umask, float* umax,
-            uint32_t nr, uint32_t rr) {
+            uint32_t blo, uint32_t bhi, uint32_t nsub, uint32_t sub,
+            unsigned long long* hist) {
+  // hist (count pass only): per-block bin counts in shared memory
+  // (dynamic, ASCI_BINS x 8 B), added to the global histogram at the end
+  extern __shared__ unsigned long long shist[];
+  if(hist) {
+    for(uint32_t i = threadIdx.x; i < ASCI_BINS; i += blockDim.x) shist[i] = 0;
+    __syncthreads();
+  }
   const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
   for(int64_t u = u0 + int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
       u < u1; u += int64_t(nwarp)) {
@@ -384,7 +442,13 @@ __global__ void __launch_bounds__(256)
     const int64_t t = u - cd.uoff[lo];
     unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
                           MODE ? outoff[u - u0] : 0, keys, rv,
-                          umax ? umax + u : nullptr, nr, rr);
+                          umax ? umax + u : nullptr, blo, bhi, nsub, sub,
+                          hist ? shist : nullptr);
+  }
+  if(hist) {
+    __syncthreads();
+    for(uint32_t i = threadIdx.x; i < ASCI_BINS; i += blockDim.x)
+      if(shist[i]) atomicAdd(hist + i, shist[i]);
   }
 }
 
@@ -734,25 +798,6 @@ struct Pairs {
   double* rv = nullptr;
   size_t n = 0;
 };
-// Device bytes that allocations can still obtain: free memory plus what the
-// default stream-ordered pool holds without using it.
-size_t device_bytes_available() {
-  size_t freeb = 0, totb = 0;
-  MB_CUDA(cudaMemGetInfo(&freeb, &totb));
-  int dev = 0;
-  MB_CUDA(cudaGetDevice(&dev));
-  cudaMemPool_t pool;
-  if(cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    unsigned long long res = 0, used = 0;  // the attributes are 64-bit
-    if(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res) ==
-           cudaSuccess &&
-       cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) ==
-           cudaSuccess &&
-       res > used)
-      freeb += size_t(res - used);
-  }
-  return freeb;
-}
 double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(
              std::chrono::steady_clock::now() - t)
@@ -902,10 +947,18 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
 
   // unit counts of the whole search (count pass over all units at once)
   int64_t* ucnt = A.get<int64_t>(U + 1);
-  if(U)
-    units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
-        I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt, nullptr, nullptr,
-        nullptr, umask, nullptr, 1u, 0u), note_launch();
+  auto* dhist = A.get<unsigned long long>(ASCI_BINS);
+  MB_CUDA(cudaMemsetAsync(dhist, 0, ASCI_BINS * 8, s));
+  if(U) {
+    const size_t hbytes = ASCI_BINS * sizeof(unsigned long long);
+    MB_CUDA(cudaFuncSetAttribute(units_k<NBITS, 0>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(hbytes)));
+    units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, hbytes,
+                        s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt,
+                             nullptr, nullptr, nullptr, umask, nullptr, 0u,
+                             ASCI_BINS, 0u, 0u, dhist), note_launch();
+  }
   int64_t* uout = A.get<int64_t>(U + 1);
   exclusive_scan<int64_t, int64_t>(ucnt, uout, size_t(U), uout + U, A);
   const int64_t Ptot = U ? to_host(uout + U, s) : 0;
@@ -918,7 +971,10 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   // unpartitioned search) and the range can go straight into the running
   // top-k: memory stays bounded by one range plus ~ndets_max candidates.
   const double rs = double(NW * 8 + 8);
-  const double per_pair = 3.0 * rs + 20.0;  // record, sort copy, flags, sums
+  // per raw contribution while a range is processed: record + sort copy,
+  // flags and radix tables (sort), then the unique list + kept copy + the
+  // running top-k concatenation (few duplicates: unique ~ raw)
+  const double per_pair = 4.0 * rs + 20.0;
   const size_t topk = ndets_max - ncdets;   // size_t arithmetic (:547)
   const double keep_reserve =
       6.0 * rs * double(std::min<uint64_t>(topk, uint64_t(Ptot)));
@@ -933,11 +989,44 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     cap = std::min<int64_t>(std::max<int64_t>(cap, int64_t(1) << 20),
                             int64_t(1) << 31);
   }
-  // ranges hash alpha strings, whose loads are uneven: 25% headroom
-  uint32_t nr = uint32_t(std::max<int64_t>(
-      1, int64_t(std::ceil(1.25 * double(Ptot) / double(cap)))));
-  if(Ptot <= cap) nr = 1;
-  if(pairs_only) nr = 1;  // the full accumulated list is the result
+  // ranges: consecutive alpha-string bins packed up to the cap from the
+  // measured bin loads (a single bin above the cap is a range of its own)
+  // (a bin above the cap is split into beta-hash classes)
+  std::vector<uint32_t> rlo, rhi, rns, rsub;
+  auto add_range = [&](uint32_t lo, uint32_t hi, uint32_t ns, uint32_t sb) {
+    rlo.push_back(lo);
+    rhi.push_back(hi);
+    rns.push_back(ns);
+    rsub.push_back(sb);
+  };
+  if(Ptot <= cap || pairs_only) {  // pairs_only: the full list is the result
+    add_range(0, ASCI_BINS, 0, 0);
+  } else {
+    std::vector<unsigned long long> hh(ASCI_BINS);
+    MB_CUDA(cudaMemcpyAsync(hh.data(), dhist, ASCI_BINS * 8,
+                            cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    uint32_t b0 = 0;
+    unsigned long long acc = 0;
+    for(uint32_t b = 0; b < ASCI_BINS; ++b) {
+      if(hh[b] > uint64_t(cap)) {
+        if(acc) add_range(b0, b, 0, 0);
+        const uint32_t ns = uint32_t(std::ceil(1.25 * double(hh[b]) / double(cap)));
+        for(uint32_t k = 0; k < ns; ++k) add_range(b, b + 1, ns, k);
+        b0 = b + 1;
+        acc = 0;
+        continue;
+      }
+      if(acc && acc + hh[b] > uint64_t(cap)) {
+        add_range(b0, b, 0, 0);
+        b0 = b;
+        acc = 0;
+      }
+      acc += hh[b];
+    }
+    if(b0 < ASCI_BINS) add_range(b0, ASCI_BINS, 0, 0);
+  }
+  const uint32_t nr = uint32_t(rlo.size());
   stats.batches = nr;
   stats.pairs_ms = ms_since(t_all);
 
@@ -1006,7 +1095,8 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       off = B.get<int64_t>(U + 1);
       units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
           I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, nullptr, nullptr,
-          nullptr, umask, nullptr, nr, rr), note_launch();
+          nullptr, umask, nullptr, rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr),
+          note_launch();
       exclusive_scan<int64_t, int64_t>(rc, off, size_t(U), off + U, B);
       P = to_host(off + U, s);
     }
@@ -1015,7 +1105,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     if(P) {
       units_k<NBITS, 1><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
           I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, off, keys, rv, umask,
-          umax, nr, rr), note_launch();
+          umax, rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr), note_launch();
       MB_CUDA(cudaGetLastError());
     }
     MB_CUDA(cudaStreamSynchronize(s));
@@ -1041,8 +1131,10 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
           f, fx, size_t(P), start, keys, k2), note_launch();
       seg_sum_k<<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(
           start, nu, size_t(P), rv, r2), note_launch();
+      // the raw records are summed: release them before the keep / top-k
       for(void* q : {static_cast<void*>(f), static_cast<void*>(fx),
-                     static_cast<void*>(start)})
+                     static_cast<void*>(start), static_cast<void*>(keys),
+                     static_cast<void*>(rv)})
         B.release(q);
       uq.keys = k2;
       uq.rv = r2;

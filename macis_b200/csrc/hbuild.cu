@@ -919,11 +919,12 @@ __global__ void __launch_bounds__(HB_THREADS)
 // long-row scratch (lcol/lval at loff[row]) and finished by the radix sort.
 template <int NBITS, typename CI, typename VT>
 __global__ void __launch_bounds__(HB_THREADS)
-    gen_fill_k(Ints I, GenData g, const uint64_t* bra, size_t nbra,
-               const double* __restrict__ hdiag,
+    gen_fill_k(Ints I, GenData g, const uint64_t* bra, int64_t row_a,
+               int64_t row_b, const double* __restrict__ hdiag,
                const int64_t* __restrict__ rowptr,
-               const int64_t* __restrict__ loff, uint64_t* lcol, double* lval,
-               CI* __restrict__ colind, VT* __restrict__ nzval,
+               const int64_t* __restrict__ loff, int64_t lbase0,
+               const uint32_t* __restrict__ lidx, uint64_t* lkey,
+               double* lval, CI* __restrict__ colind, VT* __restrict__ nzval,
                double* __restrict__ diag, int64_t* __restrict__ rowcnt,
                double thresh) {
   using D = DetTraits<NBITS>;
@@ -934,7 +935,7 @@ __global__ void __launch_bounds__(HB_THREADS)
   uint32_t* bc = s_col[wid];
   double* bv = s_val[wid];
   const int64_t nwarp = int64_t(gridDim.x) * HB_WARPS;
-  for(int64_t row = int64_t(blockIdx.x) * HB_WARPS + wid; row < int64_t(nbra);
+  for(int64_t row = row_a + int64_t(blockIdx.x) * HB_WARPS + wid; row < row_b;
       row += nwarp) {
     const int32_t rg = g.rowgroup[row];
     const int64_t ncand = rowptr[row + 1] - rowptr[row];
@@ -943,7 +944,10 @@ __global__ void __launch_bounds__(HB_THREADS)
       continue;
     }
     const bool lng = ncand > GEN_CAP;
-    const int64_t lbase = lng ? loff[row] : 0;
+    // long rows: (long-row index, column) sort keys and values into this
+    // chunk's scratch
+    const int64_t lbase = lng ? loff[row] - lbase0 : 0;
+    const uint64_t lhi = lng ? uint64_t(lidx[row]) << 32 : 0;
     const uint64_t* bd = bra + row * D::NW;
     const Spin<NSW> ba = D::alpha(bd), bb = D::beta(bd);
     const double hd = hdiag[row];
@@ -965,7 +969,7 @@ __global__ void __launch_bounds__(HB_THREADS)
       if(act) {
         const int64_t pos = c + __popc(msk & lanemask_lt());
         if(lng) {
-          lcol[lbase + pos] = col;
+          lkey[lbase + pos] = lhi | col;
           lval[lbase + pos] = h;
         } else {
           bc[pos] = col;
@@ -1034,7 +1038,7 @@ __global__ void __launch_bounds__(HB_THREADS)
 // FP64 values; write them back with threshold compaction.
 template <typename CI, typename VT>
 __global__ void long_rows_write_k(const int64_t* lrows, int64_t nl,
-                                  const int64_t* loff_sorted,
+                                  const int64_t* loff_sorted, int64_t base0,
                                   const uint64_t* keys, const double* vals,
                                   const int64_t* rowptr, CI* colind,
                                   VT* nzval, double* diag, int64_t* rowcnt,
@@ -1044,7 +1048,7 @@ __global__ void long_rows_write_k(const int64_t* lrows, int64_t nl,
   for(int64_t r = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
       r < nl; r += nwarp) {
     const int64_t row = lrows[r];
-    const int64_t b = loff_sorted[r], e = loff_sorted[r + 1];
+    const int64_t b = loff_sorted[r] - base0, e = loff_sorted[r + 1] - base0;
     const int64_t out0 = rowptr[row];
     int64_t kept = 0;
     for(int64_t base = b; base < e; base += 32) {
@@ -1069,17 +1073,6 @@ __global__ void long_rows_write_k(const int64_t* lrows, int64_t nl,
     }
     if(lane == 0) rowcnt[row] = kept;
   }
-}
-
-__global__ void long_keys_k(const int64_t* lrows, int64_t nl,
-                            const int64_t* loff, const uint64_t* lcol,
-                            uint64_t* keys) {
-  const int64_t nwarp = int64_t(gridDim.x) * (blockDim.x >> 5);
-  const int lane = threadIdx.x & 31;
-  for(int64_t r = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      r < nl; r += nwarp)
-    for(int64_t i = loff[r] + lane; i < loff[r + 1]; i += 32)
-      keys[i] = (uint64_t(r) << 32) | lcol[i];
 }
 
 __global__ void long_flags_k(const int64_t* rowptr, size_t n, uint32_t* f) {
@@ -1135,6 +1128,7 @@ template <int NBITS, typename CI, typename VT>
 static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
                        const uint64_t* ket, size_t nket, double thresh,
                        macis_b200_csr* out) {
+  bool general_fill_timed = false;  // the chunked general fill sums its own time
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
   cudaStream_t s = h->stream;
@@ -1395,9 +1389,8 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     out->long_rows = nl;
     int64_t *lrows = nullptr, *lcnt = nullptr, *loff = nullptr,
             *loff_row = nullptr;
-    uint64_t* lcol = nullptr;
-    double* lval = nullptr;
     int64_t ltot = 0;
+    std::vector<int64_t> h_lrows, h_loff;
     if(nl) {
       lrows = A.get<int64_t>(nl + 1);
       lcnt = A.get<int64_t>(nl + 1);
@@ -1409,27 +1402,58 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       ltot = to_host(loff + nl, s);
       long_rowoff_k<<<grid_for(nl, 256, 4 * sms), 256, 0, s>>>(lrows, loff, nl,
                                                               loff_row), note_launch();
-      lcol = A.get<uint64_t>(ltot + 1);
-      lval = A.get<double>(ltot + 1);
+      h_lrows.resize(nl);
+      h_loff.resize(nl + 1);
+      MB_CUDA(cudaMemcpyAsync(h_lrows.data(), lrows, nl * 8,
+                              cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaMemcpyAsync(h_loff.data(), loff, (nl + 1) * 8,
+                              cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaStreamSynchronize(s));
     }
-    cudaEventRecord(ev[0], s);
-    gen_fill_k<NBITS, CI, VT><<<gr, HB_THREADS, 0, s>>>(
-        I, gd, bra, nbra, hdiag, rowptr64, loff_row, lcol, lval, colind,
-        nzval, out->diag, rowcnt, thresh), note_launch();
-    cudaEventRecord(ev[1], s);
-    MB_CUDA(cudaGetLastError());
-    if(nl) {
-      uint64_t* lk = A.get<uint64_t>(ltot + 1);
-      uint64_t* lk2 = A.get<uint64_t>(ltot + 1);
-      double* lv2 = A.get<double>(ltot + 1);
-      long_keys_k<<<grid_for(size_t(nl) * 32, 256, 8 * sms), 256, 0, s>>>(
-          lrows, nl, loff, lcol, lk), note_launch();
-      radix_sort<1, double>(lk, lval, lk2, lv2, size_t(ltot), A);
-      long_rows_write_k<CI, VT><<<grid_for(size_t(nl) * 32, 256, 8 * sms),
-                                  256, 0, s>>>(lrows, nl, loff, lk, lval,
-                                               rowptr64, colind, nzval,
-                                               out->diag, rowcnt, thresh), note_launch();
-    }
+    // Long rows are finished in chunks of consecutive rows whose scratch
+    // (key + value, and the sort's second copy: 32 B per entry) fits in
+    // what is free; short rows of the chunk are written by the same launch.
+    int64_t lchunk = int64_t(0.7 * double(device_bytes_available()) / 32.0);
+    lchunk = std::max<int64_t>(lchunk, int64_t(1) << 20);
+    constexpr int gen_dyn = 0;
+    float fill_ms_tot = 0.f;
+    int64_t la = 0;  // next long row (list index)
+    int64_t row_a = 0;
+    do {
+      int64_t lb = la;  // long rows [la, lb) in this chunk
+      while(lb < int64_t(nl) && (lb == la || h_loff[lb + 1] - h_loff[la] <= lchunk))
+        ++lb;
+      const int64_t row_b = lb < int64_t(nl) ? h_lrows[lb] : int64_t(nbra);
+      const int64_t cbase = nl ? h_loff[la] : 0;
+      const int64_t centries = nl ? h_loff[lb] - cbase : 0;
+      Arena C(s);
+      uint64_t* lkey = C.get<uint64_t>(centries + 1);
+      double* lval = C.get<double>(centries + 1);
+      cudaEventRecord(ev[0], s);
+      gen_fill_k<NBITS, CI, VT><<<gr, HB_THREADS, gen_dyn, s>>>(
+          I, gd, bra, row_a, row_b, hdiag, rowptr64, loff_row, cbase, lpos,
+          lkey, lval, colind, nzval, out->diag, rowcnt, thresh), note_launch();
+      cudaEventRecord(ev[1], s);
+      MB_CUDA(cudaGetLastError());
+      MB_CUDA(cudaEventSynchronize(ev[1]));
+      float ms = 0.f;
+      MB_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      fill_ms_tot += ms;
+      if(lb > la) {
+        uint64_t* lk2 = C.get<uint64_t>(centries + 1);
+        double* lv2 = C.get<double>(centries + 1);
+        radix_sort<1, double>(lkey, lval, lk2, lv2, size_t(centries), C);
+        long_rows_write_k<CI, VT><<<grid_for(size_t(lb - la) * 32, 256, 8 * sms),
+                                    256, 0, s>>>(
+            lrows + la, lb - la, loff + la, cbase, lkey, lval, rowptr64,
+            colind, nzval, out->diag, rowcnt, thresh), note_launch();
+        MB_CUDA(cudaGetLastError());
+      }
+      la = lb;
+      row_a = row_b;
+    } while(row_a < int64_t(nbra));
+    out->fill_ms = fill_ms_tot;
+    general_fill_timed = true;
   }
 
   // ------------------------------------------- exact row pointer + compaction
@@ -1463,7 +1487,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
   out->nzval = nzval;
   MB_CUDA(cudaGetLastError());
   MB_CUDA(cudaStreamSynchronize(s));
-  cudaEventElapsedTime(&out->fill_ms, ev[0], ev[1]);
+  if(!general_fill_timed) cudaEventElapsedTime(&out->fill_ms, ev[0], ev[1]);
 }
 
 macis_b200_csr* build_csr_device(macis_b200_ham* h, const uint64_t* bra,

@@ -397,6 +397,25 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
   return passes;
 }
 
+// Device bytes that allocations can still obtain: free memory plus what the
+// default stream-ordered pool holds without using it.
+inline size_t device_bytes_available() {
+  size_t freeb = 0, totb = 0;
+  MB_CUDA(cudaMemGetInfo(&freeb, &totb));
+  int dev = 0;
+  MB_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  if(cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long res = 0, used = 0;  // the attributes are 64-bit
+    if(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res) ==
+           cudaSuccess &&
+       cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) ==
+           cudaSuccess &&
+       res > used)
+      freeb += size_t(res - used);
+  }
+  return freeb;
+}
 // Copy a device value to the host (synchronising the stream).
 template <typename T>
 T to_host(const T* d, cudaStream_t s) {

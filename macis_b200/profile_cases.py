@@ -12,6 +12,10 @@
         # ASCI n = 48, 12a/12b, bitset<128>: grow from HF (factor 8, <= 1e5
         # core dets) then 3 refine iterations; --mode fp64 (exact search,
         # FP64 Davidson) or learned_mixed (screened search, FP32-H Davidson)
+    python -m macis_b200.profile_cases c4 --ntdets 1000000 --mode ...
+        # the same on n = 64, 16a/16b, bitset<128>; learned_mixed also runs
+        # one exact search from its last core set and reports the top-k
+        # recall of the screened one
 
 Each case runs its hot call a few times (--reps) and prints one timing line.
 """
@@ -113,13 +117,12 @@ def screen_n48(reps, ncore=10000):
         print(r)
 
 
-def c3(ntdets, mode, refine=3, ncore=100000, seed=0):
-    """One C3-shaped ASCI run; prints one JSON line with the per-iteration
-    log, the final energy and the wall time."""
+def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12):
+    """One C3-shaped ASCI run (C4 with n = 64, k = 16); prints one JSON line
+    with the per-iteration log, the final energy and the wall time."""
     import json
     import logging
     logging.basicConfig(level=logging.INFO, format="%(name)s %(message)s")
-    n, k = 48, 12
     T, V = mb.synthetic_integrals(n, seed)
     H = mb.HamiltonianGenerator(T, V, 128)
     s = mb.ASCISettings(ntdets_max=int(ntdets), ntdets_min=100,
@@ -140,14 +143,29 @@ def c3(ntdets, mode, refine=3, ncore=100000, seed=0):
     for _ in range(int(refine)):  # refine.hpp:15-66, fixed iteration count
         E, dets, X = mb.asci_iter(s, m, len(dets), E, dets, X, H, n, scr)
     dt = time.perf_counter() - t0
+    recall = None
+    if scr is not None:
+        # top-k recall of the screened search against the exact one, from
+        # the same core set (the last iteration's wavefunction)
+        core, C = mb.reorder_ci_on_coeff(dets, np.asarray(X))
+        nc = min(int(ncore), len(core))
+        sc = mb.ScreenSettings(network=scr.network, keep_frac=scr.keep_frac,
+                               explore_frac=0.0, train=False)
+        got = mb.asci_search(s, len(dets), core[:nc], E, C[:nc], n, H,
+                             screen=sc, use_net=True)
+        exact = mb.asci_search(s, len(dets), core[:nc], E, C[:nc], n, H)
+        ea = set(map(bytes, exact[:len(exact) - nc]))
+        recall = sum(1 for d in got[:len(got) - nc] if bytes(d) in ea) / max(
+            len(ea), 1)
     # variational energy of the final wavefunction with the FP64 H (the
     # mixed mode solved with FP32 off-diagonal values)
-    A = mb.make_csr_hamiltonian(dets, H, EPS)
+    A = mb.make_csr_hamiltonian(dets, H, EPS, np.int64)
     Xd = np.asarray(X, dtype=np.float64)
     E_fp64 = float(Xd @ A.spmv(Xd)) / float(Xd @ Xd)
     del A
     out = {"mode": mode, "ntdets": int(ntdets), "ndets": len(dets),
-           "E_grow": Eg, "E_final": E, "E_final_fp64_H": E_fp64,
+           "n": n, "electrons": [k, k], "E_grow": Eg, "E_final": E,
+           "E_final_fp64_H": E_fp64, "topk_recall_last": recall,
            "seconds": dt, "grow_seconds": t_grow,
            "iterations": m.iteration_log}
     print(json.dumps(out, default=float))
@@ -179,6 +197,8 @@ def main():
         screen_n48(a.reps)
     elif a.case == "c3":
         c3(a.ntdets, a.mode)
+    elif a.case == "c4":
+        c3(a.ntdets, a.mode, n=64, k=16)
     else:
         raise SystemExit(f"unknown case {a.case}")
 

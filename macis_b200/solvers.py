@@ -13,7 +13,7 @@ import time
 import numpy as np
 
 from . import _lib
-from ._lib import LIB, MacisError, check
+from ._lib import ECAPACITY, LIB, MacisError, check
 from .hamiltonian import DeviceCSR, make_csr_hamiltonian
 
 __all__ = ["SparseMatrixOperator", "diagonal_guess", "davidson",
@@ -100,7 +100,23 @@ def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
              davidson_max_m)
     value_t = np.float32 if precision == MIXED else np.float64
     t0 = time.perf_counter()
-    H = make_csr_hamiltonian(dets, ham_gen, h_el_tol, index_t, value_t)
+    if index_t is None:
+        # int32 indices while nnz fits (2^31 - 1), else int64; the need for
+        # int64 is remembered per generator so that later, larger spaces go
+        # straight to it
+        index_t = np.int64 if ndets >= getattr(
+            ham_gen, "_int64_from_ndets", 1 << 62) else np.int32
+        try:
+            H = make_csr_hamiltonian(dets, ham_gen, h_el_tol, index_t, value_t)
+        except MacisError as e:
+            if index_t is not np.int32 or e.code != ECAPACITY:
+                raise
+            ham_gen._int64_from_ndets = ndets
+            log.info("  nnz exceeds int32 indices: 64-bit indices")
+            H = make_csr_hamiltonian(dets, ham_gen, h_el_tol, np.int64,
+                                     value_t)
+    else:
+        H = make_csr_hamiltonian(dets, ham_gen, h_el_tol, index_t, value_t)
     t1 = time.perf_counter()
     log.info("  NNZ = %d, H_DUR = %.5e ms", H.nnz, (t1 - t0) * 1e3)
     log.info("  HMEM_LOC = %.2e GiB", H.mem_footprint() / 1073741824.0)
