@@ -212,19 +212,7 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def allmax(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
-
-    def allsum(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return t.item()
+    from macis_b200.dist import reduce_max, reduce_sum
 
     T, V, dets = c2_inputs()
     N = len(dets)
@@ -270,8 +258,8 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     launches = LIB.macis_b200_launch_count() - launches0
     ck = clocks.stop() if clocks else None
-    tot_ms = allmax(sum(step_ms))
-    nnz_all = allsum(float(nnz))
+    tot_ms = reduce_max(sum(step_ms), device=dev)
+    nnz_all = reduce_sum(float(nnz), device=dev)
     value = nnz_all * args.steps / (tot_ms / 1e3)
     res = {}
     if rank == 0:

@@ -1,0 +1,288 @@
+"""Row-block distribution of the Hamiltonian and its Davidson solve over
+ranks: one process per GPU, torch.distributed for the exchange.
+
+The reference distributes H by rows (make_dist_csr_hamiltonian,
+include/macis/csr_hamiltonian.hpp:49-82): every rank holds all determinants
+and integrals and builds the rows ``row_bounds(M, world, rank)`` against the
+full ket list; the build needs no exchange. Its parallel Davidson
+(p_davidson, include/macis/solvers/davidson.hpp:283-394) keeps the local rows
+of every subspace vector; the operator first gathers the vector from all
+ranks (sparsexx pspmbv), inner products are summed over ranks
+(p_gram_schmidt, :228-256), and the k x k Rayleigh-Ritz problem is reduced
+over ranks, solved on rank 0 and broadcast (p_rayleigh_ritz, :258-280).
+
+Here the ranks are torch.distributed processes. With NCCL every rank drives
+one GPU: its H block is built by libmacis_b200 and the gathered vector and
+the local products stay in HBM. The same host logic runs on CPU tensors
+over gloo, which is how the multi-rank path is tested without GPUs.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .hamiltonian import DeviceCSR, _dev_ptr, _host_dets, row_bounds
+from ._lib import LIB, check
+
+__all__ = ["rank_world", "local_rows", "reduce_max", "reduce_sum",
+           "allgather_rows", "DistCSR", "make_dist_csr_hamiltonian",
+           "RowBlockOperator", "p_gram_schmidt", "p_rayleigh_ritz",
+           "p_davidson", "gather_row_blocks"]
+
+
+def _dist():
+    import torch.distributed as dist
+    return dist
+
+
+def rank_world(group=None):
+    """(rank, world size) of this process; (0, 1) without a process group."""
+    dist = _dist()
+    if not (dist.is_available() and dist.is_initialized()):
+        return 0, 1
+    return dist.get_rank(group), dist.get_world_size(group)
+
+
+def local_rows(M, group=None):
+    """Row block [lo, hi) this rank owns (dist_sparse_matrix default
+    partition, sparsexx/matrix_types/dist_sparse_matrix.hpp:47-62)."""
+    r, w = rank_world(group)
+    return row_bounds(M, w, r)
+
+
+def _scalar_reduce(x, op, group, device):
+    import torch
+    r, w = rank_world(group)
+    if w == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    _dist().all_reduce(t, op=op, group=group)
+    return float(t.item())
+
+
+def reduce_max(x, group=None, device="cpu"):
+    """Maximum of a scalar over ranks (timings: the slowest rank)."""
+    return _scalar_reduce(x, _dist().ReduceOp.MAX, group, device)
+
+
+def reduce_sum(x, group=None, device="cpu"):
+    """Sum of a scalar over ranks (counts: nnz, determinants)."""
+    return _scalar_reduce(x, _dist().ReduceOp.SUM, group, device)
+
+
+def allgather_rows(x_local, N, group=None):
+    """The full length-N vector from every rank's row block (the gather
+    of pspmbv). Blocks differ in length only on the last rank; each is padded
+    to the longest so that one all_gather moves them all."""
+    import torch
+    r, w = rank_world(group)
+    if w == 1:
+        return x_local
+    per = N // w
+    longest = per + N % w
+    buf = torch.zeros(longest, dtype=x_local.dtype, device=x_local.device)
+    buf[:x_local.numel()] = x_local
+    parts = [torch.empty_like(buf) for _ in range(w)]
+    _dist().all_gather(parts, buf, group=group)
+    return torch.cat([p[:row_bounds(N, w, q)[1] - row_bounds(N, w, q)[0]]
+                      for q, p in enumerate(parts)])
+
+
+class DistCSR:
+    """This rank's row block of a row-distributed H: ``local`` is the
+    DeviceCSR of rows [lo, hi) against all N columns."""
+
+    def __init__(self, local, lo, hi, N, group=None, bra=None):
+        self.local, self.lo, self.hi, self.N = local, lo, hi, N
+        self.group = group
+        self._bra = bra
+
+    @property
+    def m_local(self):
+        return self.hi - self.lo
+
+    def nnz_total(self, device="cpu"):
+        return int(reduce_sum(self.local.nnz, self.group, device))
+
+    def diagonal(self, device=None):
+        """H_ii for the local rows i in [lo, hi), as a float64 tensor: the
+        diagonal of the block's diagonal tile (columns [lo, hi)), which p_davidson
+        preconditions with (the reference takes it from
+        H.diagonal_tile()). The block's own stored diagonal is the entry in
+        column == local row, the same thing only on the rank with lo = 0."""
+        import torch
+        if self.lo == 0 or self.m_local == 0:
+            d = self.local.diagonal()
+        else:
+            b = self._bra
+            if hasattr(b, "cpu"):
+                b = b.cpu().numpy().view(np.uint64)
+            d = np.atleast_1d(self.local.ham.matrix_element(b, b))
+        d = torch.from_numpy(np.ascontiguousarray(d, dtype=np.float64))
+        return d if device is None else d.to(device)
+
+    def local_spmv(self, x_full, y_local):
+        """y_local = H[lo:hi, :] x_full on this rank's GPU (device tensors)."""
+        import torch
+        if not (x_full.is_cuda and y_local.is_cuda):
+            raise RuntimeError("local_spmv needs CUDA tensors")
+        torch.cuda.current_stream().synchronize()
+        check(LIB.macis_b200_spmv(self.local.handle, 1, 1.0,
+                                  C.c_void_p(x_full.data_ptr()), self.N, 0.0,
+                                  C.c_void_p(y_local.data_ptr()),
+                                  max(self.m_local, 1), _lib.DEVICE_PTRS))
+        return y_local
+
+    def operator(self):
+        """RowBlockOperator over this block for p_davidson."""
+        import torch
+
+        def mv(x_full):
+            y = torch.empty(self.m_local, dtype=torch.float64,
+                            device=x_full.device)
+            return self.local_spmv(x_full, y)
+        return RowBlockOperator(mv, self.N, self.group)
+
+
+def make_dist_csr_hamiltonian(dets, ham_gen, H_thresh, index_t=np.int32,
+                              value_t=np.float64, group=None):
+    """make_dist_csr_hamiltonian (csr_hamiltonian.hpp:49-82): rows
+    local_rows(len(dets)) of H against the full determinant list, built on
+    this rank's GPU. `dets` is a host array or a CUDA tensor of the full list
+    (replicated on every rank, as in the reference)."""
+    p = _dev_ptr(dets)
+    if p is not None:
+        words = ham_gen.nbits // 64
+        N = dets.numel() // words
+        lo, hi = local_rows(N, group)
+        flat = dets.reshape(-1)
+        bra = flat[lo * words:hi * words]
+        local = DeviceCSR.build(ham_gen, bra, flat, H_thresh, index_t, value_t)
+    else:
+        d = _host_dets(dets, ham_gen.nbits)
+        N = len(d)
+        lo, hi = local_rows(N, group)
+        bra = d[lo:hi]
+        local = DeviceCSR.build(ham_gen, bra, d, H_thresh, index_t, value_t)
+    return DistCSR(local, lo, hi, N, group, bra)
+
+
+class RowBlockOperator:
+    """Operator action on row-distributed vectors: gather the full vector,
+    then apply this rank's row block (``local_matvec(x_full) -> y_local``)."""
+
+    def __init__(self, local_matvec, N, group=None):
+        self.local_matvec, self.N, self.group = local_matvec, N, group
+
+    def __call__(self, x_local):
+        return self.local_matvec(allgather_rows(x_local, self.N, self.group))
+
+
+def _allreduce_(t, group):
+    if rank_world(group)[1] > 1:
+        _dist().all_reduce(t, group=group)
+    return t
+
+
+def p_gram_schmidt(V, k, v, group=None):
+    """Project v (local rows, updated in place) out of the first k columns of
+    V twice, then normalise: p_gram_schmidt, davidson.hpp:228-256."""
+    Vk = V[:, :k]
+    for _ in range(2):
+        inner = _allreduce_(Vk.T @ v, group)
+        v -= Vk @ inner
+    nrm = math.sqrt(_allreduce_((v @ v).reshape(1), group).item())
+    v /= nrm
+    return v
+
+
+def p_rayleigh_ritz(V, AV, k, group=None):
+    """Eigenpairs of V^T A V over the first k columns, the k x k projection
+    summed over ranks, diagonalised on rank 0 and broadcast:
+    p_rayleigh_ritz, davidson.hpp:258-280."""
+    import torch
+    Cm = _allreduce_((V[:, :k].T @ AV[:, :k]).contiguous(), group)
+    r, w = rank_world(group)
+    lam = torch.empty(k, dtype=Cm.dtype, device=Cm.device)
+    vec = torch.empty_like(Cm)
+    if r == 0:
+        # syev with Uplo::Lower reads the lower triangle only
+        lam_, vec_ = torch.linalg.eigh(torch.tril(Cm) + torch.tril(Cm, -1).T)
+        lam.copy_(lam_)
+        vec.copy_(vec_)
+    if w > 1:
+        _dist().broadcast(lam, 0, group=group)
+        _dist().broadcast(vec, 0, group=group)
+    return lam, vec
+
+
+def p_davidson(N_local, max_m, op, D_local, tol, X_local, group=None,
+               log=None):
+    """Lowest eigenpair of a row-distributed symmetric operator:
+    p_davidson, davidson.hpp:283-394 (no restarts, like the reference).
+
+    `op(x_local) -> y_local` applies A (a RowBlockOperator); D_local holds
+    this rank's rows of diag(A); X_local (this rank's rows of the normalised
+    guess) is overwritten with the eigenvector. Every rank returns the same
+    (iterations, eigenvalue). Raises RuntimeError if the residual norm does
+    not reach `tol` within `max_m` subspace vectors."""
+    import torch
+    if N_local and X_local is None:
+        raise RuntimeError("Davidson: No Guess Provided")
+    dev, dt = X_local.device, torch.float64
+    V = torch.zeros((N_local, max_m + 1), dtype=dt, device=dev)
+    AV = torch.zeros((N_local, max_m + 1), dtype=dt, device=dev)
+    V[:, 0] = X_local
+    AV[:, 0] = op(V[:, 0].contiguous())
+    v1 = AV[:, 0].clone()
+    p_gram_schmidt(V, 1, v1, group)
+    V[:, 1] = v1
+    converged = False
+    it = 1
+    lam0 = 0.0
+    for i in range(1, max_m):
+        k = i + 1
+        AV[:, i] = op(V[:, i].contiguous())
+        lam, Cm = p_rayleigh_ritz(V, AV, k, group)
+        lam0 = float(lam[0].item())
+        c0 = Cm[:, 0]
+        X_local.copy_(V[:, :k] @ c0)
+        R = AV[:, :k] @ c0 - lam0 * X_local
+        res = math.sqrt(_allreduce_((R @ R).reshape(1), group).item())
+        if log is not None:
+            log.info(f"iter = {i:4d}, LAM(0) = {lam0:20.12e}, "
+                     f"RNORM = {res:20.12e}")
+        if res < tol:
+            converged = True
+            break
+        R = -R / (D_local - lam0)
+        p_gram_schmidt(V, k, R, group)
+        V[:, i + 1] = R
+        it += 1
+    if not converged:
+        raise RuntimeError("Davidson Did Not Converge!")
+    return it, lam0
+
+
+def gather_row_blocks(rowptr, colind, nzval, dst=0, group=None):
+    """Concatenate every rank's CSR row block (host arrays, blocks in rank
+    order) into the full matrix on rank `dst`; other ranks get None."""
+    dist = _dist()
+    r, w = rank_world(group)
+    mine = (np.asarray(rowptr, np.int64), np.asarray(colind, np.int64),
+            np.asarray(nzval))
+    if w == 1:
+        return mine
+    got = [None] * w if r == dst else None
+    dist.gather_object(mine, got, dst=dst, group=group)
+    if r != dst:
+        return None
+    rps, cis, nzs = [], [], []
+    off = 0
+    for q, (rp, ci, nz) in enumerate(got):
+        rps.append(rp[(1 if q else 0):] - rp[0] + off)
+        off += int(rp[-1] - rp[0])
+        cis.append(ci)
+        nzs.append(nz)
+    return np.concatenate(rps), np.concatenate(cis), np.concatenate(nzs)

@@ -1,0 +1,171 @@
+"""The multi-rank (N > 1) path on CPU: two gloo ranks, spawned processes.
+
+Each rank computes its row block [lo, hi) of H with the oracle (the stand-in
+for the block libmacis_b200 builds on that rank's GPU), and the host logic of
+macis_b200.dist is checked: the row partition of make_dist_csr_hamiltonian
+(csr_hamiltonian.hpp:49-82), gathering blocks back into the full matrix, the
+max / sum reductions the benchmark uses for its timings and counts, and the
+parallel Davidson (p_davidson, davidson.hpp:283-394) against the serial
+solve on the full matrix."""
+import socket
+import traceback
+
+import numpy as np
+import pytest
+
+from cases import fci
+
+WORLD = 2
+TIMEOUT_S = 240
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _problem():
+    # 35 x 35 = 1225 determinants: an odd count, so the last rank gets the
+    # extra row
+    return fci(7, 3, 3, 64, seed=4)
+
+
+def _block_op(port, hp, dets, lo, hi):
+    import torch
+    rp, ci, nz = port.build_csr(hp, dets[lo:hi], dets, np.finfo(float).eps)
+
+    def mv(x_full):
+        return torch.from_numpy(port.spmv(rp, ci, nz, x_full.numpy()))
+    return (rp, ci, nz), mv
+
+
+def _rank_main(rank, port_no, case, q):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    try:
+        dist.init_process_group(
+            "gloo", init_method=f"tcp://127.0.0.1:{port_no}", rank=rank,
+            world_size=WORLD, timeout=datetime.timedelta(seconds=60))
+        import oracle
+        from macis_b200 import dist as md
+        port = oracle.port()
+        T, V, dets = _problem()
+        N = len(dets)
+        hp = port.ham(64, 7, T, V)
+        lo, hi = md.local_rows(N)
+        (rp, ci, nz), mv = _block_op(port, hp, dets, lo, hi)
+        out = {"rank": rank, "lo": lo, "hi": hi}
+        if case == "csr":
+            full = md.gather_row_blocks(rp, ci, nz)
+            out["full"] = full
+            out["max"] = md.reduce_max(10.0 * (rank + 1))
+            out["sum"] = md.reduce_sum(float(len(ci)))
+            xl = torch.arange(lo, hi, dtype=torch.float64)
+            out["gathered"] = md.allgather_rows(xl, N).numpy()
+        elif case == "davidson":
+            D = np.empty(hi - lo)
+            rows = np.repeat(np.arange(hi - lo), np.diff(rp))
+            on = ci == rows + lo
+            D[rows[on]] = nz[on]
+            # guess: unit vector on the globally lowest diagonal element
+            allD = md.allgather_rows(torch.from_numpy(D), N).numpy()
+            g = int(np.argmin(allD))
+            X = torch.zeros(hi - lo, dtype=torch.float64)
+            if lo <= g < hi:
+                X[g - lo] = 1.0
+            op = md.RowBlockOperator(mv, N)
+            it, E = md.p_davidson(hi - lo, 200, op, torch.from_numpy(D),
+                                  1e-8, X)
+            out.update(it=it, E=E, X=md.allgather_rows(X, N).numpy(),
+                       guess=g)
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put(out)
+    except Exception:
+        q.put({"rank": rank, "error": traceback.format_exc()})
+
+
+def _run(case):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, p, case, q))
+             for r in range(WORLD)]
+    for pr in procs:
+        pr.start()
+    res = {}
+    try:
+        for _ in range(WORLD):
+            o = q.get(timeout=TIMEOUT_S)
+            res[o["rank"]] = o
+    finally:
+        for pr in procs:
+            pr.join(timeout=30)
+            if pr.is_alive():
+                pr.kill()
+    for o in res.values():
+        assert "error" not in o, o["error"]
+    return res
+
+
+def test_row_blocks_gather_and_reductions(port):
+    res = _run("csr")
+    T, V, dets = _problem()
+    N = len(dets)
+    assert (res[0]["lo"], res[0]["hi"]) == (0, N // 2)
+    assert (res[1]["lo"], res[1]["hi"]) == (N // 2, N)
+    full = port.build_csr(port.ham(64, 7, T, V), dets, dets,
+                          np.finfo(float).eps)
+    got = res[0]["full"]
+    assert np.array_equal(got[0], full[0])
+    assert np.array_equal(got[1], full[1])
+    assert np.array_equal(got[2], full[2])
+    assert res[1]["full"] is None
+    for r in range(WORLD):
+        assert res[r]["max"] == 20.0
+        assert res[r]["sum"] == float(len(full[1]))
+        assert np.array_equal(res[r]["gathered"], np.arange(N, dtype=float))
+
+
+def test_p_davidson_two_ranks_matches_serial(port):
+    res = _run("davidson")
+    T, V, dets = _problem()
+    rp, ci, nz = port.build_csr(port.ham(64, 7, T, V), dets, dets,
+                                np.finfo(float).eps)
+    X0 = np.zeros(len(dets))
+    X0[res[0]["guess"]] = 1.0
+    E, it, X = port.davidson(rp, ci, nz, 200, 1e-8, X0)
+    for r in range(WORLD):
+        assert res[r]["E"] == res[0]["E"]             # same on every rank
+        assert abs(res[r]["E"] - E) < 1e-9
+        assert abs(res[r]["it"] - it) <= 1
+        Xr = res[r]["X"]
+        assert abs(abs(Xr @ X) / (np.linalg.norm(Xr) * np.linalg.norm(X))
+                   - 1.0) < 1e-10
+
+
+def test_p_davidson_single_rank_no_group(port):
+    """Without a process group the same code is the serial solver."""
+    import torch
+
+    from macis_b200 import dist as md
+    T, V, dets = _problem()
+    N = len(dets)
+    assert md.rank_world() == (0, 1)
+    (rp, ci, nz), mv = _block_op(port, port.ham(64, 7, T, V), dets, 0, N)
+    D = np.asarray([nz[rp[i]:rp[i + 1]][ci[rp[i]:rp[i + 1]] == i][0]
+                    for i in range(N)])
+    X = torch.zeros(N, dtype=torch.float64)
+    X[int(np.argmin(D))] = 1.0
+    X0 = X.numpy().copy()
+    it, E = md.p_davidson(N, 200, md.RowBlockOperator(mv, N),
+                          torch.from_numpy(D), 1e-8, X)
+    E_ref, it_ref, _ = port.davidson(rp, ci, nz, 200, 1e-8, X0)
+    assert abs(E - E_ref) < 1e-9 and abs(it - it_ref) <= 1
+    with pytest.raises(RuntimeError, match="Did Not Converge"):
+        md.p_davidson(N, 3, md.RowBlockOperator(mv, N), torch.from_numpy(D),
+                      1e-14, torch.from_numpy(X0.copy()))
