@@ -207,7 +207,77 @@ struct DPData {
   const int64_t* l4off;    // UB+1
   const int32_t* l4col;
   const uint32_t* l4info;
+  // same-spin parts of the single-excitation elements (dp_pg_k)
+  const int64_t* pgaoff;   // UA+1
+  const double* pga;
+  const int64_t* pgboff;   // UB+1
+  const double* pgb;
 };
+
+// Occupied and empty orbitals of a spin string, in ascending order, into
+// occ[0..no) and vir[0..n-no) (one orbital per lane).
+template <int NSW>
+__device__ __forceinline__ void spin_lists(const Spin<NSW>& s, int n, int lane,
+                                           uint8_t* occ, uint8_t* vir) {
+  for(int i = lane; i < n; i += 32) {
+    int below = 0;  // occupied orbitals below i
+#pragma unroll
+    for(int w = 0; w < NSW; ++w) {
+      const int lo = 64 * w;
+      if(i > lo)
+        below += __popcll(s.w[w] &
+                          (i - lo >= 64 ? ~0ull : ((1ull << (i - lo)) - 1)));
+    }
+    if(sp_test(s, i))
+      occ[below] = uint8_t(i);
+    else
+      vir[i - below] = uint8_t(i);
+  }
+}
+
+// Singles per spin string: popcount * (n - popcount).
+template <int NSW>
+__global__ void dp_pgcount_k(const uint64_t* strings, int64_t ns, int n,
+                             int64_t* cnt) {
+  for(int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < ns;
+      i += int64_t(gridDim.x) * blockDim.x) {
+    const int no = sp_popc(ld_spin<NSW>(strings, i));
+    cnt[i] = int64_t(no) * (n - no);
+  }
+}
+
+// Same-spin part of every single excitation of every spin string s:
+//   pg[off[s] + i nv + j] = T(v,o) + sum_{p in occ(s)} G_red(p,v,o)
+// with v the i-th occupied and o the j-th empty orbital of s, summed in the
+// order of matrix_element_2 (matrix_elements.hpp:86-104: T, then the
+// same-spin G_red terms by ascending p). The element of a determinant adds
+// the other-spin V_red terms to this partial sum in the same order, so the
+// split is bit-exact. One warp per string.
+template <int NSW>
+__global__ void dp_pg_k(Ints I, const uint64_t* strings, int64_t ns,
+                        const int64_t* off, double* pg) {
+  __shared__ uint8_t lists[8][256];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int n = I.n, n2 = n * n;
+  uint8_t* occ = lists[wid];
+  uint8_t* vir = occ + 128;
+  for(int64_t st = int64_t(blockIdx.x) * 8 + wid; st < ns;
+      st += int64_t(gridDim.x) * 8) {
+    const Spin<NSW> sp = ld_spin<NSW>(strings, st);
+    const int no = sp_popc(sp), nv = n - no;
+    __syncwarp();
+    spin_lists<NSW>(sp, n, lane, occ, vir);
+    __syncwarp();
+    double* out = pg + off[st];
+    for(int u = lane; u < no * nv; u += 32) {
+      const int v = occ[u / nv], o = vir[u % nv];
+      double h = __ldg(I.T + v + o * n);
+      const double* Gov = I.G_red + v * n + o * n2;
+      for(int k = 0; k < no; ++k) h += __ldg(Gov + occ[k]);
+      out[u] = h;
+    }
+  }
+}
 
 // Per alpha string: how many connected A' at popcount 0, 2, 4.
 __global__ void dp_acount_k(const int64_t* aoff, const uint32_t* ainfo,
@@ -274,22 +344,18 @@ constexpr int DP_WARPS = 8;
 constexpr int DP_THREADS = 32 * DP_WARPS;
 
 struct DPShared {
-  int n, stage_ints;
+  int n;
   int64_t l2max, l4max;
-  size_t ints_off, f_off, l2_off, l4_off, occ_off, bytes;
+  size_t f_off, l2_off, l4_off, occ_off, bytes;
 };
 
-__host__ __device__ inline DPShared dp_shared_layout(int n, int stage_ints,
-                                                     int64_t l2max,
+__host__ __device__ inline DPShared dp_shared_layout(int n, int64_t l2max,
                                                      int64_t l4max) {
   DPShared L;
   L.n = n;
-  L.stage_ints = stage_ints;
   L.l2max = l2max;
   L.l4max = l4max;
   size_t o = 0;
-  L.ints_off = o;
-  if(stage_ints) o += (size_t(n) * n + 2 * size_t(n) * n * n) * 8;
   L.f_off = o;
   o += size_t(DP_WARPS) * 2 * n * n * 8;
   L.l2_off = o;
@@ -375,20 +441,6 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int n = L.n;
   const int n2 = n * n;
-  const double* sT = I.T;
-  const double* sG = I.G_red;
-  const double* sV = I.V_red;
-  if(L.stage_ints) {
-    double* p = reinterpret_cast<double*>(dsm + L.ints_off);
-    for(int x = threadIdx.x; x < n2; x += DP_THREADS) p[x] = I.T[x];
-    for(int x = threadIdx.x; x < n2 * n; x += DP_THREADS) {
-      p[n2 + x] = I.G_red[x];
-      p[n2 + n2 * n + x] = I.V_red[x];
-    }
-    sT = p;
-    sG = p + n2;
-    sV = p + n2 + n2 * n;
-  }
   double* F = reinterpret_cast<double*>(dsm + L.f_off) + size_t(wid) * 2 * n2;
   const uint2* sl2 = reinterpret_cast<const uint2*>(dsm + L.l2_off);
   const uint2* sl4 = reinterpret_cast<const uint2*>(dsm + L.l4_off);
@@ -428,57 +480,35 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
     for(int S = 0; S < 2; ++S) {
       no[S] = sp_popc(sp[S]);
       nv[S] = n - no[S];
-      for(int i = lane; i < n; i += 32) {
-        int below = 0;  // occupied orbitals below i
-#pragma unroll
-        for(int w = 0; w < NSW; ++w) {
-          const int lo = 64 * w;
-          if(i > lo)
-            below += __popcll(sp[S].w[w] &
-                              (i - lo >= 64 ? ~0ull : ((1ull << (i - lo)) - 1)));
-        }
-        if(sp_test(sp[S], i))
-          occl[S * 128 + below] = uint8_t(i);
-        else
-          virl[S * 128 + (i - below)] = uint8_t(i);
-      }
+      spin_lists<NSW>(sp[S], n, lane, occl + S * 128, virl + S * 128);
     }
     __syncwarp();
-    // singles table: F[spin][v*n + o] = T(v,o) + sum_{p in occ_same}
-    // G_red(p,v,o) + sum_{p in occ_other} V_red(p,v,o)  (matrix_elements.hpp:
-    // 76-96 without the sign), v occupied and o empty in the bra
+    // singles table: F[spin][v*n + o] = (T(v,o) + sum_{p in occ_same}
+    // G_red(p,v,o)) + sum_{p in occ_other} V_red(p,v,o)
+    // (matrix_elements.hpp:86-104 without the sign), v occupied and o empty
+    // in the bra. The bracket is the per-string partial sum of dp_pg_k.
     {
       const int nsa = no[0] * nv[0], nsb = no[1] * nv[1];
+      const double* __restrict__ pga = d.pga + d.pgaoff[A];
+      const double* __restrict__ pgb = d.pgb + d.pgboff[B];
+      // i = u / nv by a float product: (u + 0.5) / nv stays >= 0.5 / nv
+      // away from an integer, far above the rounding error for u < 2^14
+      const float rva = 1.0f / float(nv[0] > 0 ? nv[0] : 1);
+      const float rvb = 1.0f / float(nv[1] > 0 ? nv[1] : 1);
       for(int t = lane; t < nsa + nsb; t += 32) {
         // selects instead of no[S] / nv[S]: a dynamic index would put the
         // arrays in local memory
         const int S = t < nsa ? 0 : 1;
         const int u = S ? t - nsa : t;
         const int nvS = S ? nv[1] : nv[0];
-        const int noS = S ? no[1] : no[0], noO = S ? no[0] : no[1];
-        const int v = occl[S * 128 + u / nvS], o = virl[S * 128 + u % nvS];
-        double h = sT[v + o * n];
-        const double* Gov = sG + v * n + o * n2;
-        const double* Vov = sV + v * n + o * n2;
-        // loads 8 at a time, additions in the reference order
-        for(int p0 = 0; p0 < noS; p0 += 8) {
-          double g[8];
-#pragma unroll
-          for(int k = 0; k < 8; ++k)
-            g[k] = p0 + k < noS ? Gov[occl[S * 128 + p0 + k]] : 0.0;
-#pragma unroll
-          for(int k = 0; k < 8; ++k)
-            if(p0 + k < noS) h += g[k];
-        }
-        for(int p0 = 0; p0 < noO; p0 += 8) {
-          double g[8];
-#pragma unroll
-          for(int k = 0; k < 8; ++k)
-            g[k] = p0 + k < noO ? Vov[occl[(1 - S) * 128 + p0 + k]] : 0.0;
-#pragma unroll
-          for(int k = 0; k < 8; ++k)
-            if(p0 + k < noO) h += g[k];
-        }
+        const int noO = S ? no[0] : no[1];
+        const int i = int((float(u) + 0.5f) * (S ? rvb : rva));
+        const int v = occl[S * 128 + i], o = virl[S * 128 + (u - i * nvS)];
+        double h = __ldg((S ? pgb : pga) + u);
+        const double* Vov = I.V_red + v * n + o * n2;
+        const uint8_t* po = occl + (1 - S) * 128;
+#pragma unroll 4
+        for(int k = 0; k < noO; ++k) h += __ldg(Vov + po[k]);
         F[S * n2 + v * n + o] = h;
       }
     }
@@ -1255,8 +1285,30 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       dp_encode_k<<<grid_for(size_t(n2_), 256, 8 * sms), 256, 0, s>>>(l2info, n2_, nn0, 1), note_launch();
       dp_encode_k<<<grid_for(size_t(n4_), 256, 8 * sms), 256, 0, s>>>(l4info, n4_, nn0, 2), note_launch();
     }
+    // orbital lists of the kernels below hold 128 entries per spin
+    MB_REQUIRE(nket < (size_t(1) << 31) && h->norb <= 127,
+               MACIS_B200_ECAPACITY,
+               "direct-product fill needs < 2^31 determinants, norb < 128");
+    // same-spin partial sums of the singles, per alpha and per beta string
+    auto pg_table = [&](const uint64_t* strs, size_t ns, int64_t*& off,
+                        double*& pg) {
+      int64_t* cnt = A.get<int64_t>(ns + 1);
+      off = A.get<int64_t>(ns + 1);
+      dp_pgcount_k<NSW><<<grid_for(ns, 256, 4 * sms), 256, 0, s>>>(
+          strs, int64_t(ns), h->norb, cnt), note_launch();
+      exclusive_scan<int64_t, int64_t>(cnt, off, ns, off + ns, A);
+      const int64_t tot = to_host(off + ns, s);
+      pg = A.get<double>(size_t(std::max<int64_t>(tot, 1)));
+      dp_pg_k<NSW><<<grid_for(ns * 32, 256, 8 * sms), 256, 0, s>>>(
+          I, strs, int64_t(ns), off, pg), note_launch();
+    };
+    int64_t *pgaoff, *pgboff;
+    double *pga, *pgb;
+    pg_table(ua, UA, pgaoff, pga);
+    pg_table(ub, UB, pgboff, pgb);
     DPData d{int64_t(UA), int64_t(UB), ua, ub, aoff, acol, ainfo,
-             l2off, l2col, l2info, l4off, l4col, l4info};
+             l2off, l2col, l2info, l4off, l4col, l4info,
+             pgaoff, pga, pgboff, pgb};
     // shared-memory plan: integrals for the singles if they fit, the longest
     // beta lists, per-warp singles tables
     int64_t l2max = 0, l4max = 0;
@@ -1271,23 +1323,18 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       }
     }
     const int nn = h->norb;
-    const size_t ints_bytes = (size_t(nn) * nn + 2 * size_t(nn) * nn * nn) * 8;
     // The integrals of the singles are read through L1 rather than staged in
     // shared memory: per-CTA copies would take the L1 capacity that the
     // G / V gathers need (measured: staging made the C2 fill 10% slower).
-    int stage = 0;
-    (void)ints_bytes;
     l2max = std::min<int64_t>(l2max, 2048);
     l4max = std::min<int64_t>(l4max, 4096);
-    DPShared Ls = dp_shared_layout(nn, stage, l2max, l4max);
+    DPShared Ls = dp_shared_layout(nn, l2max, l4max);
     if(Ls.bytes > 200 * 1024) {
-      Ls = dp_shared_layout(nn, 0, std::min<int64_t>(l2max, 512),
+      Ls = dp_shared_layout(nn, std::min<int64_t>(l2max, 512),
                             std::min<int64_t>(l4max, 1024));
     }
     MB_REQUIRE(Ls.bytes <= 220 * 1024, MACIS_B200_EINVAL,
                "norb too large for the direct-product fill");
-    MB_REQUIRE(nket < (size_t(1) << 31) && nn <= 127, MACIS_B200_ECAPACITY,
-               "direct-product fill needs < 2^31 determinants");
     MB_CUDA(cudaFuncSetAttribute(dp_fill_k<NBITS, CI, VT>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(Ls.bytes)));
