@@ -2,6 +2,8 @@
 
     python -m macis_b200.profile_cases hbuild_c1   # CAS(10e,10o) CSR build
     python -m macis_b200.profile_cases hbuild_c2   # CAS(12e,12o) CSR build
+    python -m macis_b200.profile_cases hbuild_c2s  # 12 orbitals, 3a/6b: the
+        # beta lists of CAS(12e,12o) at a quarter of its output (3.3 GB)
     python -m macis_b200.profile_cases spmv_c1     # FP64 SpMV on CAS(10e,10o)
     python -m macis_b200.profile_cases hbuild_sel  # selected (shuffled) space
     python -m macis_b200.profile_cases asci_n48    # one ASCI search, n = 48
@@ -29,13 +31,14 @@ import macis_b200 as mb
 EPS = float(np.finfo(np.float64).eps)
 
 
-def fci(norb, k, nbits=64, seed=0):
+def fci(norb, k, nbits=64, seed=0, kb=None):
     T, V = mb.synthetic_integrals(norb, seed)
-    return T, V, mb.generate_hilbert_space(norb, k, k, nbits)
+    return T, V, mb.generate_hilbert_space(norb, k, k if kb is None else kb,
+                                           nbits)
 
 
-def hbuild(norb, k, reps, shuffle=False):
-    T, V, dets = fci(norb, k)
+def hbuild(norb, k, reps, shuffle=False, kb=None):
+    T, V, dets = fci(norb, k, kb=kb)
     if shuffle:
         dets = dets[np.random.default_rng(1).permutation(len(dets))]
     H = mb.HamiltonianGenerator(T, V, 64)
@@ -183,6 +186,8 @@ def main():
         hbuild(10, 5, a.reps)
     elif a.case == "hbuild_c2":
         hbuild(12, 6, a.reps)
+    elif a.case == "hbuild_c2s":
+        hbuild(12, 3, a.reps, kb=6)
     elif a.case == "hbuild_sel":
         hbuild(10, 5, a.reps, shuffle=True)
     elif a.case == "spmv_c1":
