@@ -39,49 +39,6 @@ struct Error : std::runtime_error {
   } while(0)
 
 // ----------------------------------------------------------- spin strings
-// Streaming (evict-first) global stores without a compiler memory barrier.
-// The CUDA __stcs intrinsics carry a "memory" clobber, which keeps every
-// later load (shared ones included) behind every earlier store, so a
-// load -> store loop waits out the load latency once per iteration. These
-// are for output that no thread of the kernel reads back.
-__device__ __forceinline__ void st_cs(int* p, int v) {
-  asm volatile("st.global.cs.s32 [%0], %1;" ::"l"(p), "r"(v));
-}
-__device__ __forceinline__ void st_cs(long long* p, long long v) {
-  asm volatile("st.global.cs.s64 [%0], %1;" ::"l"(p), "l"(v));
-}
-__device__ __forceinline__ void st_cs(double* p, double v) {
-  asm volatile("st.global.cs.f64 [%0], %1;" ::"l"(p), "d"(v));
-}
-__device__ __forceinline__ void st_cs(float* p, float v) {
-  asm volatile("st.global.cs.f32 [%0], %1;" ::"l"(p), "f"(v));
-}
-// Read-only global loads through the non-coherent path, as non-volatile asm
-// so that the compiler may issue them early (the __ldg intrinsics are
-// volatile). Only for data that the kernel never writes.
-__device__ __forceinline__ double ld_nc(const double* p) {
-  double r;
-  asm("ld.global.nc.f64 %0, [%1];" : "=d"(r) : "l"(p));
-  return r;
-}
-__device__ __forceinline__ int ld_nc(const int* p) {
-  int r;
-  asm("ld.global.nc.s32 %0, [%1];" : "=r"(r) : "l"(p));
-  return r;
-}
-__device__ __forceinline__ unsigned ld_nc(const unsigned* p) {
-  unsigned r;
-  asm("ld.global.nc.u32 %0, [%1];" : "=r"(r) : "l"(p));
-  return r;
-}
-__device__ __forceinline__ int4 ld_nc(const int4* p) {
-  int4 r;
-  asm("ld.global.nc.v4.s32 {%0,%1,%2,%3}, [%4];"
-      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
-      : "l"(p));
-  return r;
-}
-
 template <int NSW>
 struct Spin {
   uint64_t w[NSW];

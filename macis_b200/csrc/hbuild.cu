@@ -212,13 +212,10 @@ struct DPData {
   const double* pga;
   const int64_t* pgboff;   // UB+1
   const double* pgb;
-  // per alpha string, from its connection list (dp_atab_k)
-  const int64_t* asoff;    // UA+1: alpha singles of A at asoff[A]..
-  const int4* aseg;        // per single: A' UB, VT row offset, position, F
-  const int64_t* adoff;    // UA+1: alpha doubles of A at adoff[A]..
-  const int4* adbl;        // per double: A' UB, position, value (2 words)
-  const int2* asame;       // per A: singles / doubles before A itself
-  // per beta L4 list entry: the signed G value of a beta double
+  // signed G value of every double of the alpha and beta L4 lists (0 for
+  // the other entries): the fill reads it with the list entry instead of
+  // gathering G
+  const double* aval;
   const double* l4val;
 };
 
@@ -287,67 +284,10 @@ __global__ void dp_pg_k(Ints I, const uint64_t* strings, int64_t ns,
   }
 }
 
-// Row positions of a determinant (A, B) without a scan. The entries of the
-// row are, in column order, the concatenation over the connected A' of A
-// (ascending) of: the L4(B) list when A' = A, the L2(B) list when A' is a
-// single excitation of A, the one entry (A', B) when A' is a double. Entry k
-// of A's list therefore starts at c0 n4l(B) + c1 n2l(B) + c2, with c0, c1, c2
-// the same / single / double entries before it. This kernel writes, per
-// alpha string (one warp each):
-//   aseg[asoff[A] + s]  s-th single: (A' UB, VT row offset v1 + o1 n times
-//                       n^2, c2 | c0 << 31, singles-table index | sign bit)
-//   adbl[adoff[A] + k]  k-th double: (A' UB, c0 | c1 << 1, the signed
-//                       G value as two words); its c2 is k
-//   asame[A]            (c1, c2) before A itself
-__global__ void dp_atab_k(const int64_t* aoff, const int32_t* acol,
-                          const uint32_t* ainfo, int64_t UA, int32_t UB, int n,
-                          const double* G, const int64_t* asoff,
-                          const int64_t* adoff, int4* aseg, int4* adbl,
-                          int2* asame) {
-  const int lane = threadIdx.x & 31;
-  const int n2 = n * n;
-  const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
-  for(int64_t A = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      A < UA; A += nw) {
-    int c0 = 0, c1 = 0, c2 = 0;
-    const int64_t e = aoff[A + 1];
-    for(int64_t c = aoff[A]; c < e; c += 32) {
-      const int64_t j = c + lane;
-      const bool valid = j < e;
-      const uint32_t ai = valid ? ainfo[j] : 0u;
-      const int cls = valid ? int((ai >> 29) & 3u) : 3;
-      const unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
-      const unsigned m1 = __ballot_sync(0xffffffffu, cls == 1);
-      const unsigned m2 = __ballot_sync(0xffffffffu, cls == 2);
-      const unsigned lt = (1u << lane) - 1u;
-      const int e0 = c0 + __popc(m0 & lt), e1 = c1 + __popc(m1 & lt),
-                e2 = c2 + __popc(m2 & lt);
-      if(valid) {
-        const int32_t cb = acol[j] * UB;
-        if(cls == 2) {
-          const double g = G[ai & 0x0FFFFFFFu];
-          const double v = (ai >> 31) ? -g : g;
-          adbl[adoff[A] + e2] = make_int4(cb, e0 | (e1 << 1),
-                                          __double2loint(v), __double2hiint(v));
-        } else if(cls == 1) {
-          aseg[asoff[A] + e1] = make_int4(
-              cb, int((ai & 0x3FFFu) * uint32_t(n2)),
-              int(uint32_t(e2) | (uint32_t(e0) << 31)),
-              int(((ai >> 14) & 0x3FFFu) | (ai & 0x80000000u)));
-        } else {
-          asame[A] = make_int2(e1, e2);
-        }
-      }
-      c0 += __popc(m0);
-      c1 += __popc(m1);
-      c2 += __popc(m2);
-    }
-  }
-}
-
-// Signed G value of each beta double of the L4 lists (0 for other entries).
-__global__ void dp_l4val_k(const uint32_t* info, int64_t m, const double* G,
-                           double* val) {
+// Signed G value of each double of an encoded connection list (0 for the
+// other entries).
+__global__ void dp_dval_k(const uint32_t* info, int64_t m, const double* G,
+                          double* val) {
   for(int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
       i += int64_t(gridDim.x) * blockDim.x) {
     const uint32_t e = info[i];
@@ -357,16 +297,6 @@ __global__ void dp_l4val_k(const uint32_t* info, int64_t m, const double* G,
       v = (e >> 31) ? -g : g;
     }
     val[i] = v;
-  }
-}
-
-// Singles and doubles counts of each alpha string, as int64 (scan inputs).
-__global__ void dp_split_counts_k(const int32_t* na, int64_t UA, int64_t* ns,
-                                  int64_t* nd) {
-  for(int64_t A = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; A < UA;
-      A += int64_t(gridDim.x) * blockDim.x) {
-    ns[A] = na[3 * A + 1];
-    nd[A] = na[3 * A + 2];
   }
 }
 
@@ -423,16 +353,19 @@ __device__ __forceinline__ float store_val<float>(double h, bool is_diag) {
 }
 
 // Direct-product fill. A CTA of DP_WARPS warps takes DP_WARPS rows that
-// share one beta string B (rows (A..A+7, B)); the beta lists L2(B), L4(B) and
-// the signed values of L4's beta doubles are staged once in shared memory.
-// Each warp first evaluates the Slater-Condon singles of its bra into a
+// share one beta string B (rows (A..A+7, B)); the beta lists L2(B), L4(B)
+// and the signed values of L4's beta doubles are staged once in shared
+// memory.
+// Each warp first evaluates all Slater-Condon singles of its bra into a
 // shared table F[spin][v*n + o] (per-string partial sums plus the other-spin
-// terms, reference summation order), then writes the row in three passes
-// whose positions come from per-alpha-string tables (dp_atab_k) instead of
-// a scan: the alpha doubles, the same-alpha segment, and the alpha-single
-// segments (lanes over the beta list, the warp over the segments). Stores
-// are streaming (the output must not evict the integrals from L2).
+// terms, reference summation order), then emits the row: entries are produced in ascending column order
+// as the concatenation over connected alpha strings A' of the beta lists,
+// two 32-entry rounds in flight, threshold compaction by ballot and
+// streaming stores (the output must not evict the integrals from L2).
 constexpr int DP_WARPS = 8;
+// resident CTAs per SM: 80 registers per thread (measured: 3 x 8 warps at
+// 80 registers beat 4 x 8 warps at 64 on the CAS(12e,12o) fill by 7%)
+constexpr int DP_CTAS = 3;
 constexpr int DP_THREADS = 32 * DP_WARPS;
 
 struct DPShared {
@@ -460,16 +393,6 @@ __host__ __device__ inline DPShared dp_shared_layout(int n, int64_t l2max,
   o += size_t(DP_WARPS) * 4 * 128;  // occ/vir lists, both spins
   L.bytes = (o + 15) & ~size_t(15);
   return L;
-}
-
-template <typename CI, typename VT>
-__device__ __forceinline__ void dp_store(CI* colind, VT* nzval, int64_t pos,
-                                         int64_t col, double h, bool isd) {
-  __stcs(reinterpret_cast<typename std::conditional<sizeof(CI) == 4, int,
-                                                    long long>::type*>(colind) +
-             pos,
-         (typename std::conditional<sizeof(CI) == 4, int, long long>::type)col);
-  __stcs(nzval + pos, store_val<VT>(h, isd));
 }
 
 // Packed list words of the fill (y of a uint2 whose x is the partner
@@ -519,7 +442,7 @@ __device__ __forceinline__ double sgnd(uint32_t w, double v) {
 }
 
 template <int NBITS, typename CI, typename VT>
-__global__ void __launch_bounds__(DP_THREADS, 4)
+__global__ void __launch_bounds__(DP_THREADS, DP_CTAS)
     dp_fill_k(Ints I, const double* __restrict__ Vt, DPData d, DPShared L,
               const double* __restrict__ hdiag,
               const int64_t* __restrict__ rowptr, CI* __restrict__ colind,
@@ -528,8 +451,8 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
               int64_t nrows) {
   constexpr int NSW = DetTraits<NBITS>::NSW;
   extern __shared__ __align__(16) unsigned char dsm[];
-  // a block of up to 32 alpha-single segments of the row: (row position,
-  // column base, VT row offset, sign bit) and the alpha-single value
+  // alpha-single segments of the current chunk: (row position, column
+  // base, VT row offset, sign bit) and the alpha-single value
   __shared__ int4 seg_d[DP_WARPS][32];
   __shared__ double seg_single[DP_WARPS][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -555,7 +478,6 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
     __syncthreads();  // previous item's lists are no longer read
     uint2* wl2 = reinterpret_cast<uint2*>(dsm + L.l2_off);
     uint2* wl4 = reinterpret_cast<uint2*>(dsm + L.l4_off);
-    double* wl4v = reinterpret_cast<double*>(dsm + L.l4v_off);
     const bool s2 = n2l <= L.l2max, s4 = n4l <= L.l4max;
     if(s2)
       for(int x = threadIdx.x; x < n2l; x += DP_THREADS)
@@ -563,7 +485,7 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
     if(s4)
       for(int x = threadIdx.x; x < n4l; x += DP_THREADS) {
         wl4[x] = make_uint2(uint32_t(d.l4col[l4b + x]), d.l4info[l4b + x]);
-        wl4v[x] = d.l4val[l4b + x];
+        reinterpret_cast<double*>(dsm + L.l4v_off)[x] = d.l4val[l4b + x];
       }
     __syncthreads();
     const int64_t A = A_lo + ac * DP_WARPS + wid;
@@ -601,83 +523,124 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
         const int noO = S ? no[0] : no[1];
         const int i = int((float(u) + 0.5f) * (S ? rvb : rva));
         const int v = occl[S * 128 + i], o = virl[S * 128 + (u - i * nvS)];
-        double h = ld_nc((S ? pgb : pga) + u);
+        double h = __ldg((S ? pgb : pga) + u);
         const double* Vov = I.V_red + v * n + o * n2;
         const uint8_t* po = occl + (1 - S) * 128;
 #pragma unroll 4
-        for(int k = 0; k < noO; ++k) h += ld_nc(Vov + po[k]);
+        for(int k = 0; k < noO; ++k) h += __ldg(Vov + po[k]);
         F[S * n2 + v * n + o] = h;
       }
     }
     __syncwarp();
     const double hd = hdiag[row];
     const int64_t out0 = rowptr[row];
-    const int32_t rowlen = int32_t(rowptr[row + 1] - out0);
     CI* __restrict__ rc = colind + out0;
     VT* __restrict__ rv = nzval + out0;
-    int32_t dropped = 0;  // this lane's count
-    using CS = typename std::conditional<sizeof(CI) == 4, int, long long>::type;
-    CS* __restrict__ rcs = reinterpret_cast<CS*>(rc);
-    // (1) alpha doubles: beta unchanged, one entry each
-    {
-      const int64_t k0 = d.adoff[A];
-      const int32_t nd = int32_t(d.adoff[A + 1] - k0);
-      const int4* __restrict__ tab = d.adbl + k0;
-      for(int32_t k = lane; k < nd; k += 32) {
-        const int4 e = ld_nc(tab + k);
-        const int32_t p = (e.y & 1) * n4l + (e.y >> 1) * n2l + k;
-        const double h = __hiloint2double(e.w, e.z);
-        const bool keep = fabs(h) > thresh;
-        dropped += keep ? 0 : 1;
-        st_cs(rcs + p, CS(keep ? e.x + B : -1));
-        st_cs(rv + p, store_val<VT>(h, false));
-      }
-    }
-    // (2) the same-alpha segment: every beta string within two excitations
-    {
-      const int2 sm = d.asame[A];
-      const int32_t p0 = sm.x * n2l + sm.y;
-      const int32_t cA = int32_t(A) * UB;
-      const int32_t nt = sm.x < 0 ? 0 : n4l;  // A not in its own list
-      for(int32_t t = lane; t < nt; t += 32) {
-        const uint2 ent = s4 ? sl4[t]
-                             : make_uint2(uint32_t(ld_nc(d.l4col + l4b + t)),
-                                          ld_nc(d.l4info + l4b + t));
-        const double vd = s4 ? sl4v[t] : ld_nc(d.l4val + l4b + t);
-        const uint32_t cb = (ent.y >> 29) & 3u, off = ent.y & 0x0FFFFFFFu;
-        // singles from this row's table (offsets < 2 n^2), doubles signed
-        const double vf = F[off < uint32_t(2 * n2) ? off : 0u];
-        const int32_t col = cA + int32_t(ent.x);
-        const double h = cb == 0 ? hd : cb == 1 ? sgnd(ent.y, vf) : vd;
-        const bool keep = fabs(h) > thresh;
-        dropped += keep ? 0 : 1;
-        const bool isd = keep && col == row;
-        st_cs(rcs + p0 + t, CS(keep ? col : -1));
-        st_cs(rv + p0 + t, store_val<VT>(h, isd));
-        if(isd) diag[row] = h;
-      }
-    }
-    // (3) alpha singles: one segment of n2l entries (beta within one
-    // excitation) per single A -> A', in blocks of 32 singles. Each lane
-    // keeps its beta list entry for the row; the warp sweeps the segments.
+    int32_t pos = 0, dropped = 0;  // dropped: this lane's count
     uint2 el = make_uint2(0u, 0u);  // this lane's entry of the beta L2 list
     if(lane < n2l)
       el = s2 ? sl2[lane]
-              : make_uint2(uint32_t(ld_nc(d.l2col + l2b + lane)),
-                           ld_nc(d.l2info + l2b + lane));
-    const int64_t s0 = d.asoff[A];
-    const int32_t nsg = int32_t(d.asoff[A + 1] - s0);
-    for(int32_t sb = 0; sb < nsg; sb += 32) {
-      const int k2 = min(32, nsg - sb);
-      __syncwarp();  // the previous block's segments are no longer read
-      if(lane < k2) {
-        const int4 g = ld_nc(d.aseg + s0 + sb + lane);
-        const int32_t p = int32_t(uint32_t(g.z) >> 31) * n4l +
-                          (sb + lane) * n2l + (g.z & 0x7FFFFFFF);
-        seg_d[wid][lane] = make_int4(p, g.x, g.y, int(uint32_t(g.w) & 0x80000000u));
-        seg_single[wid][lane] = sgnd(uint32_t(g.w), F[g.w & 0x3FFF]);
+              : make_uint2(uint32_t(__ldg(d.l2col + l2b + lane)),
+                           __ldg(d.l2info + l2b + lane));
+    using CS = typename std::conditional<sizeof(CI) == 4, int, long long>::type;
+    CS* __restrict__ rcs = reinterpret_cast<CS*>(rc);
+    // entries whose column differs from the row (every phase but the
+    // same-alpha segment): no diagonal test
+    auto put = [&](bool act, int32_t p, int32_t col, double h) {
+      if(act) {
+        const bool keep = fabs(h) > thresh;
+        dropped += !keep;
+        __stcs(rcs + p, CS(keep ? col : -1));
+        __stcs(rv + p, store_val<VT>(h, false));
+      }
+    };
+    auto put_d = [&](bool act, int32_t p, int32_t col, double h) {
+      if(act) {
+        const bool keep = fabs(h) > thresh;
+        dropped += !keep;
+        const bool isd = keep && col == row;
+        __stcs(rcs + p, CS(keep ? col : -1));
+        __stcs(rv + p, store_val<VT>(h, isd));
+        if(isd) diag[row] = h;
+      }
+    };
+    const int64_t c1 = d.aoff[A + 1];
+    // the next chunk of the alpha list is loaded while this one is emitted
+    int32_t nx_col = 0;
+    uint32_t nx_ai = 0;
+    double nx_val = 0.0;
+    {
+      const int64_t j = d.aoff[A] + lane;
+      if(j < c1) {
+        nx_col = __ldg(d.acol + j);
+        nx_ai = __ldg(d.ainfo + j);
+        nx_val = __ldg(d.aval + j);
+      }
+    }
+    for(int64_t c = d.aoff[A]; c < c1; c += 32) {
+      const int64_t j = c + lane;
+      int32_t colA = 0;
+      uint32_t ai = 0;
+      double aval = 0.0;
+      int cls = 3, cnt = 0;
+      if(j < c1) {
+        colA = nx_col * UB;
+        ai = nx_ai;
+        aval = nx_val;
+        cls = int((ai >> 29) & 3u);
+        cnt = cls == 0 ? n4l : cls == 1 ? n2l : 1;
+      }
+      if(j + 32 < c1) {
+        nx_col = __ldg(d.acol + j + 32);
+        nx_ai = __ldg(d.ainfo + j + 32);
+        nx_val = __ldg(d.aval + j + 32);
+      }
+      const int incl = warp_incl_scan(cnt);
+      const int32_t spos = pos + incl - cnt;
+      pos += __shfl_sync(0xffffffffu, incl, 31);
+      // (1) alpha doubles: beta unchanged, one entry each
+      {
+        put(cls == 2, spos, colA + B, aval);
+      }
+      // (2) the same-alpha segment: every beta string within two excitations
+      unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
+      while(m0) {
+        const int L0 = __ffs(m0) - 1;
+        m0 &= m0 - 1;
+        const int32_t sp0 = __shfl_sync(0xffffffffu, spos, L0);
+        const int32_t cA = __shfl_sync(0xffffffffu, colA, L0);
+        for(int32_t t = lane; t - lane < n4l; t += 32) {
+          const bool act = t < n4l;
+          double h = 0;
+          int32_t col = 0;
+          if(act) {
+            const uint2 ent = s4 ? sl4[t]
+                                 : make_uint2(uint32_t(__ldg(d.l4col + l4b + t)),
+                                              __ldg(d.l4info + l4b + t));
+            const uint32_t cb = (ent.y >> 29) & 3u, off = ent.y & 0x0FFFFFFFu;
+            // singles from this row's table (shared; offsets < 2 n^2),
+            // doubles already signed
+            const double vf = F[off < uint32_t(2 * n2) ? off : 0u];
+            const double vd = s4 ? sl4v[t] : __ldg(d.l4val + l4b + t);
+            col = cA + int32_t(ent.x);
+            h = cb == 0 ? hd : cb == 1 ? sgnd(ent.y, vf) : vd;
+          }
+          put_d(act, sp0 + t, col, h);
+        }
+      }
+      // (3) alpha singles: one segment of n2l entries (beta within one
+      // excitation) per connected alpha string. Each lane keeps its beta
+      // list entry for the row; the warp sweeps the segments.
+      const unsigned m2 = __ballot_sync(0xffffffffu, cls == 1);
+      if(cls == 1) {
+        const int rk = __popc(m2 & lanemask_lt());
+        const uint32_t pa_ = ai & 0x3FFFu;  // v1 + o1 n
+        seg_d[wid][rk] = make_int4(spos, colA, int(pa_ * uint32_t(n2)),
+                                   int(ai & 0x80000000u));
+        seg_single[wid][rk] = sgnd(ai, F[(ai >> 14) & 0x3FFFu]);
       }
       __syncwarp();
+      const int k2 = __popc(m2);
       if(lane < n2l) {
         // branch-free body: the same-beta entry (offset 0) also loads from
         // its VT row and then selects the alpha-single value
@@ -690,7 +653,7 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
         for(int q = 0; q < k2; ++q) {
           const int4 sd = seg_d[wid][q];
           const double sgl = seg_single[wid][q];
-          const double v = ld_nc(gVT + uint32_t(sd.z + int(boff)));
+          const double v = __ldg(gVT + uint32_t(sd.z + int(boff)));
           // sign of the element: one XOR on the high word
           const double hv = __hiloint2double(
               __double2hiint(v) ^ (sd.w ^ int(bsg)), __double2loint(v));
@@ -698,8 +661,8 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
           const bool keep = fabs(h) > thresh;
           dropped += keep ? 0 : 1;
           const uint32_t p = uint32_t(sd.x);
-          st_cs(rcl + p, CS(keep ? sd.y + elx : -1));
-          st_cs(rvl + p, store_val<VT>(h, false));
+          __stcs(rcl + p, CS(keep ? sd.y + elx : -1));
+          __stcs(rvl + p, store_val<VT>(h, false));
         }
       }
       if(n2l > 32) {  // list entries 32.. of every segment, flattened
@@ -712,11 +675,11 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
           if((sg + 1) * w2 <= e) ++sg;
           const int32_t t = 32 + e - sg * w2;
           const uint2 ent = s2 ? sl2[t]
-                               : make_uint2(uint32_t(ld_nc(d.l2col + l2b + t)),
-                                            ld_nc(d.l2info + l2b + t));
+                               : make_uint2(uint32_t(__ldg(d.l2col + l2b + t)),
+                                            __ldg(d.l2info + l2b + t));
           const int4 sd = seg_d[wid][sg];
           const double sgl = seg_single[wid][sg];
-          const double v = ld_nc(gVT + uint32_t(sd.z + int(ent.y & 0x0FFFFFFFu)));
+          const double v = __ldg(gVT + uint32_t(sd.z + int(ent.y & 0x0FFFFFFFu)));
           const double hv = __hiloint2double(
               __double2hiint(v) ^ (sd.w ^ int(ent.y & 0x80000000u)),
               __double2loint(v));
@@ -724,15 +687,16 @@ __global__ void __launch_bounds__(DP_THREADS, 4)
           const bool keep = fabs(h) > thresh;
           dropped += keep ? 0 : 1;
           const uint32_t p = uint32_t(sd.x + t);
-          st_cs(rcs + p, CS(keep ? sd.y + int32_t(ent.x) : -1));
-          st_cs(rv + p, store_val<VT>(h, false));
+          __stcs(rcs + p, CS(keep ? sd.y + int32_t(ent.x) : -1));
+          __stcs(rv + p, store_val<VT>(h, false));
         }
       }
+      __syncwarp();
     }
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1)
       dropped += __shfl_xor_sync(0xffffffffu, dropped, o);
-    if(lane == 0) rowcnt[row] = int64_t(rowlen) - dropped;
+    if(lane == 0) rowcnt[row] = int64_t(pos) - dropped;
   }
 }
 
@@ -1362,38 +1326,20 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     double *pga, *pgb;
     pg_table(ua, UA, pgaoff, pga);
     pg_table(ub, UB, pgboff, pgb);
-    // per alpha string: singles (segment data), doubles (positions and
-    // values) and the position of A itself; signed values of beta doubles
-    int64_t *asoff, *adoff;
-    int4 *aseg, *adbl;
-    int2* asame;
-    double* l4val;
+    // signed values of the alpha doubles and of the beta L4 doubles
+    double *aval, *l4val;
     {
-      int64_t* cs = A.get<int64_t>(UA + 1);
-      int64_t* cd = A.get<int64_t>(UA + 1);
-      asoff = A.get<int64_t>(UA + 1);
-      adoff = A.get<int64_t>(UA + 1);
-      dp_split_counts_k<<<grid_for(UA, 256, 4 * sms), 256, 0, s>>>(
-          na, int64_t(UA), cs, cd), note_launch();
-      exclusive_scan<int64_t, int64_t>(cs, asoff, UA, asoff + UA, A);
-      exclusive_scan<int64_t, int64_t>(cd, adoff, UA, adoff + UA, A);
-      const int64_t nst = to_host(asoff + UA, s), ndt = to_host(adoff + UA, s);
-      aseg = A.get<int4>(size_t(std::max<int64_t>(nst, 1)));
-      adbl = A.get<int4>(size_t(std::max<int64_t>(ndt, 1)));
-      asame = A.get<int2>(UA);
-      MB_CUDA(cudaMemsetAsync(asame, 0xFF, UA * sizeof(int2), s));  // -1: none
-      dp_atab_k<<<grid_for(UA * 32, 256, 8 * sms), 256, 0, s>>>(
-          aoff, acol, ainfo, int64_t(UA), int32_t(UB), h->norb, I.G, asoff,
-          adoff, aseg, adbl, asame), note_launch();
-      const int64_t n4t = to_host(l4off + UB, s);
-      l4val = A.get<double>(size_t(std::max<int64_t>(n4t, 1)));
-      dp_l4val_k<<<grid_for(size_t(n4t), 256, 8 * sms), 256, 0, s>>>(
-          l4info, n4t, I.G, l4val), note_launch();
+      const int64_t na_ = to_host(aoff + UA, s), n4_ = to_host(l4off + UB, s);
+      aval = A.get<double>(size_t(std::max<int64_t>(na_, 1)));
+      l4val = A.get<double>(size_t(std::max<int64_t>(n4_, 1)));
+      dp_dval_k<<<grid_for(size_t(na_), 256, 8 * sms), 256, 0, s>>>(
+          ainfo, na_, I.G, aval), note_launch();
+      dp_dval_k<<<grid_for(size_t(n4_), 256, 8 * sms), 256, 0, s>>>(
+          l4info, n4_, I.G, l4val), note_launch();
     }
     DPData d{int64_t(UA), int64_t(UB), ua, ub, aoff, acol, ainfo,
              l2off, l2col, l2info, l4off, l4col, l4info,
-             pgaoff, pga, pgboff, pgb,
-             asoff, aseg, adoff, adbl, asame, l4val};
+             pgaoff, pga, pgboff, pgb, aval, l4val};
     // shared-memory plan: integrals for the singles if they fit, the longest
     // beta lists, per-warp singles tables
     int64_t l2max = 0, l4max = 0;
@@ -1423,17 +1369,27 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     MB_CUDA(cudaFuncSetAttribute(dp_fill_k<NBITS, CI, VT>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(Ls.bytes)));
-    // shared-memory carveout: just enough for four CTAs, the rest is L1
-    {
-      const size_t per_cta = Ls.bytes + 5 * 1024 + 1024;  // + static + reserve
-      const int pct = int(std::min<size_t>(100, (4 * per_cta * 100) / (228 * 1024) + 1));
-      MB_CUDA(cudaFuncSetAttribute(dp_fill_k<NBITS, CI, VT>,
-                                   cudaFuncAttributePreferredSharedMemoryCarveout,
-                                   pct));
-    }
+    // shared-memory carveout: the smallest that keeps DP_CTAS CTAs resident
+    // (dynamic + static shared memory + the 1 KB the SM reserves per CTA),
+    // the rest is L1. The carveout is a preference that the driver maps to
+    // one of a few sizes, so it is raised until the occupancy query agrees.
     int per_sm = 0;
-    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, dp_fill_k<NBITS, CI, VT>, DP_THREADS, Ls.bytes));
+    {
+      cudaFuncAttributes fa;
+      MB_CUDA(cudaFuncGetAttributes(&fa, dp_fill_k<NBITS, CI, VT>));
+      const size_t per_cta = Ls.bytes + fa.sharedSizeBytes + 1024;
+      int pct = int(std::min<size_t>(
+          100, (DP_CTAS * per_cta * 100 + 228 * 1024 - 1) / (228 * 1024)));
+      for(;;) {
+        MB_CUDA(cudaFuncSetAttribute(
+            dp_fill_k<NBITS, CI, VT>,
+            cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, dp_fill_k<NBITS, CI, VT>, DP_THREADS, Ls.bytes));
+        if(per_sm >= DP_CTAS || pct >= 100) break;
+        pct = std::min(100, pct + 5);
+      }
+    }
     const unsigned g = unsigned(std::max(1, per_sm) * sms);
     if(!h->VT) {
       const size_t n4 = size_t(nn) * nn * nn * nn;
