@@ -876,14 +876,106 @@ struct GenData {
   const uint64_t* kalpha;   // ket group alpha
   const uint64_t* sbeta;    // sorted ket betas
   const uint32_t* sidx;     // sorted ket -> original index
+  // beta hash tables of the large ket groups (gen_hsize_k / gen_hinsert_k)
+  const int64_t* hoff;      // ket group -> table range (empty: no table)
+  const int32_t* htab;      // sorted position - group start, -1 empty
+  const int32_t* gbpop;     // ket group -> common beta popcount (-1: none)
+  int n;                    // orbitals
 };
+
+// Ket groups of at least GEN_HASH_MIN members get a hash table of their
+// betas so that a bra row connected to them by an alpha single excitation
+// can look up its own beta single excitations instead of testing every
+// member (a few hundred lookups against up to ~1e5 member tests for the
+// large groups of ASCI spaces).
+constexpr int64_t GEN_HASH_MIN = 256;
+
+template <int NSW>
+__device__ __forceinline__ uint64_t spin_hash(const Spin<NSW>& a) {
+  uint64_t x = 0;
+#pragma unroll
+  for(int w = 0; w < NSW; ++w) x = (x ^ a.w[w]) * 0x9E3779B97F4A7C15ull;
+  x ^= x >> 29;
+  x *= 0xBF58476D1CE4E5B9ull;
+  return x ^ (x >> 32);
+}
+
+// Per ket group (one warp each): the table size (a power of two >= 2 G for
+// groups of G >= GEN_HASH_MIN members whose betas share one popcount, else
+// 0) and that popcount (-1 when the group has no table).
+template <int NSW>
+__global__ void gen_hsize_k(const int64_t* goff, uint32_t ng,
+                            const uint64_t* sbeta, int64_t* hsz,
+                            int32_t* gbpop) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for(int64_t gi = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      gi < int64_t(ng); gi += nw) {
+    const int64_t m0 = goff[gi], m1 = goff[gi + 1];
+    int64_t sz = 0;
+    int pc = -1;
+    if(m1 - m0 >= GEN_HASH_MIN) {
+      pc = sp_popc(ld_spin<NSW>(sbeta, m0));
+      bool same = true;
+      for(int64_t m = m0 + lane; m < m1; m += 32)
+        same = same && sp_popc(ld_spin<NSW>(sbeta, m)) == pc;
+      same = __all_sync(0xffffffffu, same);
+      if(same) {
+        sz = 1;
+        while(sz < 2 * (m1 - m0)) sz <<= 1;
+      } else {
+        pc = -1;
+      }
+    }
+    if(lane == 0) {
+      hsz[gi] = sz;
+      gbpop[gi] = pc;
+    }
+  }
+}
+
+// Inserts the first sorted position of every distinct beta of a ket group
+// into its table (linear probing; the table has at least twice as many
+// slots as entries, so every insertion finds a free slot).
+template <int NSW>
+__global__ void gen_hinsert_k(const int64_t* goff, uint32_t ng,
+                              const uint64_t* sbeta, const int64_t* hoff,
+                              int32_t* htab) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for(int64_t gi = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      gi < int64_t(ng); gi += nw) {
+    const int64_t h0 = hoff[gi], hs = hoff[gi + 1] - h0;
+    if(hs == 0) continue;
+    const uint64_t mask = uint64_t(hs) - 1;
+    const int64_t m0 = goff[gi], m1 = goff[gi + 1];
+    for(int64_t m = m0 + lane; m < m1; m += 32) {
+      const Spin<NSW> b = ld_spin<NSW>(sbeta, m);
+      if(m > m0 && ld_spin<NSW>(sbeta, m - 1) == b) continue;  // duplicate
+      uint64_t slot = spin_hash<NSW>(b) & mask;
+      for(int64_t t = 0; t < hs; ++t) {
+        if(atomicCAS(htab + h0 + slot, -1, int32_t(m - m0)) == -1) break;
+        slot = (slot + 1) & mask;
+      }
+    }
+  }
+}
 
 // Enumerates the candidate kets of one bra row warp-synchronously; calls
 // emit(active, sorted_pos, ket_group, pa, pb) for chunks of <= 32.
 template <int NSW, class F>
 __device__ __forceinline__ void gen_enumerate(const GenData& g, int32_t rg,
-                                              Spin<NSW> bb, F&& emit) {
+                                              Spin<NSW> bb, uint8_t* ov,
+                                              F&& emit) {
   const int lane = threadIdx.x & 31;
+  // occupied / empty orbitals of the bra beta (ov[0..128), ov[128..256)),
+  // for the hash lookups of its single excitations
+  const int nob = sp_popc(bb), nvb = g.n - nob;
+  const int nenum = 1 + nob * nvb;  // the beta itself and its singles
+  const float rnv = 1.0f / float(nvb > 0 ? nvb : 1);
+  __syncwarp();
+  spin_lists<NSW>(bb, g.n, lane, ov, ov + 128);
+  __syncwarp();
   const int64_t c1 = g.aoff[rg + 1];
   for(int64_t c = g.aoff[rg]; c < c1; c += 32) {
     const int64_t j = c + lane;
@@ -931,6 +1023,46 @@ __device__ __forceinline__ void gen_enumerate(const GenData& g, int32_t rg,
       const int ppa = __shfl_sync(0xffffffffu, pa, L);
       const int limit = 4 - ppa;
       const int64_t m0 = g.goff[gg], m1 = g.goff[gg + 1];
+      const int64_t h0 = g.hoff[gg], hs = g.hoff[gg + 1] - h0;
+      if(ppa == 2 && hs > 0 && g.gbpop[gg] == nob &&
+         m1 - m0 > 8 * int64_t(nenum)) {
+        // alpha single into a large group: only betas within one
+        // excitation of bb connect, and all of them have bb's popcount
+        const uint64_t mask = uint64_t(hs) - 1;
+        for(int u0 = 0; u0 < nenum; u0 += 32) {
+          const int u = u0 + lane;
+          int64_t lo = 0, hi = 0;
+          int pbv = 0;
+          if(u < nenum) {
+            Spin<NSW> q = bb;
+            if(u > 0) {
+              const int i = int((float(u - 1) + 0.5f) * rnv);
+              const int j = (u - 1) - i * nvb;
+              q = sp_flip(sp_flip(q, ov[i]), ov[128 + j]);
+              pbv = 2;
+            }
+            uint64_t slot = spin_hash<NSW>(q) & mask;
+            for(int64_t t = 0; t < hs; ++t) {
+              const int32_t r = g.htab[h0 + slot];
+              if(r < 0) break;
+              if(ld_spin<NSW>(g.sbeta, m0 + r) == q) {
+                lo = m0 + r;
+                hi = lo + 1;
+                while(hi < m1 && ld_spin<NSW>(g.sbeta, hi) == q) ++hi;
+                break;
+              }
+              slot = (slot + 1) & mask;
+            }
+          }
+          const int rem = int(hi - lo);
+          int mr = rem;
+#pragma unroll
+          for(int o = 16; o; o >>= 1)
+            mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+          for(int r = 0; r < mr; ++r) emit(r < rem, lo + r, gg, 2, pbv);
+        }
+        continue;
+      }
       for(int64_t base = m0; base < m1; base += 32) {
         const int64_t m = base + lane;
         bool act = m < m1;
@@ -947,6 +1079,7 @@ template <int NBITS>
 __global__ void __launch_bounds__(HB_THREADS)
     gen_count_k(GenData g, const uint64_t* bra, size_t nbra, int64_t* cnt) {
   using D = DetTraits<NBITS>;
+  __shared__ uint8_t s_ov[HB_WARPS][256];
   const int64_t nwarp = int64_t(gridDim.x) * HB_WARPS;
   for(int64_t row = int64_t(blockIdx.x) * HB_WARPS + (threadIdx.x >> 5);
       row < int64_t(nbra); row += nwarp) {
@@ -954,8 +1087,8 @@ __global__ void __launch_bounds__(HB_THREADS)
     int64_t c = 0;
     if(rg >= 0) {
       const auto bb = D::beta(bra + row * D::NW);
-      gen_enumerate<D::NSW>(g, rg, bb, [&](bool act, int64_t, int32_t, int,
-                                            int) {
+      gen_enumerate<D::NSW>(g, rg, bb, s_ov[threadIdx.x >> 5],
+                            [&](bool act, int64_t, int32_t, int, int) {
         c += __popc(__ballot_sync(0xffffffffu, act));
       });
     }
@@ -981,6 +1114,9 @@ __global__ void __launch_bounds__(HB_THREADS)
   constexpr int NSW = D::NSW;
   __shared__ uint32_t s_col[HB_WARPS][GEN_CAP];
   __shared__ double s_val[HB_WARPS][GEN_CAP];
+  // orbital lists of the bra beta, 256 bytes per warp: dynamic, since the
+  // candidate buffers take the whole static allowance
+  extern __shared__ __align__(16) uint8_t gen_ov[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t* bc = s_col[wid];
   double* bv = s_val[wid];
@@ -1002,8 +1138,8 @@ __global__ void __launch_bounds__(HB_THREADS)
     const Spin<NSW> ba = D::alpha(bd), bb = D::beta(bd);
     const double hd = hdiag[row];
     int64_t c = 0;
-    gen_enumerate<NSW>(g, rg, bb, [&](bool act, int64_t m, int32_t kg, int pa,
-                                      int pb) {
+    gen_enumerate<NSW>(g, rg, bb, gen_ov + wid * 256, [&](bool act, int64_t m,
+                                                 int32_t kg, int pa, int pb) {
       double h = 0;
       uint32_t col = 0;
       if(act) {
@@ -1460,7 +1596,24 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     uint8_t* apa = A.get<uint8_t>(natot + 1);
     gen_aconn_k<NSW><<<ga, 256, 0, s>>>(balpha, nbg, kalpha, nkg, aoff, acnt,
                                         acol, apa), note_launch();
-    GenData gd{rowgroup, aoff, acol, apa, kgoff, kalpha, ksbeta, kidx};
+    // beta hash tables of the large ket groups
+    int64_t* hoff = A.get<int64_t>(nkg + 1);
+    int32_t* gbpop = A.get<int32_t>(nkg + 1);
+    int32_t* htab;
+    {
+      int64_t* hsz = A.get<int64_t>(nkg + 1);
+      const unsigned gh = grid_for(size_t(nkg) * 32, 256, 16 * sms);
+      gen_hsize_k<NSW><<<gh, 256, 0, s>>>(kgoff, nkg, ksbeta, hsz, gbpop), note_launch();
+      exclusive_scan<int64_t, int64_t>(hsz, hoff, nkg, hoff + nkg, A);
+      A.release(hsz);
+      const int64_t htot = to_host(hoff + nkg, s);
+      htab = A.get<int32_t>(size_t(std::max<int64_t>(htot, 1)));
+      MB_CUDA(cudaMemsetAsync(htab, 0xFF, size_t(std::max<int64_t>(htot, 1)) * 4, s));
+      if(htot > 0)
+        gen_hinsert_k<NSW><<<gh, 256, 0, s>>>(kgoff, nkg, ksbeta, hoff, htab), note_launch();
+    }
+    GenData gd{rowgroup, aoff, acol, apa, kgoff, kalpha, ksbeta, kidx,
+               hoff, htab, gbpop, h->norb};
     const unsigned gr = grid_for(nbra, HB_WARPS, size_t(sms) * 16);
     gen_count_k<NBITS><<<gr, HB_THREADS, 0, s>>>(gd, bra, nbra, rowcnt), note_launch();
     exclusive_scan<int64_t, int64_t>(rowcnt, rowptr64, nbra, rowptr64 + nbra, A);
@@ -1503,7 +1656,10 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     // what is free; short rows of the chunk are written by the same launch.
     int64_t lchunk = int64_t(0.7 * double(device_bytes_available()) / 32.0);
     lchunk = std::max<int64_t>(lchunk, int64_t(1) << 20);
-    constexpr int gen_dyn = 0;
+    constexpr int gen_dyn = HB_WARPS * 256;
+    MB_CUDA(cudaFuncSetAttribute(gen_fill_k<NBITS, CI, VT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 gen_dyn));
     float fill_ms_tot = 0.f;
     int64_t la = 0;  // next long row (list index)
     int64_t row_a = 0;

@@ -193,3 +193,34 @@ def test_matrix_element_batch(ref):
     got = H.matrix_element(dets[i], dets[j])
     exp = ref.matrix_element(ref.ham(128, 8, T, V), dets[i], dets[j])
     assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("nbits", [64, 128])
+def test_general_path_large_groups(ref, nbits):
+    """Rows whose alpha string is a single excitation of a large alpha group
+    (here the HF alpha with all 462 betas) look their beta singles up in the
+    group's hash table instead of testing every member; parity with the
+    reference, with a duplicated determinant inside the large group."""
+    from macis_b200.integrals import synthetic_integrals
+    rng = np.random.default_rng(3)
+    n, k = 11, 5
+    T, V = synthetic_integrals(n, 2)
+    betas = [sum(1 << i for i in c) for c in
+             __import__("itertools").combinations(range(n), k)]
+    hf = (1 << k) - 1
+    a_list, b_list = [hf] * len(betas), list(betas)
+    for i in range(k):
+        for x in range(k, n):
+            a = hf ^ (1 << i) ^ (1 << x)
+            for b in rng.choice(betas, 20, replace=False):
+                a_list.append(a)
+                b_list.append(int(b))
+    dets = mb.sd.make_dets(a_list, b_list, nbits)
+    dets = np.concatenate([dets, dets[7:8]])          # duplicate in the group
+    dets = shuffled(dets, seed=5)
+    H = mb.HamiltonianGenerator(T, V, nbits)
+    A = mb.make_csr_hamiltonian(dets, H, np.finfo(float).eps)
+    assert A.build_stats()["direct_product"] == 0
+    assert_csr_equal(A.to_host(), ref.build_csr(ref.ham(nbits, n, T, V), dets,
+                                                dets, np.finfo(float).eps,
+                                                nthreads=8))
