@@ -837,33 +837,146 @@ __global__ void gen_group_end_k(int64_t* goff, uint32_t ng, int64_t end) {
   goff[ng] = end;
 }
 
+// ---- beta-major view of the kets: a row's alpha-double connections are the
+// kets with its own beta whose alpha is 4 bits away, found by walking the
+// kets of that beta when there are fewer of them than alpha-double groups.
+
+// Sort keys with the beta string most significant.
+template <int NBITS>
+__global__ void gen_bkeys_k(const uint64_t* dets, size_t n, uint64_t* keys,
+                            uint32_t* idx) {
+  using D = DetTraits<NBITS>;
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const uint64_t* d = dets + i * D::NW;
+    const auto a = D::alpha(d), b = D::beta(d);
+    if constexpr(NBITS == 64) {
+      keys[i] = (b.w[0] << 32) | a.w[0];
+    } else if constexpr(NBITS == 128) {
+      keys[2 * i] = a.w[0];
+      keys[2 * i + 1] = b.w[0];
+    } else {
+      keys[4 * i] = a.w[0];
+      keys[4 * i + 1] = a.w[1];
+      keys[4 * i + 2] = b.w[0];
+      keys[4 * i + 3] = b.w[1];
+    }
+    idx[i] = uint32_t(i);
+  }
+}
+
+template <int NBITS>
+__device__ __forceinline__ void bkey_spins(const uint64_t* keys, size_t i,
+                                           Spin<DetTraits<NBITS>::NSW>& a,
+                                           Spin<DetTraits<NBITS>::NSW>& b) {
+  if constexpr(NBITS == 64) {
+    b.w[0] = keys[i] >> 32;
+    a.w[0] = keys[i] & 0xffffffffull;
+  } else if constexpr(NBITS == 128) {
+    a.w[0] = keys[2 * i];
+    b.w[0] = keys[2 * i + 1];
+  } else {
+    a.w[0] = keys[4 * i];
+    a.w[1] = keys[4 * i + 1];
+    b.w[0] = keys[4 * i + 2];
+    b.w[1] = keys[4 * i + 3];
+  }
+}
+
+// amaj[idx[m]] = m: original ket index -> alpha-major sorted position.
+__global__ void gen_invert_k(const uint32_t* idx, size_t n, uint32_t* amaj) {
+  for(size_t m = size_t(blockIdx.x) * blockDim.x + threadIdx.x; m < n;
+      m += size_t(gridDim.x) * blockDim.x)
+    amaj[idx[m]] = uint32_t(m);
+}
+
+// mgroup[m] = alpha group of sorted position m (-1 stays for zero dets).
+__global__ void gen_mgroup_k(const int64_t* goff, uint32_t ng,
+                             int32_t* mgroup) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for(int64_t gi = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      gi < int64_t(ng); gi += nw)
+    for(int64_t m = goff[gi] + lane; m < goff[gi + 1]; m += 32)
+      mgroup[m] = int32_t(gi);
+}
+
+// Per beta-major position: its alpha string and alpha-major position; flags
+// at the first position of every distinct beta.
+template <int NBITS>
+__global__ void gen_bmajor_k(const uint64_t* bkeys, const uint32_t* bidx,
+                             size_t n, const uint32_t* amaj, uint64_t* bm_alpha,
+                             uint32_t* bm_m, uint32_t* bflags) {
+  constexpr int NSW = DetTraits<NBITS>::NSW;
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    Spin<NSW> a, b;
+    bkey_spins<NBITS>(bkeys, i, a, b);
+    st_spin<NSW>(bm_alpha, i, a);
+    bm_m[i] = amaj[bidx[i]];
+    uint32_t f = 1;
+    if(i > 0) {
+      Spin<NSW> pa, pb;
+      bkey_spins<NBITS>(bkeys, i - 1, pa, pb);
+      f = (pb == b) ? 0u : 1u;
+    }
+    bflags[i] = f;
+  }
+}
+
+// Distinct betas (sorted) and the start of each in beta-major order.
+template <int NBITS>
+__global__ void gen_bgroups_k(const uint64_t* bkeys, const uint32_t* bflags,
+                              const uint32_t* bgx, size_t n, int64_t* bgoff,
+                              uint64_t* bgbeta) {
+  constexpr int NSW = DetTraits<NBITS>::NSW;
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    if(!bflags[i]) continue;
+    Spin<NSW> a, b;
+    bkey_spins<NBITS>(bkeys, i, a, b);
+    bgoff[bgx[i]] = int64_t(i);
+    st_spin<NSW>(bgbeta, bgx[i], b);
+  }
+}
+
 // Alpha connectivity between bra groups and ket groups: (ket group, pa).
+// Count pass (col == nullptr): cnt[l] = all connected groups, cnt4[l] =
+// those at pa == 4. Fill pass: the pa <= 3 entries of bra group l first, in
+// ket-group order, then its pa == 4 entries from off[l] + cnt[l] - cnt4[l].
 template <int NSW>
 __global__ void gen_aconn_k(const uint64_t* balpha, size_t nb,
                             const uint64_t* kalpha, size_t nk,
-                            const int64_t* off, int64_t* cnt, int32_t* col,
-                            uint8_t* pa_out) {
+                            const int64_t* off, int64_t* cnt, int64_t* cnt4,
+                            int32_t* col, uint8_t* pa_out) {
   const int lane = threadIdx.x & 31;
   const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
   for(size_t l = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
       l < nb; l += nwarp) {
     const Spin<NSW> L = ld_spin<NSW>(balpha, l);
-    int64_t c = 0;
+    int64_t c = 0, c4 = 0;
     const int64_t base = off ? off[l] : 0;
+    const int64_t base4 = col ? base + cnt[l] - cnt4[l] : 0;
     for(size_t r0 = 0; r0 < nk; r0 += 32) {
       const size_t r = r0 + lane;
       int p = 99;
       if(r < nk) p = sp_popc(L ^ ld_spin<NSW>(kalpha, r));
-      const bool hit = p <= 4;
+      const bool hit = p <= 3, hit4 = p == 4;
       const unsigned m = __ballot_sync(0xffffffffu, hit);
-      if(col && hit) {
-        const int64_t pos = base + c + __popc(m & lanemask_lt());
+      const unsigned m4 = __ballot_sync(0xffffffffu, hit4);
+      if(col && (hit || hit4)) {
+        const int64_t pos = hit ? base + c + __popc(m & lanemask_lt())
+                                : base4 + c4 + __popc(m4 & lanemask_lt());
         col[pos] = int32_t(r);
         pa_out[pos] = uint8_t(p);
       }
       c += __popc(m);
+      c4 += __popc(m4);
     }
-    if(!col && lane == 0) cnt[l] = c;
+    if(!col && lane == 0) {
+      cnt[l] = c + c4;
+      cnt4[l] = c4;
+    }
   }
 }
 
@@ -881,6 +994,14 @@ struct GenData {
   const int32_t* htab;      // sorted position - group start, -1 empty
   const int32_t* gbpop;     // ket group -> common beta popcount (-1: none)
   int n;                    // orbitals
+  const int64_t* a4cnt;     // bra group -> its pa == 4 entries (at the end)
+  // beta-major view of the kets (gen_bmajor_k / gen_bgroups_k)
+  const uint64_t* bgbeta;   // distinct ket betas, sorted
+  const int64_t* bgoff;     // their ranges in beta-major order
+  int64_t nbgb;             // number of distinct ket betas
+  const uint64_t* bm_alpha; // per beta-major position: alpha string
+  const uint32_t* bm_m;     // per beta-major position: alpha-major position
+  const int32_t* mgroup;    // alpha-major position -> ket group (-1: none)
 };
 
 // Ket groups of at least GEN_HASH_MIN members get a hash table of their
@@ -965,8 +1086,8 @@ __global__ void gen_hinsert_k(const int64_t* goff, uint32_t ng,
 // emit(active, sorted_pos, ket_group, pa, pb) for chunks of <= 32.
 template <int NSW, class F>
 __device__ __forceinline__ void gen_enumerate(const GenData& g, int32_t rg,
-                                              Spin<NSW> bb, uint8_t* ov,
-                                              F&& emit) {
+                                              Spin<NSW> ba, Spin<NSW> bb,
+                                              uint8_t* ov, F&& emit) {
   const int lane = threadIdx.x & 31;
   // occupied / empty orbitals of the bra beta (ov[0..128), ov[128..256)),
   // for the hash lookups of its single excitations
@@ -976,10 +1097,45 @@ __device__ __forceinline__ void gen_enumerate(const GenData& g, int32_t rg,
   __syncwarp();
   spin_lists<NSW>(bb, g.n, lane, ov, ov + 128);
   __syncwarp();
+  // the kets with beta bb (beta-major range [b0, b1))
+  int64_t b0 = 0, b1 = 0;
+  {
+    int64_t lo = 0, hi = g.nbgb;
+    while(lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if(sp_cmp(ld_spin<NSW>(g.bgbeta, mid), bb) < 0)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if(lo < g.nbgb && ld_spin<NSW>(g.bgbeta, lo) == bb) {
+      b0 = g.bgoff[lo];
+      b1 = g.bgoff[lo + 1];
+    }
+  }
   const int64_t c1 = g.aoff[rg + 1];
-  for(int64_t c = g.aoff[rg]; c < c1; c += 32) {
+  const int64_t c4 = c1 - g.a4cnt[rg];  // the pa == 4 entries start here
+  // alpha doubles through the kets of beta bb when they are fewer than the
+  // alpha-double groups (each of which would take a binary search)
+  const bool by_beta = b1 - b0 < c1 - c4;
+  const int64_t cend = by_beta ? c4 : c1;
+  if(by_beta) {
+    for(int64_t p0 = b0; p0 < b1; p0 += 32) {
+      const int64_t p = p0 + lane;
+      bool act = false;
+      int64_t m = 0;
+      int32_t kg = 0;
+      if(p < b1) {
+        m = g.bm_m[p];
+        kg = g.mgroup[m];
+        act = kg >= 0 && sp_popc(ld_spin<NSW>(g.bm_alpha, p) ^ ba) == 4;
+      }
+      emit(act, m, kg, 4, 0);
+    }
+  }
+  for(int64_t c = g.aoff[rg]; c < cend; c += 32) {
     const int64_t j = c + lane;
-    const bool valid = j < c1;
+    const bool valid = j < cend;
     int32_t kg = 0;
     int pa = 99;
     if(valid) {
@@ -1086,8 +1242,9 @@ __global__ void __launch_bounds__(HB_THREADS)
     const int32_t rg = g.rowgroup[row];
     int64_t c = 0;
     if(rg >= 0) {
+      const auto ba = D::alpha(bra + row * D::NW);
       const auto bb = D::beta(bra + row * D::NW);
-      gen_enumerate<D::NSW>(g, rg, bb, s_ov[threadIdx.x >> 5],
+      gen_enumerate<D::NSW>(g, rg, ba, bb, s_ov[threadIdx.x >> 5],
                             [&](bool act, int64_t, int32_t, int, int) {
         c += __popc(__ballot_sync(0xffffffffu, act));
       });
@@ -1138,7 +1295,7 @@ __global__ void __launch_bounds__(HB_THREADS)
     const Spin<NSW> ba = D::alpha(bd), bb = D::beta(bd);
     const double hd = hdiag[row];
     int64_t c = 0;
-    gen_enumerate<NSW>(g, rg, bb, gen_ov + wid * 256, [&](bool act, int64_t m,
+    gen_enumerate<NSW>(g, rg, ba, bb, gen_ov + wid * 256, [&](bool act, int64_t m,
                                                  int32_t kg, int pa, int pb) {
       double h = 0;
       uint32_t col = 0;
@@ -1586,16 +1743,17 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     }
     // alpha connectivity bra groups -> ket groups
     int64_t* acnt = A.get<int64_t>(nbg + 1);
+    int64_t* acnt4 = A.get<int64_t>(nbg + 1);
     int64_t* aoff = A.get<int64_t>(nbg + 1);
     const unsigned ga = grid_for(size_t(nbg) * 32, 256, 16 * sms);
     gen_aconn_k<NSW><<<ga, 256, 0, s>>>(balpha, nbg, kalpha, nkg, nullptr,
-                                        acnt, nullptr, nullptr), note_launch();
+                                        acnt, acnt4, nullptr, nullptr), note_launch();
     exclusive_scan<int64_t, int64_t>(acnt, aoff, nbg, aoff + nbg, A);
     const int64_t natot = to_host(aoff + nbg, s);
     int32_t* acol = A.get<int32_t>(natot + 1);
     uint8_t* apa = A.get<uint8_t>(natot + 1);
     gen_aconn_k<NSW><<<ga, 256, 0, s>>>(balpha, nbg, kalpha, nkg, aoff, acnt,
-                                        acol, apa), note_launch();
+                                        acnt4, acol, apa), note_launch();
     // beta hash tables of the large ket groups
     int64_t* hoff = A.get<int64_t>(nkg + 1);
     int32_t* gbpop = A.get<int32_t>(nkg + 1);
@@ -1612,8 +1770,51 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       if(htot > 0)
         gen_hinsert_k<NSW><<<gh, 256, 0, s>>>(kgoff, nkg, ksbeta, hoff, htab), note_launch();
     }
+    // beta-major view of the kets
+    uint64_t *bm_alpha, *bgbeta;
+    uint32_t* bm_m;
+    int32_t* mgroup;
+    int64_t* bgoff;
+    int64_t nbgb = 0;
+    {
+      uint64_t* bkeys = A.get<uint64_t>(nket * KW);
+      uint32_t* bidx = A.get<uint32_t>(nket);
+      uint64_t* k2 = A.get<uint64_t>(nket * KW);
+      uint32_t* i2 = A.get<uint32_t>(nket);
+      gen_bkeys_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
+          ket, nket, bkeys, bidx), note_launch();
+      radix_sort<KW, uint32_t>(bkeys, bidx, k2, i2, nket, A);
+      A.release(k2);
+      A.release(i2);
+      uint32_t* amaj = A.get<uint32_t>(nket);
+      gen_invert_k<<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(kidx, nket,
+                                                               amaj), note_launch();
+      mgroup = A.get<int32_t>(nket);
+      MB_CUDA(cudaMemsetAsync(mgroup, 0xFF, nket * 4, s));
+      gen_mgroup_k<<<grid_for(size_t(nkg) * 32, 256, 16 * sms), 256, 0, s>>>(
+          kgoff, nkg, mgroup), note_launch();
+      bm_alpha = A.get<uint64_t>(nket * NSW);
+      bm_m = A.get<uint32_t>(nket);
+      uint32_t* bfl = A.get<uint32_t>(nket);
+      uint32_t* bgx = A.get<uint32_t>(nket + 1);
+      gen_bmajor_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
+          bkeys, bidx, nket, amaj, bm_alpha, bm_m, bfl), note_launch();
+      exclusive_scan<uint32_t, uint32_t>(bfl, bgx, nket, bgx + nket, A);
+      nbgb = int64_t(to_host(bgx + nket, s));
+      bgoff = A.get<int64_t>(size_t(nbgb) + 1);
+      bgbeta = A.get<uint64_t>((size_t(nbgb) + 1) * NSW);
+      gen_bgroups_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
+          bkeys, bfl, bgx, nket, bgoff, bgbeta), note_launch();
+      gen_group_end_k<<<1, 1, 0, s>>>(bgoff, uint32_t(nbgb), int64_t(nket)), note_launch();
+      A.release(bkeys);
+      A.release(bidx);
+      A.release(amaj);
+      A.release(bfl);
+      A.release(bgx);
+    }
     GenData gd{rowgroup, aoff, acol, apa, kgoff, kalpha, ksbeta, kidx,
-               hoff, htab, gbpop, h->norb};
+               hoff, htab, gbpop, h->norb, acnt4,
+               bgbeta, bgoff, nbgb, bm_alpha, bm_m, mgroup};
     const unsigned gr = grid_for(nbra, HB_WARPS, size_t(sms) * 16);
     gen_count_k<NBITS><<<gr, HB_THREADS, 0, s>>>(gd, bra, nbra, rowcnt), note_launch();
     exclusive_scan<int64_t, int64_t>(rowcnt, rowptr64, nbra, rowptr64 + nbra, A);
