@@ -446,8 +446,9 @@ def asci_extra(mb, ncore=10000, ndets_max=1000000, seed=0):
     """One exact FP64 asci_search on the n = 48 core set."""
     n, H, core, C, E0 = _n48_core(mb, ncore, seed)
     s = mb.ASCISettings()
-    # a warm-up search sizes the memory pool, as in a multi-iteration run
-    mb.asci_search(s, ndets_max, core[:ncore // 4], E0, C[:ncore // 4], n, H)
+    # a warm-up search of the same size grows the memory pool, as the
+    # previous iteration of a refine loop would
+    mb.asci_search(s, ndets_max, core, E0, C, n, H)
     t = time.perf_counter()
     out = mb.asci_search(s, ndets_max, core, E0, C, n, H)
     dt = time.perf_counter() - t

@@ -7,6 +7,7 @@
     python -m macis_b200.profile_cases spmv_c1     # FP64 SpMV on CAS(10e,10o)
     python -m macis_b200.profile_cases hbuild_sel  # selected (shuffled) space
     python -m macis_b200.profile_cases asci_n48    # one ASCI search, n = 48
+        # (--ncore core determinants, default 10000)
     python -m macis_b200.profile_cases mlp_fwd     # network forward, 2M rows
     python -m macis_b200.profile_cases mlp_train   # one training epoch
     python -m macis_b200.profile_cases screen_n48  # screened search, n = 48
@@ -181,6 +182,7 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--ntdets", type=float, default=1e6)
     ap.add_argument("--mode", default="fp64")
+    ap.add_argument("--ncore", type=int, default=10000)
     a = ap.parse_args()
     if a.case == "hbuild_c1":
         hbuild(10, 5, a.reps)
@@ -193,7 +195,7 @@ def main():
     elif a.case == "spmv_c1":
         spmv(10, 5, a.reps)
     elif a.case == "asci_n48":
-        asci_n48(a.reps)
+        asci_n48(a.reps, ncore=a.ncore)
     elif a.case == "mlp_fwd":
         mlp_fwd(a.reps)
     elif a.case == "mlp_train":
