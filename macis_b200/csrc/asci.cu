@@ -43,8 +43,21 @@ struct CoreData {
   double* eps;    // ncdets x 2 x n
   double* hd;     // ncdets
   int64_t* uoff;  // ncdets+1 unit offsets
+  int32_t* udet;  // per unit: the core det it belongs to
   const double* pairmax;  // 2 n^2 outer-pair integral bounds (screening)
 };
+
+// udet[u] = c for the units u of core det c (one warp per det): one load
+// per unit instead of a binary search over uoff.
+__global__ void unit_owner_fill_k(const int64_t* uoff, size_t ncdets,
+                                  int32_t* udet) {
+  const int lane = threadIdx.x & 31;
+  const size_t nw = size_t(gridDim.x) * (blockDim.x >> 5);
+  for(size_t c = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      c < ncdets; c += nw)
+    for(int64_t u = uoff[c] + lane; u < uoff[c + 1]; u += 32)
+      udet[u] = int32_t(c);
+}
 
 // Outer-pair integral bounds (macis_b200_ham::pairmax). G rows are
 // contiguous (warp per pair); V is read with one thread per pair so that a
@@ -430,15 +443,8 @@ __global__ void __launch_bounds__(256)
       if(MODE == 0 && (threadIdx.x & 31) == 0) counts[u - u0] = 0;
       continue;
     }
-    // det owning unit u: last c in [c0, c1) with uoff[c] <= u
-    size_t lo = c0, hi = c1;
-    while(hi - lo > 1) {
-      const size_t mid = (lo + hi) >> 1;
-      if(cd.uoff[mid] <= u)
-        lo = mid;
-      else
-        hi = mid;
-    }
+    // core det owning unit u (in [c0, c1))
+    const size_t lo = size_t(cd.udet[u]);
     const int64_t t = u - cd.uoff[lo];
     unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
                           MODE ? outoff[u - u0] : 0, keys, rv,
@@ -471,15 +477,7 @@ __host__ __device__ constexpr int unit_din() {
 }
 
 __device__ __forceinline__ size_t unit_owner(const CoreData& cd, int64_t u) {
-  size_t lo = 0, hi = cd.ncdets;
-  while(hi - lo > 1) {
-    const size_t mid = (lo + hi) >> 1;
-    if(cd.uoff[mid] <= u)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
+  return size_t(cd.udet[u]);
 }
 
 __device__ __forceinline__ uint32_t bf16_bits(float x) {
@@ -841,7 +839,14 @@ static int64_t core_setup(macis_b200_ham* h, Arena& A, const uint64_t* cdets,
     MB_CUDA(cudaGetLastError());
   }
   exclusive_scan<int64_t, int64_t>(units, cd.uoff, ncdets, cd.uoff + ncdets, A);
-  return ncdets ? to_host(cd.uoff + ncdets, s) : 0;
+  const int64_t U = ncdets ? to_host(cd.uoff + ncdets, s) : 0;
+  MB_REQUIRE(ncdets < (size_t(1) << 31), MACIS_B200_ECAPACITY,
+             "ASCI search needs < 2^31 core determinants");
+  cd.udet = A.get<int32_t>(size_t(U) + 1);
+  if(U > 0)
+    unit_owner_fill_k<<<grid_for(ncdets * 32, 256, 16 * sms), 256, 0, s>>>(
+        cd.uoff, ncdets, cd.udet), note_launch();
+  return U;
 }
 
 static void check_net(const macis_b200_mlp* net, cudaStream_t s) {
