@@ -231,6 +231,14 @@ __device__ __forceinline__ UnitDesc decode_unit(int nA, int nB, int nvA,
 }
 
 // One unit of contributions; MODE 0 counts, MODE 1 writes. Warp-synchronous.
+// q / d for 0 <= q < 2^14 and 1 <= d <= 128 from a float product with rd =
+// 1 / d: (q + 0.5) / d is at least 0.5 / d away from an integer, far above
+// the float rounding error (< 2^-22 q / d), so truncation gives the quotient
+// without a 64-bit integer division per contribution.
+__device__ __forceinline__ int small_div(int64_t q, float rd) {
+  return int((float(q) + 0.5f) * rd);
+}
+
 template <int NBITS, int MODE>
 __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                          double E0, double tol, int64_t* count_out,
@@ -299,7 +307,8 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const uint8_t* virS = S ? virB : virA;
         const int nO = S ? nA : nB;
         const uint8_t* occO = S ? occA : occB;
-        const int i = occS[q / nvS], a = virS[q % nvS];
+        const int qd = small_div(q, 1.0f / float(nvS));
+        const int i = occS[qd], a = virS[int(q) - qd * nvS];
         uint32_t cbin = 0;
         if(S == 0 && (chk || hist))
           cbin = alpha_bin<NSW>(sp_flip(sp_flip(sA, i), a));
@@ -335,7 +344,8 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const uint8_t* occS = S ? occB : occA;
         const uint8_t* virS = S ? virB : virA;
         const int span = nvS - 1 - aa;
-        const int jj = ii + 1 + int(q / span), bb = aa + 1 + int(q % span);
+        const int qd = small_div(q, 1.0f / float(span));
+        const int jj = ii + 1 + qd, bb = aa + 1 + (int(q) - qd * span);
         const int i = occS[ii], a = virS[aa], j = occS[jj], b = virS[bb];
         uint32_t cbin = 0;
         if(S == 0 && (chk || hist))
@@ -373,7 +383,8 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
       } else {
         // append_os_doubles_asci_contributions (determinant_contributions.hpp:122-160)
         const int i = occA[ii], a = virA[aa];
-        const int j = occB[q / nvB], b = virB[q % nvB];
+        const int qd = small_div(q, 1.0f / float(nvB));
+        const int j = occB[qd], b = virB[int(q) - qd * nvB];
         const bool inr =
             !chkb || beta_sub<NSW>(sp_flip(sp_flip(sB, j), b), nsub) == sub;
         const double Vv =
