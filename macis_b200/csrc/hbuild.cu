@@ -353,7 +353,7 @@ __device__ __forceinline__ float store_val<float>(double h, bool is_diag) {
 }
 
 // Direct-product fill. A CTA of DP_WARPS warps takes DP_WARPS rows that
-// share one beta string B (rows (A..A+7, B)); the beta lists L2(B), L4(B)
+// share one beta string B (rows (A..A+DP_WARPS-1, B)); the beta lists L2(B), L4(B)
 // and the signed values of L4's beta doubles are staged once in shared
 // memory.
 // Each warp first evaluates all Slater-Condon singles of its bra into a
@@ -362,10 +362,12 @@ __device__ __forceinline__ float store_val<float>(double h, bool is_diag) {
 // as the concatenation over connected alpha strings A' of the beta lists,
 // two 32-entry rounds in flight, threshold compaction by ballot and
 // streaming stores (the output must not evict the integrals from L2).
-constexpr int DP_WARPS = 8;
-// resident CTAs per SM: 80 registers per thread (measured: 3 x 8 warps at
-// 80 registers beat 4 x 8 warps at 64 on the CAS(12e,12o) fill by 7%)
-constexpr int DP_CTAS = 3;
+constexpr int DP_WARPS = 12;
+// resident CTAs per SM: 24 warps of 80 registers (measured on the
+// CAS(12e,12o) fill: 24 warps at 80 registers beat 32 at 64 by 7 %; of the
+// 24-warp shapes 12 x 2 is ~1.5 % ahead of 8 x 3 and 6 x 4, since 12 rows
+// share each staged beta list)
+constexpr int DP_CTAS = 2;
 constexpr int DP_THREADS = 32 * DP_WARPS;
 
 struct DPShared {
