@@ -201,6 +201,37 @@ int macis_b200_davidson_ex(const macis_b200_csr* A,
                            const macis_b200_davidson_opts* opts, double* X,
                            double* E, int64_t* niter, unsigned flags);
 
+/* Matrix-free Hamiltonian over one determinant list, for lists whose CSR
+ * matrix would not fit in device memory: every application evaluates the
+ * elements again from the determinants and the integrals (the same
+ * enumeration, Slater-Condon rules and threshold as macis_b200_build_csr,
+ * double_loop.hpp:31-98) and accumulates H x without storing H. It stands
+ * where the reference hands Davidson a SparseMatrixOperator
+ * (include/macis/solvers/davidson.hpp:47-58): the reference's davidson
+ * (:129-225) accepts any functor with operator_action. flags: with
+ * MACIS_B200_HOP_FP32 the off-diagonal elements are rounded to FP32 before
+ * the product (the values of an FP32-valued CSR matrix; the diagonal stays
+ * FP64), MACIS_B200_DEVICE_PTRS for a device determinant list. Sums run in
+ * enumeration order, not column order, so results agree with the CSR
+ * product to rounding (~1e-15 relative), not bit for bit. */
+#define MACIS_B200_HOP_FP32 2u
+typedef struct macis_b200_hop macis_b200_hop;
+int macis_b200_hop_create(const macis_b200_ham* h, const uint64_t* dets,
+                          size_t ndets, double H_thresh, unsigned flags,
+                          macis_b200_hop** out);
+int macis_b200_hop_destroy(macis_b200_hop* op);
+/* AV = alpha * H * V + beta * AV for K columns, as macis_b200_spmv. */
+int macis_b200_hop_apply(const macis_b200_hop* op, int64_t K, double alpha,
+                         const double* V, int64_t LDV, double beta, double* AV,
+                         int64_t LDAV, unsigned flags);
+/* Diagonal of H, FP64 (submatrix.hpp:264-292 on the matrix it stands for). */
+int macis_b200_hop_diagonal(const macis_b200_hop* op, double* D,
+                            unsigned flags);
+/* macis_b200_davidson_ex with the matrix-free operator. */
+int macis_b200_hop_davidson(const macis_b200_hop* op,
+                            const macis_b200_davidson_opts* opts, double* X,
+                            double* E, int64_t* niter, unsigned flags);
+
 /* Lowest nwant eigenpairs (W ascending, eigenvectors in the columns of Vec,
  * ld k) of the symmetric k x k matrix whose lower triangle is `lower`
  * (column-major, ld k): the syev step of lobpcgxx::rayleigh_ritz

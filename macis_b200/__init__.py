@@ -19,8 +19,8 @@ from .asci import (ASCISettings, MCSCFSettings, asci_grow, asci_iter,  # noqa
                    asci_pairs, asci_refine, asci_search, last_search_stats,
                    reorder_ci_on_coeff)
 from .hamiltonian import (DeviceCSR, HamiltonianGenerator,  # noqa: F401
-                          make_csr_hamiltonian, make_csr_hamiltonian_block,
-                          row_bounds)
+                          MatrixFreeHamiltonian, make_csr_hamiltonian,
+                          make_csr_hamiltonian_block, row_bounds)
 from .integrals import fcidump_fill, synthetic_integrals  # noqa: F401
 from .screening import (ScreeningNetwork, ScreenSettings,  # noqa: F401
                         unit_features, unit_width)

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libmacis_b200.so")
 
 OK, EINVAL, ENOMEM, ECAPACITY, ETIMEOUT, ENOCONV, ECUDA, ENOGROW = range(8)
 DEVICE_PTRS = 1
+HOP_FP32 = 2  # matrix-free H: off-diagonal elements rounded to FP32
 FP64, MIXED = 0, 1
 
 _p64 = C.POINTER(C.c_uint64)
@@ -123,6 +124,16 @@ _SIGS = {
     "macis_b200_asci_unit_features": (C.c_int, [_vp, _vp, _sz, C.c_double, _vp,
                                                 _sz, _sz, _vp,
                                                 C.POINTER(_sz)]),
+    "macis_b200_hop_create": (C.c_int, [_vp, _vp, _sz, C.c_double, C.c_uint,
+                                        C.POINTER(_vp)]),
+    "macis_b200_hop_destroy": (C.c_int, [_vp]),
+    "macis_b200_hop_apply": (C.c_int, [_vp, C.c_int64, C.c_double, _vp,
+                                       C.c_int64, C.c_double, _vp, C.c_int64,
+                                       C.c_uint]),
+    "macis_b200_hop_diagonal": (C.c_int, [_vp, _vp, C.c_uint]),
+    "macis_b200_hop_davidson": (C.c_int, [_vp, C.POINTER(DavidsonOptsC), _vp,
+                                          C.POINTER(C.c_double),
+                                          C.POINTER(C.c_int64), C.c_uint]),
 }
 
 EXPORTS = tuple(_SIGS)

@@ -512,3 +512,93 @@ int macis_b200_mlp_samples(const macis_b200_mlp* m, size_t* n, uint16_t* X,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------- matrix-free H
+extern "C" {
+
+int macis_b200_hop_create(const macis_b200_ham* h, const uint64_t* dets,
+                          size_t ndets, double H_thresh, unsigned flags,
+                          macis_b200_hop** out) {
+  return guarded([&] {
+    MB_REQUIRE(h && out, MACIS_B200_EINVAL, "null argument");
+    require_dets(dets, ndets, flags);
+    *out = hop_create(const_cast<macis_b200_ham*>(h), dets, ndets, H_thresh,
+                      (flags & MACIS_B200_HOP_FP32) != 0,
+                      (flags & MACIS_B200_DEVICE_PTRS) != 0);
+  });
+}
+
+int macis_b200_hop_destroy(macis_b200_hop* op) {
+  return guarded([&] { hop_destroy(op); });
+}
+
+int macis_b200_hop_apply(const macis_b200_hop* op, int64_t K, double alpha,
+                         const double* V, int64_t LDV, double beta, double* AV,
+                         int64_t LDAV, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(op && (K == 0 || (V && AV)), MACIS_B200_EINVAL, "null argument");
+    const int64_t n = hop_size(op);
+    MB_REQUIRE(K >= 0 && LDV >= n && LDAV >= n, MACIS_B200_EINVAL,
+               "bad leading dimension");
+    cudaStream_t s = hop_stream(op);
+    if(flags & MACIS_B200_DEVICE_PTRS) {
+      for(int64_t k = 0; k < K; ++k)
+        hop_apply(op, alpha, V + k * LDV, beta, AV + k * LDAV);
+    } else {
+      Arena W(s);
+      double* dv = W.get<double>(size_t(n));
+      double* dy = W.get<double>(size_t(n));
+      for(int64_t k = 0; k < K; ++k) {
+        MB_CUDA(cudaMemcpyAsync(dv, V + k * LDV, n * 8, cudaMemcpyHostToDevice, s));
+        if(beta != 0.0)
+          MB_CUDA(cudaMemcpyAsync(dy, AV + k * LDAV, n * 8,
+                                  cudaMemcpyHostToDevice, s));
+        hop_apply(op, alpha, dv, beta, dy);
+        MB_CUDA(cudaMemcpyAsync(AV + k * LDAV, dy, n * 8,
+                                cudaMemcpyDeviceToHost, s));
+      }
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int macis_b200_hop_diagonal(const macis_b200_hop* op, double* D,
+                            unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(op && D, MACIS_B200_EINVAL, "null argument");
+    cudaStream_t s = hop_stream(op);
+    const auto k = (flags & MACIS_B200_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice
+                                                    : cudaMemcpyDeviceToHost;
+    MB_CUDA(cudaMemcpyAsync(D, hop_diag(op), hop_size(op) * 8, k, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int macis_b200_hop_davidson(const macis_b200_hop* op,
+                            const macis_b200_davidson_opts* o, double* X,
+                            double* E, int64_t* niter, unsigned flags) {
+  int rc = MACIS_B200_OK;
+  int st = guarded([&] {
+    MB_REQUIRE(op && o && X && E && niter, MACIS_B200_EINVAL, "null argument");
+    cudaStream_t s = hop_stream(op);
+    const int64_t n = hop_size(op);
+    DevBuf<double> x(X, size_t(n), flags, s);
+    DavOperator dop;
+    dop.n = n;
+    dop.diag = hop_diag(op);
+    dop.s = s;
+    dop.apply = [op](const double* xin, double* y) {
+      hop_apply(op, 1.0, xin, 0.0, y);
+    };
+    rc = davidson_op(dop, o->max_m, o->tol, o->use_guess != 0, x.d, E, niter,
+                     o->restart_keep, o->max_iter);
+    if(!(flags & MACIS_B200_DEVICE_PTRS))
+      MB_CUDA(cudaMemcpyAsync(X, x.d, n * 8, cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  });
+  if(st) return st;
+  if(rc == MACIS_B200_ENOCONV) g_err = "Davidson Did Not Converge!";
+  return rc;
+}
+
+}  // extern "C"

@@ -311,17 +311,31 @@ int davidson_device(const macis_b200_csr* A, int64_t max_m, double tol,
                     bool use_guess, double* X, double* E, int64_t* niter,
                     int restart_keep, int64_t max_iter) {
   MB_REQUIRE(A->m == A->n, MACIS_B200_EINVAL, "Davidson needs a square matrix");
-  const int64_t N = A->m;
+  DavOperator op;
+  op.n = A->m;
+  op.diag = A->diag;
+  op.s = A->stream;
+  op.apply = [A](const double* x, double* y) {
+    spmv_device_x64(A, 1.0, x, 0.0, y, A->stream);
+  };
+  return davidson_op(op, max_m, tol, use_guess, X, E, niter, restart_keep,
+                     max_iter);
+}
+
+int davidson_op(const DavOperator& op, int64_t max_m, double tol,
+                bool use_guess, double* X, double* E, int64_t* niter,
+                int restart_keep, int64_t max_iter) {
+  const int64_t N = op.n;
   MB_REQUIRE(N > 0, MACIS_B200_EINVAL, "Davidson: empty matrix");
   MB_REQUIRE(max_m >= 1 && max_m <= 1000, MACIS_B200_EINVAL,
              "Davidson: max_m must be in [1, 1000]");
   MB_REQUIRE(restart_keep >= 0 && restart_keep < max_m, MACIS_B200_EINVAL,
              "Davidson: restart_keep must be in [0, max_m)");
-  cudaStream_t s = A->stream;
+  cudaStream_t s = op.s;
   Arena Ar(s);
   max_m = std::min<int64_t>(max_m, N);
   if(restart_keep >= max_m) restart_keep = int(max_m) - 1;
-  const double* D = A->diag;
+  const double* D = op.diag;
   if(!use_guess) {
     // diagonal_guess: unit vector at the first minimum of the diagonal
     std::vector<double> hD(N);
@@ -339,7 +353,7 @@ int davidson_device(const macis_b200_csr* A, int64_t max_m, double tol,
   double* tmp = restart_keep ? Ar.get<double>(size_t(N) * restart_keep) : nullptr;
   DavCtx ctx(s, N, Ar);
   MB_CUDA(cudaMemcpyAsync(V, X, N * 8, cudaMemcpyDeviceToDevice, s));
-  spmv_device_x64(A, 1.0, V, 0.0, AV, s);
+  op.apply(V, AV);
   MB_CUDA(cudaMemcpyAsync(V + N, AV, N * 8, cudaMemcpyDeviceToDevice, s));
   ctx.cgs2(V, 1, V + N);
 
@@ -358,7 +372,7 @@ int davidson_device(const macis_b200_csr* A, int64_t max_m, double tol,
   int64_t i = 1;  // index of the newest basis vector (AV_i not yet formed)
   for(;; ++iter) {
     const int k = int(i + 1);
-    spmv_device_x64(A, 1.0, V + i * N, 0.0, AV + i * N, s);
+    op.apply(V + i * N, AV + i * N);
     // new row of V^T AV: V_i . AV_c for c <= i (lower triangle)
     ctx.multidot(AV, N, k, V + i * N, ctx.dots);
     MB_CUDA(cudaMemcpyAsync(rowdots.data(), ctx.dots, k * 8,

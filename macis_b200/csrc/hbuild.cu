@@ -1469,6 +1469,141 @@ __global__ void rowptr_cast_k(const int64_t* in, size_t n, CI* out) {
 }
 
 // ----------------------------------------------------------- driver
+// General-path tables of a (bra, ket) pair: kets sorted by (alpha, beta)
+// with their alpha groups, the bra rows' groups, the alpha connectivity of
+// bra groups to ket groups (pa <= 3 first, pa == 4 last), beta hash tables
+// of the large ket groups and the beta-major view of the kets. Everything
+// lives in A; `sub` says that bra is the contiguous block of ket starting
+// at row r0.
+template <int NBITS>
+static GenData gen_plan(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
+                        const uint64_t* ket, size_t nket, bool sub, int64_t r0,
+                        Arena& A) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  cudaStream_t s = A.s;
+  const int sms = num_sms();
+  constexpr int KW = GenKey<NBITS>::KW;
+  auto sort_side = [&](const uint64_t* dets, size_t n, uint64_t*& keys,
+                       uint32_t*& idx, int64_t*& goff, uint64_t*& galpha,
+                       uint64_t*& sbeta, int32_t* rowgroup, uint32_t& ng) {
+    keys = A.get<uint64_t>(n * KW);
+    idx = A.get<uint32_t>(n);
+    uint64_t* k2 = A.get<uint64_t>(n * KW);
+    uint32_t* i2 = A.get<uint32_t>(n);
+    gen_keys_k<NBITS><<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(dets, n,
+                                                               keys, idx), note_launch();
+    radix_sort<KW, uint32_t>(keys, idx, k2, i2, n, A);
+    A.release(k2);
+    A.release(i2);
+    uint32_t* flags = A.get<uint32_t>(n);
+    uint32_t* gx = A.get<uint32_t>(n + 1);
+    auto* nz = A.get<unsigned long long>(1);
+    MB_CUDA(cudaMemsetAsync(nz, 0, 8, s));
+    gen_group_flags_k<NBITS><<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(
+        keys, n, flags, nz), note_launch();
+    exclusive_scan<uint32_t, uint32_t>(flags, gx, n, gx + n, A);
+    ng = to_host(gx + n, s);
+    goff = A.get<int64_t>(ng + 1);
+    galpha = A.get<uint64_t>((ng + 1) * NSW);
+    sbeta = A.get<uint64_t>(n * NSW);
+    gen_groups_k<NBITS><<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(
+        keys, idx, flags, gx, n, goff, galpha, sbeta, rowgroup), note_launch();
+    gen_group_end_k<<<1, 1, 0, s>>>(goff, ng, int64_t(n)), note_launch();
+  };
+  uint64_t *kkeys, *kalpha, *ksbeta;
+  uint32_t *kidx, nkg = 0;
+  int64_t* kgoff;
+  int32_t* rowgroup = A.get<int32_t>(sub ? nket : nbra);
+  sort_side(ket, nket, kkeys, kidx, kgoff, kalpha, ksbeta,
+            sub ? rowgroup : nullptr, nkg);
+  if(sub) rowgroup += r0;
+  const uint64_t* balpha = kalpha;
+  uint32_t nbg = nkg;
+  if(!sub) {
+    uint64_t *bkeys, *bsbeta, *bal;
+    uint32_t* bidx;
+    int64_t* bgoff;
+    sort_side(bra, nbra, bkeys, bidx, bgoff, bal, bsbeta, rowgroup, nbg);
+    balpha = bal;
+  }
+  // alpha connectivity bra groups -> ket groups
+  int64_t* acnt = A.get<int64_t>(nbg + 1);
+  int64_t* acnt4 = A.get<int64_t>(nbg + 1);
+  int64_t* aoff = A.get<int64_t>(nbg + 1);
+  const unsigned ga = grid_for(size_t(nbg) * 32, 256, 16 * sms);
+  gen_aconn_k<NSW><<<ga, 256, 0, s>>>(balpha, nbg, kalpha, nkg, nullptr,
+                                      acnt, acnt4, nullptr, nullptr), note_launch();
+  exclusive_scan<int64_t, int64_t>(acnt, aoff, nbg, aoff + nbg, A);
+  const int64_t natot = to_host(aoff + nbg, s);
+  int32_t* acol = A.get<int32_t>(natot + 1);
+  uint8_t* apa = A.get<uint8_t>(natot + 1);
+  gen_aconn_k<NSW><<<ga, 256, 0, s>>>(balpha, nbg, kalpha, nkg, aoff, acnt,
+                                      acnt4, acol, apa), note_launch();
+  // beta hash tables of the large ket groups
+  int64_t* hoff = A.get<int64_t>(nkg + 1);
+  int32_t* gbpop = A.get<int32_t>(nkg + 1);
+  int32_t* htab;
+  {
+    int64_t* hsz = A.get<int64_t>(nkg + 1);
+    const unsigned gh = grid_for(size_t(nkg) * 32, 256, 16 * sms);
+    gen_hsize_k<NSW><<<gh, 256, 0, s>>>(kgoff, nkg, ksbeta, hsz, gbpop), note_launch();
+    exclusive_scan<int64_t, int64_t>(hsz, hoff, nkg, hoff + nkg, A);
+    A.release(hsz);
+    const int64_t htot = to_host(hoff + nkg, s);
+    htab = A.get<int32_t>(size_t(std::max<int64_t>(htot, 1)));
+    MB_CUDA(cudaMemsetAsync(htab, 0xFF, size_t(std::max<int64_t>(htot, 1)) * 4, s));
+    if(htot > 0)
+      gen_hinsert_k<NSW><<<gh, 256, 0, s>>>(kgoff, nkg, ksbeta, hoff, htab), note_launch();
+  }
+  // beta-major view of the kets
+  uint64_t *bm_alpha, *bgbeta;
+  uint32_t* bm_m;
+  int32_t* mgroup;
+  int64_t* bgoff;
+  int64_t nbgb = 0;
+  {
+    uint64_t* bkeys = A.get<uint64_t>(nket * KW);
+    uint32_t* bidx = A.get<uint32_t>(nket);
+    uint64_t* k2 = A.get<uint64_t>(nket * KW);
+    uint32_t* i2 = A.get<uint32_t>(nket);
+    gen_bkeys_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
+        ket, nket, bkeys, bidx), note_launch();
+    radix_sort<KW, uint32_t>(bkeys, bidx, k2, i2, nket, A);
+    A.release(k2);
+    A.release(i2);
+    uint32_t* amaj = A.get<uint32_t>(nket);
+    gen_invert_k<<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(kidx, nket,
+                                                             amaj), note_launch();
+    mgroup = A.get<int32_t>(nket);
+    MB_CUDA(cudaMemsetAsync(mgroup, 0xFF, nket * 4, s));
+    gen_mgroup_k<<<grid_for(size_t(nkg) * 32, 256, 16 * sms), 256, 0, s>>>(
+        kgoff, nkg, mgroup), note_launch();
+    bm_alpha = A.get<uint64_t>(nket * NSW);
+    bm_m = A.get<uint32_t>(nket);
+    uint32_t* bfl = A.get<uint32_t>(nket);
+    uint32_t* bgx = A.get<uint32_t>(nket + 1);
+    gen_bmajor_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
+        bkeys, bidx, nket, amaj, bm_alpha, bm_m, bfl), note_launch();
+    exclusive_scan<uint32_t, uint32_t>(bfl, bgx, nket, bgx + nket, A);
+    nbgb = int64_t(to_host(bgx + nket, s));
+    bgoff = A.get<int64_t>(size_t(nbgb) + 1);
+    bgbeta = A.get<uint64_t>((size_t(nbgb) + 1) * NSW);
+    gen_bgroups_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
+        bkeys, bfl, bgx, nket, bgoff, bgbeta), note_launch();
+    gen_group_end_k<<<1, 1, 0, s>>>(bgoff, uint32_t(nbgb), int64_t(nket)), note_launch();
+    A.release(bkeys);
+    A.release(bidx);
+    A.release(amaj);
+    A.release(bfl);
+    A.release(bgx);
+  }
+  GenData gd{rowgroup, aoff, acol, apa, kgoff, kalpha, ksbeta, kidx,
+             hoff, htab, gbpop, h->norb, acnt4,
+             bgbeta, bgoff, nbgb, bm_alpha, bm_m, mgroup};
+  return gd;
+}
+
 template <int NBITS, typename CI, typename VT>
 static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
                        const uint64_t* ket, size_t nket, double thresh,
@@ -1699,124 +1834,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     MB_CUDA(cudaGetLastError());
   } else {
     // ------------------------------------------------ general path
-    constexpr int KW = GenKey<NBITS>::KW;
-    auto sort_side = [&](const uint64_t* dets, size_t n, uint64_t*& keys,
-                         uint32_t*& idx, int64_t*& goff, uint64_t*& galpha,
-                         uint64_t*& sbeta, int32_t* rowgroup, uint32_t& ng) {
-      keys = A.get<uint64_t>(n * KW);
-      idx = A.get<uint32_t>(n);
-      uint64_t* k2 = A.get<uint64_t>(n * KW);
-      uint32_t* i2 = A.get<uint32_t>(n);
-      gen_keys_k<NBITS><<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(dets, n,
-                                                                 keys, idx), note_launch();
-      radix_sort<KW, uint32_t>(keys, idx, k2, i2, n, A);
-      A.release(k2);
-      A.release(i2);
-      uint32_t* flags = A.get<uint32_t>(n);
-      uint32_t* gx = A.get<uint32_t>(n + 1);
-      auto* nz = A.get<unsigned long long>(1);
-      MB_CUDA(cudaMemsetAsync(nz, 0, 8, s));
-      gen_group_flags_k<NBITS><<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(
-          keys, n, flags, nz), note_launch();
-      exclusive_scan<uint32_t, uint32_t>(flags, gx, n, gx + n, A);
-      ng = to_host(gx + n, s);
-      goff = A.get<int64_t>(ng + 1);
-      galpha = A.get<uint64_t>((ng + 1) * NSW);
-      sbeta = A.get<uint64_t>(n * NSW);
-      gen_groups_k<NBITS><<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(
-          keys, idx, flags, gx, n, goff, galpha, sbeta, rowgroup), note_launch();
-      gen_group_end_k<<<1, 1, 0, s>>>(goff, ng, int64_t(n)), note_launch();
-    };
-    uint64_t *kkeys, *kalpha, *ksbeta;
-    uint32_t *kidx, nkg = 0;
-    int64_t* kgoff;
-    int32_t* rowgroup = A.get<int32_t>(sub ? nket : nbra);
-    sort_side(ket, nket, kkeys, kidx, kgoff, kalpha, ksbeta,
-              sub ? rowgroup : nullptr, nkg);
-    if(sub) rowgroup += r0;
-    const uint64_t* balpha = kalpha;
-    uint32_t nbg = nkg;
-    if(!sub) {
-      uint64_t *bkeys, *bsbeta, *bal;
-      uint32_t* bidx;
-      int64_t* bgoff;
-      sort_side(bra, nbra, bkeys, bidx, bgoff, bal, bsbeta, rowgroup, nbg);
-      balpha = bal;
-    }
-    // alpha connectivity bra groups -> ket groups
-    int64_t* acnt = A.get<int64_t>(nbg + 1);
-    int64_t* acnt4 = A.get<int64_t>(nbg + 1);
-    int64_t* aoff = A.get<int64_t>(nbg + 1);
-    const unsigned ga = grid_for(size_t(nbg) * 32, 256, 16 * sms);
-    gen_aconn_k<NSW><<<ga, 256, 0, s>>>(balpha, nbg, kalpha, nkg, nullptr,
-                                        acnt, acnt4, nullptr, nullptr), note_launch();
-    exclusive_scan<int64_t, int64_t>(acnt, aoff, nbg, aoff + nbg, A);
-    const int64_t natot = to_host(aoff + nbg, s);
-    int32_t* acol = A.get<int32_t>(natot + 1);
-    uint8_t* apa = A.get<uint8_t>(natot + 1);
-    gen_aconn_k<NSW><<<ga, 256, 0, s>>>(balpha, nbg, kalpha, nkg, aoff, acnt,
-                                        acnt4, acol, apa), note_launch();
-    // beta hash tables of the large ket groups
-    int64_t* hoff = A.get<int64_t>(nkg + 1);
-    int32_t* gbpop = A.get<int32_t>(nkg + 1);
-    int32_t* htab;
-    {
-      int64_t* hsz = A.get<int64_t>(nkg + 1);
-      const unsigned gh = grid_for(size_t(nkg) * 32, 256, 16 * sms);
-      gen_hsize_k<NSW><<<gh, 256, 0, s>>>(kgoff, nkg, ksbeta, hsz, gbpop), note_launch();
-      exclusive_scan<int64_t, int64_t>(hsz, hoff, nkg, hoff + nkg, A);
-      A.release(hsz);
-      const int64_t htot = to_host(hoff + nkg, s);
-      htab = A.get<int32_t>(size_t(std::max<int64_t>(htot, 1)));
-      MB_CUDA(cudaMemsetAsync(htab, 0xFF, size_t(std::max<int64_t>(htot, 1)) * 4, s));
-      if(htot > 0)
-        gen_hinsert_k<NSW><<<gh, 256, 0, s>>>(kgoff, nkg, ksbeta, hoff, htab), note_launch();
-    }
-    // beta-major view of the kets
-    uint64_t *bm_alpha, *bgbeta;
-    uint32_t* bm_m;
-    int32_t* mgroup;
-    int64_t* bgoff;
-    int64_t nbgb = 0;
-    {
-      uint64_t* bkeys = A.get<uint64_t>(nket * KW);
-      uint32_t* bidx = A.get<uint32_t>(nket);
-      uint64_t* k2 = A.get<uint64_t>(nket * KW);
-      uint32_t* i2 = A.get<uint32_t>(nket);
-      gen_bkeys_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
-          ket, nket, bkeys, bidx), note_launch();
-      radix_sort<KW, uint32_t>(bkeys, bidx, k2, i2, nket, A);
-      A.release(k2);
-      A.release(i2);
-      uint32_t* amaj = A.get<uint32_t>(nket);
-      gen_invert_k<<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(kidx, nket,
-                                                               amaj), note_launch();
-      mgroup = A.get<int32_t>(nket);
-      MB_CUDA(cudaMemsetAsync(mgroup, 0xFF, nket * 4, s));
-      gen_mgroup_k<<<grid_for(size_t(nkg) * 32, 256, 16 * sms), 256, 0, s>>>(
-          kgoff, nkg, mgroup), note_launch();
-      bm_alpha = A.get<uint64_t>(nket * NSW);
-      bm_m = A.get<uint32_t>(nket);
-      uint32_t* bfl = A.get<uint32_t>(nket);
-      uint32_t* bgx = A.get<uint32_t>(nket + 1);
-      gen_bmajor_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
-          bkeys, bidx, nket, amaj, bm_alpha, bm_m, bfl), note_launch();
-      exclusive_scan<uint32_t, uint32_t>(bfl, bgx, nket, bgx + nket, A);
-      nbgb = int64_t(to_host(bgx + nket, s));
-      bgoff = A.get<int64_t>(size_t(nbgb) + 1);
-      bgbeta = A.get<uint64_t>((size_t(nbgb) + 1) * NSW);
-      gen_bgroups_k<NBITS><<<grid_for(nket, 256, 8 * sms), 256, 0, s>>>(
-          bkeys, bfl, bgx, nket, bgoff, bgbeta), note_launch();
-      gen_group_end_k<<<1, 1, 0, s>>>(bgoff, uint32_t(nbgb), int64_t(nket)), note_launch();
-      A.release(bkeys);
-      A.release(bidx);
-      A.release(amaj);
-      A.release(bfl);
-      A.release(bgx);
-    }
-    GenData gd{rowgroup, aoff, acol, apa, kgoff, kalpha, ksbeta, kidx,
-               hoff, htab, gbpop, h->norb, acnt4,
-               bgbeta, bgoff, nbgb, bm_alpha, bm_m, mgroup};
+    GenData gd = gen_plan<NBITS>(h, bra, nbra, ket, nket, sub, r0, A);
     const unsigned gr = grid_for(nbra, HB_WARPS, size_t(sms) * 16);
     gen_count_k<NBITS><<<gr, HB_THREADS, 0, s>>>(gd, bra, nbra, rowcnt), note_launch();
     exclusive_scan<int64_t, int64_t>(rowcnt, rowptr64, nbra, rowptr64 + nbra, A);
@@ -1992,5 +2010,161 @@ macis_b200_csr* build_csr_device(macis_b200_ham* h, const uint64_t* bra,
   cudaEventDestroy(e1);
   return out;
 }
+
+}  // namespace mb
+
+// ------------------------------------------------ matrix-free H x
+// The operator keeps its own stream and a copy of the generator's integral
+// pointers: the generator must outlive every product, but destroying the
+// operator never touches it.
+struct macis_b200_hop {
+  mb::Ints I{};
+  int nbits = 64;
+  cudaStream_t stream = nullptr;
+  int64_t n = 0;
+  double thresh = 0.0;
+  bool mixed = false;
+  uint64_t* dets = nullptr;  // device copy of the determinant list
+  double* diag = nullptr;    // H_ii
+  mb::Arena* A = nullptr;    // owns dets, diag and the enumeration tables
+  mb::GenData g{};
+};
+
+namespace mb {
+
+// y = alpha H x + beta y, one warp per row: the candidates of the general
+// build's enumeration (gen_enumerate), each element evaluated, thresholded
+// as in the build and accumulated into the row sum (no storage). mixed:
+// off-diagonal elements rounded to FP32 first, as in an FP32-valued CSR.
+template <int NBITS>
+__global__ void __launch_bounds__(HB_THREADS)
+    gen_apply_k(Ints I, GenData g, const uint64_t* dets, int64_t n,
+                const double* __restrict__ hdiag, double thresh, int mixed,
+                double alpha, const double* __restrict__ x, double beta,
+                double* __restrict__ y) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  extern __shared__ __align__(16) uint8_t gen_ov[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t nwarp = int64_t(gridDim.x) * HB_WARPS;
+  for(int64_t row = int64_t(blockIdx.x) * HB_WARPS + wid; row < n;
+      row += nwarp) {
+    const int32_t rg = g.rowgroup[row];
+    double acc = 0.0;
+    if(rg >= 0) {
+      const uint64_t* bd = dets + row * D::NW;
+      const Spin<NSW> ba = D::alpha(bd), bb = D::beta(bd);
+      const double hd = hdiag[row];
+      gen_enumerate<NSW>(g, rg, ba, bb, gen_ov + wid * 256,
+                         [&](bool act, int64_t m, int32_t kg, int pa, int pb) {
+        if(act) {
+          const uint32_t col = g.sidx[m];
+          double h;
+          if(pa == 0 && pb == 0)
+            h = hd;
+          else
+            h = me_generic(I, ba, bb, ld_spin<NSW>(g.kalpha, kg),
+                           ld_spin<NSW>(g.sbeta, m));
+          if(fabs(h) > thresh) {
+            if(mixed && int64_t(col) != row) h = double(float(h));
+            acc += h * x[col];
+          }
+        }
+      });
+#pragma unroll
+      for(int o = 16; o > 0; o >>= 1)
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    }
+    if(lane == 0) y[row] = alpha * acc + (beta != 0.0 ? beta * y[row] : 0.0);
+  }
+}
+
+macis_b200_hop* hop_create(macis_b200_ham* h, const uint64_t* dets, size_t n,
+                           double thresh, bool mixed, bool device_ptrs) {
+  MB_REQUIRE(n > 0, MACIS_B200_EINVAL, "empty determinant list");
+  MB_REQUIRE(n < (size_t(1) << 31), MACIS_B200_ECAPACITY,
+             "matrix-free H needs < 2^31 determinants");
+  const size_t nw = size_t(h->nbits / 64);
+  const int sms = num_sms();
+  const Ints I = h->ints();
+  auto* op = new macis_b200_hop;
+  op->I = I;
+  op->nbits = h->nbits;
+  op->n = int64_t(n);
+  op->thresh = thresh;
+  op->mixed = mixed;
+  if(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) !=
+     cudaSuccess) {
+    delete op;
+    MB_REQUIRE(false, MACIS_B200_ECUDA, "stream creation failed");
+  }
+  cudaStream_t s = op->stream;
+  try {
+    op->A = new Arena(s);
+    op->dets = op->A->get<uint64_t>(n * nw);
+    MB_CUDA(cudaMemcpyAsync(op->dets, dets, n * nw * 8,
+                            device_ptrs ? cudaMemcpyDeviceToDevice
+                                        : cudaMemcpyHostToDevice, s));
+    op->diag = op->A->get<double>(n);
+#define MB_HOP_PLAN(NB)                                                     \
+  hdiag_k<NB><<<grid_for(n, 256, 8 * sms), 256, 0, s>>>(I, op->dets, n,     \
+                                                        op->diag),          \
+      note_launch();                                                        \
+  op->g = gen_plan<NB>(h, op->dets, n, op->dets, n, true, 0, *op->A);
+    if(h->nbits == 64) {
+      MB_HOP_PLAN(64)
+    } else if(h->nbits == 128) {
+      MB_HOP_PLAN(128)
+    } else {
+      MB_HOP_PLAN(256)
+    }
+#undef MB_HOP_PLAN
+    MB_CUDA(cudaStreamSynchronize(s));
+  } catch(...) {
+    cudaStreamSynchronize(s);
+    delete op->A;
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    delete op;
+    throw;
+  }
+  return op;
+}
+
+void hop_apply(const macis_b200_hop* op, double alpha, const double* x,
+               double beta, double* y) {
+  cudaStream_t s = op->stream;
+  const unsigned gr = grid_for(size_t(op->n), HB_WARPS, size_t(num_sms()) * 16);
+  constexpr int dyn = HB_WARPS * 256;
+  const Ints I = op->I;
+#define MB_HOP_APPLY(NB)                                                     \
+  gen_apply_k<NB><<<gr, HB_THREADS, dyn, s>>>(I, op->g, op->dets, op->n,     \
+                                              op->diag, op->thresh,          \
+                                              op->mixed ? 1 : 0, alpha, x,   \
+                                              beta, y),                      \
+      note_launch();
+  if(op->nbits == 64) {
+    MB_HOP_APPLY(64)
+  } else if(op->nbits == 128) {
+    MB_HOP_APPLY(128)
+  } else {
+    MB_HOP_APPLY(256)
+  }
+#undef MB_HOP_APPLY
+  MB_CUDA(cudaGetLastError());
+}
+
+void hop_destroy(macis_b200_hop* op) {
+  if(!op) return;
+  cudaStreamSynchronize(op->stream);
+  delete op->A;
+  cudaStreamSynchronize(op->stream);
+  cudaStreamDestroy(op->stream);
+  delete op;
+}
+
+int64_t hop_size(const macis_b200_hop* op) { return op->n; }
+const double* hop_diag(const macis_b200_hop* op) { return op->diag; }
+cudaStream_t hop_stream(const macis_b200_hop* op) { return op->stream; }
 
 }  // namespace mb

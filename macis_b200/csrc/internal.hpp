@@ -1,6 +1,7 @@
 // Internal handle types and cross-file entry points of libmacis_b200.
 #pragma once
 #include <cuda_runtime.h>
+#include <functional>
 
 #include <string>
 #include <vector>
@@ -118,6 +119,29 @@ void spmv_device(const macis_b200_csr* A, double alpha, const double* x,
 int davidson_device(const macis_b200_csr* A, int64_t max_m, double tol,
                     bool use_guess, double* X, double* E, int64_t* niter,
                     int restart_keep, int64_t max_iter);
+
+// The operator Davidson works with: y = H x on device vectors of length n,
+// diag(H) in device memory, everything on stream s (the reference's
+// davidson takes any functor with operator_action, davidson.hpp:47-58, 129).
+struct DavOperator {
+  int64_t n = 0;
+  const double* diag = nullptr;
+  cudaStream_t s = nullptr;
+  std::function<void(const double* x, double* y)> apply;
+};
+int davidson_op(const DavOperator& op, int64_t max_m, double tol,
+                bool use_guess, double* X, double* E, int64_t* niter,
+                int restart_keep, int64_t max_iter);
+
+// Matrix-free H over one determinant list (hbuild.cu).
+macis_b200_hop* hop_create(macis_b200_ham* h, const uint64_t* dets, size_t n,
+                           double thresh, bool mixed, bool device_ptrs);
+void hop_apply(const macis_b200_hop* op, double alpha, const double* x,
+               double beta, double* y);
+void hop_destroy(macis_b200_hop* op);
+int64_t hop_size(const macis_b200_hop* op);
+const double* hop_diag(const macis_b200_hop* op);
+cudaStream_t hop_stream(const macis_b200_hop* op);
 
 // Lowest nwant eigenpairs of a k x k symmetric matrix (lower triangle).
 void small_syev_lowest(int k, const double* lower, int nwant, double* W,

@@ -10,6 +10,10 @@ Mirrors the reference API:
   functions of include/macis/csr_hamiltonian.hpp:23-45.
 * ``DeviceCSR`` -- the sparsexx::csr_matrix<double, index_t> result, kept in
   HBM (``to_host`` gives the by-value arrays of the reference).
+* ``MatrixFreeHamiltonian`` -- H over one determinant list without storing
+  it, for lists whose CSR matrix does not fit in device memory: the operator
+  the reference's davidson accepts (include/macis/solvers/davidson.hpp:
+  47-58, 129).
 """
 import ctypes as C
 
@@ -19,7 +23,7 @@ from . import _lib
 from ._lib import LIB, check
 
 __all__ = ["HamiltonianGenerator", "DeviceCSR", "make_csr_hamiltonian_block",
-           "make_csr_hamiltonian", "row_bounds"]
+           "make_csr_hamiltonian", "row_bounds", "MatrixFreeHamiltonian"]
 
 
 def row_bounds(M, world_size, rank):
@@ -194,3 +198,54 @@ def make_csr_hamiltonian(dets, ham_gen, H_thresh, index_t=np.int32,
     """csr_hamiltonian.hpp:39-45: square block over one determinant list."""
     return ham_gen.make_csr_hamiltonian_block(dets, dets, H_thresh, index_t,
                                               value_t)
+
+
+class MatrixFreeHamiltonian:
+    """H over one determinant list, applied without storing it: every
+    product evaluates the elements again from the determinants and the
+    integrals (same enumeration, Slater-Condon rules and threshold as the
+    CSR build). value_t=np.float32 rounds the off-diagonal elements to FP32
+    as an FP32-valued CSR matrix would (the diagonal stays FP64). Products
+    agree with the CSR product to rounding (sums in enumeration order)."""
+
+    def __init__(self, dets, ham_gen, H_thresh, value_t=np.float64):
+        flags = _lib.HOP_FP32 if np.dtype(value_t) == np.float32 else 0
+        p = _dev_ptr(dets)
+        if p is not None:
+            flags |= _lib.DEVICE_PTRS
+            n = dets.numel() * 8 // (ham_gen.nbits // 8)
+            keep = dets
+        else:
+            keep = _host_dets(dets, ham_gen.nbits)
+            p, n = keep.ctypes.data, len(keep)
+        h = C.c_void_p()
+        check(LIB.macis_b200_hop_create(ham_gen.handle, p, n, float(H_thresh),
+                                        flags, C.byref(h)))
+        del keep
+        self._h = h
+        self.ham = ham_gen
+        self.m = self.n = int(n)
+        self.value_t = np.float32 if flags & _lib.HOP_FP32 else np.float64
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            LIB.macis_b200_hop_destroy(h)
+            self._h = None
+
+    def diagonal(self):
+        d = np.empty(self.m)
+        check(LIB.macis_b200_hop_diagonal(self._h, d.ctypes.data, 0))
+        return d
+
+    def spmv(self, x, alpha=1.0, beta=0.0, y=None):
+        """alpha * H x + beta * y on host vectors."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.m) if y is None else np.array(y, dtype=np.float64)
+        check(LIB.macis_b200_hop_apply(self._h, 1, alpha, x.ctypes.data,
+                                       self.n, beta, y.ctypes.data, self.m, 0))
+        return y

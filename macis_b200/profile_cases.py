@@ -5,6 +5,7 @@
     python -m macis_b200.profile_cases hbuild_c2s  # 12 orbitals, 3a/6b: the
         # beta lists of CAS(12e,12o) at a quarter of its output (3.3 GB)
     python -m macis_b200.profile_cases spmv_c1     # FP64 SpMV on CAS(10e,10o)
+    python -m macis_b200.profile_cases hop_c2      # matrix-free H x, CAS(12e,12o)
     python -m macis_b200.profile_cases hbuild_sel  # selected (shuffled) space
     python -m macis_b200.profile_cases asci_n48    # one ASCI search, n = 48
         # (--ncore core determinants, default 10000)
@@ -75,6 +76,26 @@ def asci_n48(reps, ncore=10000):
         print(f"asci {r['seconds']:.3f} s raw={r['raw_pairs']} "
               f"unique={r['unique_pairs']} batches={r['batches']} "
               f"phases={r['phase_ms']}")
+
+
+def hop(norb, k, reps):
+    """Matrix-free H x on the FCI list against the CSR product (host-staged
+    vectors; the determinant list and the tables stay on the device)."""
+    T, V, dets = fci(norb, k)
+    H = mb.HamiltonianGenerator(T, V, 64)
+    t = time.perf_counter()
+    Hm = mb.MatrixFreeHamiltonian(dets, H, EPS)
+    print(f"matrix-free setup {1e3 * (time.perf_counter() - t):.1f} ms")
+    x = np.random.default_rng(0).standard_normal(len(dets))
+    for _ in range(reps):
+        t = time.perf_counter()
+        y = Hm.spmv(x)
+        print(f"matrix-free H x {1e3 * (time.perf_counter() - t):.1f} ms")
+    A = mb.make_csr_hamiltonian(dets, H, EPS)
+    t = time.perf_counter()
+    y0 = A.spmv(x)
+    print(f"CSR H x {1e3 * (time.perf_counter() - t):.1f} ms (host-staged), "
+          f"max rel diff {np.abs(y - y0).max() / np.abs(y0).max():.2e}")
 
 
 def _rand_rows(n, din, seed=0):
@@ -188,6 +209,10 @@ def main():
         hbuild(10, 5, a.reps)
     elif a.case == "hbuild_c2":
         hbuild(12, 6, a.reps)
+    elif a.case == "hop_c1":
+        hop(10, 5, a.reps)
+    elif a.case == "hop_c2":
+        hop(12, 6, a.reps)
     elif a.case == "hbuild_c2s":
         hbuild(12, 3, a.reps, kb=6)
     elif a.case == "hbuild_sel":

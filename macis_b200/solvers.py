@@ -45,8 +45,8 @@ def diagonal_guess(N, A, X):
 
 def davidson(N, max_m, op, D, tol, X, use_guess=True, restart_keep=0,
              max_iter=0):
-    """Lowest eigenpair of op.H; X holds the guess and receives the Ritz
-    vector. Returns (iterations, eigenvalue). D (the diagonal) is taken
+    """Lowest eigenpair of op.H (a DeviceCSR or a MatrixFreeHamiltonian); X
+    holds the guess and receives the Ritz vector. Returns (iterations, eigenvalue). D (the diagonal) is taken
     from the matrix itself, as extract_diagonal_elements would give it.
     restart_keep = 0 is the reference solver (at most max_m basis vectors);
     restart_keep > 0 adds a thick restart keeping that many Ritz vectors,
@@ -60,8 +60,10 @@ def davidson(N, max_m, op, D, tol, X, use_guess=True, restart_keep=0,
     it = C.c_int64()
     o = _lib.DavidsonOptsC(int(max_m), float(tol), int(use_guess),
                            int(restart_keep), int(max_iter))
-    rc = LIB.macis_b200_davidson_ex(H.handle, C.byref(o), xs.ctypes.data,
-                                    C.byref(E), C.byref(it), 0)
+    from .hamiltonian import MatrixFreeHamiltonian
+    fn = (LIB.macis_b200_hop_davidson if isinstance(H, MatrixFreeHamiltonian)
+          else LIB.macis_b200_davidson_ex)
+    rc = fn(H.handle, C.byref(o), xs.ctypes.data, C.byref(E), C.byref(it), 0)
     if rc == _lib.ENOCONV:
         raise RuntimeError("Davidson Did Not Converge!")
     check(rc)
