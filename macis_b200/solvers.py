@@ -13,8 +13,9 @@ import time
 import numpy as np
 
 from . import _lib
-from ._lib import ECAPACITY, LIB, MacisError, check
-from .hamiltonian import DeviceCSR, make_csr_hamiltonian
+from ._lib import ECAPACITY, ENOMEM, LIB, MacisError, check
+from .hamiltonian import (DeviceCSR, MatrixFreeHamiltonian,
+                          make_csr_hamiltonian)
 
 __all__ = ["SparseMatrixOperator", "diagonal_guess", "davidson",
            "selected_ci_diag", "small_syev", "FP64", "MIXED"]
@@ -88,12 +89,15 @@ def small_syev(lower, nwant=1):
 def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
                      davidson_res_tol, C=None, precision=FP64,
                      index_t=np.int32, timings=None, restart_keep=0,
-                     max_iter=0):
+                     max_iter=0, matrix_free=None):
     """Build H for `dets` and solve for the lowest root. Returns (E0, C).
     C is used as the guess when max|C| > 1/N (selected_ci_diag.hpp:96-101),
     else the diagonal guess is taken. precision MIXED stores the
     off-diagonal H in FP32 (FP64 diagonal) and keeps residuals, CGS2,
-    Rayleigh-Ritz and the energy in FP64."""
+    Rayleigh-Ritz and the energy in FP64. matrix_free: True applies H
+    without storing it (MatrixFreeHamiltonian), False always stores the
+    CSR matrix, None (default) stores it unless the build runs out of
+    device memory."""
     log = logging.getLogger("ci_solver")
     dets = np.ascontiguousarray(dets, dtype=np.uint64)
     ndets = dets.shape[0]
@@ -102,6 +106,46 @@ def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
              davidson_max_m)
     value_t = np.float32 if precision == MIXED else np.float64
     t0 = time.perf_counter()
+    H = None
+    if matrix_free:
+        H = MatrixFreeHamiltonian(dets, ham_gen, h_el_tol, value_t)
+    else:
+        try:
+            H = _build_csr(dets, ham_gen, h_el_tol, index_t, value_t, log)
+        except MacisError as e:
+            if matrix_free is not None or e.code != ENOMEM:
+                raise
+            log.info("  the CSR matrix does not fit in device memory: "
+                     "matrix-free H")
+            H = MatrixFreeHamiltonian(dets, ham_gen, h_el_tol, value_t)
+    t1 = time.perf_counter()
+    if isinstance(H, MatrixFreeHamiltonian):
+        log.info("  matrix-free H, setup %.5e ms", (t1 - t0) * 1e3)
+    else:
+        log.info("  NNZ = %d, H_DUR = %.5e ms", H.nnz, (t1 - t0) * 1e3)
+        log.info("  HMEM_LOC = %.2e GiB", H.mem_footprint() / 1073741824.0)
+    X = np.zeros(ndets)
+    use_guess = False
+    if C is not None and len(C) == ndets and ndets:
+        if np.max(np.abs(C)) > 1.0 / ndets:
+            X[:] = C
+            use_guess = True
+    it, E = davidson(ndets, davidson_max_m, H, None,
+                     davidson_res_tol, X, use_guess=use_guess,
+                     restart_keep=restart_keep, max_iter=max_iter)
+    t2 = time.perf_counter()
+    log.info("  DAV_NITER = %d, E0 = %.6e Eh, DAVIDSON_DUR = %.5e ms", it, E,
+             (t2 - t1) * 1e3)
+    if timings is not None:
+        timings.update(h_ms=(t1 - t0) * 1e3, dav_ms=(t2 - t1) * 1e3,
+                       nnz=getattr(H, "nnz", None), niter=it)
+    return E, X
+
+
+def _build_csr(dets, ham_gen, h_el_tol, index_t, value_t, log):
+    """The CSR build of selected_ci_diag; index_t None picks int32 while nnz
+    fits and int64 beyond."""
+    ndets = dets.shape[0]
     if index_t is None:
         # int32 indices while nnz fits (2^31 - 1), else int64; the need for
         # int64 is remembered per generator so that later, larger spaces go
@@ -119,22 +163,4 @@ def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
                                      value_t)
     else:
         H = make_csr_hamiltonian(dets, ham_gen, h_el_tol, index_t, value_t)
-    t1 = time.perf_counter()
-    log.info("  NNZ = %d, H_DUR = %.5e ms", H.nnz, (t1 - t0) * 1e3)
-    log.info("  HMEM_LOC = %.2e GiB", H.mem_footprint() / 1073741824.0)
-    X = np.zeros(ndets)
-    use_guess = False
-    if C is not None and len(C) == ndets and ndets:
-        if np.max(np.abs(C)) > 1.0 / ndets:
-            X[:] = C
-            use_guess = True
-    it, E = davidson(ndets, davidson_max_m, SparseMatrixOperator(H), None,
-                     davidson_res_tol, X, use_guess=use_guess,
-                     restart_keep=restart_keep, max_iter=max_iter)
-    t2 = time.perf_counter()
-    log.info("  DAV_NITER = %d, E0 = %.6e Eh, DAVIDSON_DUR = %.5e ms", it, E,
-             (t2 - t1) * 1e3)
-    if timings is not None:
-        timings.update(h_ms=(t1 - t0) * 1e3, dav_ms=(t2 - t1) * 1e3,
-                       nnz=H.nnz, niter=it)
-    return E, X
+    return H

@@ -103,3 +103,24 @@ def test_davidson_matches_csr():
     it1, E1 = mb.davidson(A.m, 60, Hm, None, 1e-8, X1, use_guess=False)
     assert abs(E1 - E0) < 1e-9 and abs(it1 - it0) <= 1
     assert abs(abs(X0 @ X1) - 1.0) < 1e-9
+
+
+def test_selected_ci_diag_matrix_free_and_fallback(monkeypatch):
+    """selected_ci_diag with matrix_free=True, and the default falling back
+    to the matrix-free operator when the CSR build runs out of device
+    memory (simulated: the build raises ENOMEM)."""
+    from macis_b200 import _lib, solvers
+    T, V, sel = _selected(64, seed=6)
+    H = mb.HamiltonianGenerator(T, V, 64)
+    E0, X0 = mb.selected_ci_diag(sel, H, EPS, 80, 1e-8)
+    E1, X1 = mb.selected_ci_diag(sel, H, EPS, 80, 1e-8, matrix_free=True)
+    assert abs(E1 - E0) < 1e-9
+
+    def no_memory(*a, **k):
+        raise _lib.MacisError(_lib.ENOMEM, "out of device memory")
+    monkeypatch.setattr(solvers, "_build_csr", no_memory)
+    t = {}
+    E2, X2 = mb.selected_ci_diag(sel, H, EPS, 80, 1e-8, timings=t)
+    assert abs(E2 - E0) < 1e-9 and t["nnz"] is None
+    with pytest.raises(_lib.MacisError):
+        mb.selected_ci_diag(sel, H, EPS, 80, 1e-8, matrix_free=False)
