@@ -186,12 +186,27 @@ def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12):
     # mixed mode solved with FP32 off-diagonal values)
     A = mb.make_csr_hamiltonian(dets, H, EPS, np.int64)
     Xd = np.asarray(X, dtype=np.float64)
-    E_fp64 = float(Xd @ A.spmv(Xd)) / float(Xd @ Xd)
+    t = time.perf_counter()
+    AX = A.spmv(Xd)
+    csr_ms = 1e3 * (time.perf_counter() - t)
+    E_fp64 = float(Xd @ AX) / float(Xd @ Xd)
     del A
+    # the same product without storing H (host-staged vectors both ways)
+    t = time.perf_counter()
+    Hm = mb.MatrixFreeHamiltonian(dets, H, EPS)
+    hop_setup_ms = 1e3 * (time.perf_counter() - t)
+    t = time.perf_counter()
+    AXm = Hm.spmv(Xd)
+    hop_ms = 1e3 * (time.perf_counter() - t)
+    hop_diff = float(np.abs(AXm - AX).max() / np.abs(AX).max())
+    del Hm
     out = {"mode": mode, "ntdets": int(ntdets), "ndets": len(dets),
            "n": n, "electrons": [k, k], "E_grow": Eg, "E_final": E,
            "E_final_fp64_H": E_fp64, "topk_recall_last": recall,
            "seconds": dt, "grow_seconds": t_grow,
+           "final_product_ms": {"csr": csr_ms, "matrix_free": hop_ms,
+                                "matrix_free_setup": hop_setup_ms,
+                                "max_rel_diff": hop_diff},
            "iterations": m.iteration_log}
     print(json.dumps(out, default=float))
     return out
