@@ -161,6 +161,45 @@ class SparseMatrixOperator {
   }
 };
 
+// Matrix-free H over one determinant list (macis_b200_hop_*), for lists
+// whose CSR matrix does not fit in device memory. operator_action has the
+// signature MACIS's own davidson (davidson.hpp:129) calls on its functor, so
+// macis::davidson(N, max_m, op, D, tol, X) runs with it directly (D from
+// diagonal()). The generator must outlive the operator's products.
+template <size_t N>
+class MatrixFreeOperator {
+  macis_b200_hop* op_ = nullptr;
+  int64_t n_ = 0;
+
+ public:
+  MatrixFreeOperator(const HamiltonianGenerator<N>& ham,
+                     macis::wavefunction_iterator_t<N> b,
+                     macis::wavefunction_iterator_t<N> e, double thresh,
+                     bool fp32_values = false) {
+    n_ = std::distance(b, e);
+    check(macis_b200_hop_create(ham.handle(), n_ ? words<N>(&*b) : nullptr,
+                                size_t(n_), thresh,
+                                fp32_values ? MACIS_B200_HOP_FP32 : 0u, &op_));
+  }
+  MatrixFreeOperator(const MatrixFreeOperator&) = delete;
+  MatrixFreeOperator& operator=(const MatrixFreeOperator&) = delete;
+  ~MatrixFreeOperator() {
+    if(op_) macis_b200_hop_destroy(op_);
+  }
+  const macis_b200_hop* get() const { return op_; }
+  int64_t size() const { return n_; }
+  std::vector<double> diagonal() const {
+    std::vector<double> d(n_);
+    check(macis_b200_hop_diagonal(op_, d.data(), 0));
+    return d;
+  }
+  void operator_action(size_t m, double alpha, const double* V, size_t LDV,
+                       double beta, double* AV, size_t LDAV) const {
+    check(macis_b200_hop_apply(op_, int64_t(m), alpha, V, int64_t(LDV), beta,
+                               AV, int64_t(LDAV), 0));
+  }
+};
+
 // davidson(N, max_m, op, D, tol, X) for a device operator: the reference
 // signature; D is taken from the matrix. Throws "Davidson Did Not Converge!".
 inline std::pair<int64_t, double> davidson(int64_t, int64_t max_m,

@@ -9,6 +9,7 @@
 #include <spdlog/sinks/null_sink.h>
 #include <spdlog/spdlog.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <fstream>
 #include <macis/asci/grow.hpp>
@@ -57,7 +58,15 @@ int main(int argc, char** argv) {
       dets.begin(), dets.end(), gpu, 1e-16, 15, 1e-8, C2);
   const double e_gpu = macis_b200::selected_ci_diag<64, int32_t>(
       dets.begin(), dets.end(), gpu, 1e-16, 15, 1e-8, C3);
-  // 3. ASCI grow with the shim drivers
+  // 3. the reference's own davidson driving the matrix-free operator
+  macis_b200::MatrixFreeOperator<64> mf(gpu, dets.begin(), dets.end(), 1e-16);
+  const auto D = mf.diagonal();
+  std::vector<double> X4(dets.size(), 0.0);
+  X4[std::min_element(D.begin(), D.end()) - D.begin()] = 1.0;
+  const double e_mf =
+      macis::davidson(int64_t(dets.size()), 15, mf, D.data(), 1e-8, X4.data())
+          .second;
+  // 4. ASCI grow with the shim drivers
   macis::ASCISettings as;
   as.ntdets_max = ntdets;
   macis::MCSCFSettings ms;
@@ -69,9 +78,9 @@ int main(int argc, char** argv) {
   for(double x : X) nrm += x * x;
   std::printf(
       "{\"ndets\": %zu, \"nnz\": %ld, \"csr_equal\": %s, \"e_cpu\": %.15g, "
-      "\"e_hook\": %.15g, \"e_gpu\": %.15g, \"asci_e0\": %.15g, "
-      "\"asci_size\": %zu, \"asci_norm\": %.15g}\n",
+      "\"e_hook\": %.15g, \"e_gpu\": %.15g, \"e_matrix_free\": %.15g, "
+      "\"asci_e0\": %.15g, \"asci_size\": %zu, \"asci_norm\": %.15g}\n",
       dets.size(), long(Hg.nnz()), csr_equal ? "true" : "false", e_cpu,
-      e_hook, e_gpu, E0, w.size(), nrm);
+      e_hook, e_gpu, e_mf, E0, w.size(), nrm);
   return 0;
 }

@@ -30,5 +30,7 @@ def test_reference_templates_with_b200_generator(tmp_path):
     assert r["ndets"] == 12636 and r["csr_equal"]
     assert r["e_cpu"] == r["e_hook"]           # identical CSR -> same Davidson
     assert abs(r["e_gpu"] - r["e_cpu"]) < 1e-8
+    # the reference's davidson on the shim's matrix-free operator
+    assert abs(r["e_matrix_free"] - r["e_cpu"]) < 1e-8
     assert r["asci_size"] == 10000 and abs(r["asci_norm"] - 1) < 1e-10
     assert abs(r["asci_e0"] - K["water_asci_grow_e0"]) < 1e-8
