@@ -232,6 +232,19 @@ int macis_b200_hop_davidson(const macis_b200_hop* op,
                             const macis_b200_davidson_opts* opts, double* X,
                             double* E, int64_t* niter, unsigned flags);
 
+/* One- and two-particle reduced density matrices of the wavefunction C over
+ * dets, added to ordm (norb x norb) and trdm (norb^4; may be NULL for the
+ * 1-RDM alone), column-major like the integrals. Replaces
+ * DoubleLoopHamiltonianGenerator::form_rdms (include/macis/
+ * hamiltonian_generator/double_loop.hpp:117-165) with bra = ket = dets, the
+ * way compute_casci_rdms calls it (include/macis/util/cas.hpp:52-56); the
+ * contributions are those of include/macis/util/rdms.hpp:15-131, dispatched
+ * in the same order. The sums are atomic, so results agree with the
+ * reference to rounding, not bit for bit. */
+int macis_b200_form_rdms(macis_b200_ham* h, const uint64_t* dets,
+                         size_t ndets, const double* C, double* ordm,
+                         double* trdm, unsigned flags);
+
 /* Lowest nwant eigenpairs (W ascending, eigenvectors in the columns of Vec,
  * ld k) of the symmetric k x k matrix whose lower triangle is `lower`
  * (column-major, ld k): the syev step of lobpcgxx::rayleigh_ritz

@@ -118,12 +118,18 @@ class HamiltonianGenerator : public macis::HamiltonianGenerator<N> {
     return DeviceCSR(A);
   }
 
-  void form_rdms(full_det_iterator, full_det_iterator, full_det_iterator,
-                 full_det_iterator, double*, matrix_span_t,
-                 rank4_span_t) override {
-    throw std::logic_error(
-        "form_rdms is not part of the B200 path; use "
-        "macis::DoubleLoopHamiltonianGenerator for RDMs");
+  // form_rdms (double_loop.hpp:117-165) for bra = ket, the way
+  // compute_casci_rdms calls it (cas.hpp:52-56); results are added to the
+  // contiguous column-major spans, trdm may be empty (1-RDM alone).
+  void form_rdms(full_det_iterator bb, full_det_iterator be,
+                 full_det_iterator kb, full_det_iterator ke, double* C,
+                 matrix_span_t ordm, rank4_span_t trdm) override {
+    if(bb != kb || be != ke)
+      throw std::logic_error(
+          "form_rdms on the B200 path takes the same bra and ket range");
+    const size_t n = std::distance(bb, be);
+    check(macis_b200_form_rdms(h_, n ? words<N>(&*bb) : nullptr, n, C,
+                               ordm.data_handle(), trdm.data_handle(), 0));
   }
 
  protected:

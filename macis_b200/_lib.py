@@ -124,6 +124,8 @@ _SIGS = {
     "macis_b200_asci_unit_features": (C.c_int, [_vp, _vp, _sz, C.c_double, _vp,
                                                 _sz, _sz, _vp,
                                                 C.POINTER(_sz)]),
+    "macis_b200_form_rdms": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp,
+                                       C.c_uint]),
     "macis_b200_hop_create": (C.c_int, [_vp, _vp, _sz, C.c_double, C.c_uint,
                                         C.POINTER(_vp)]),
     "macis_b200_hop_destroy": (C.c_int, [_vp]),

@@ -602,3 +602,34 @@ int macis_b200_hop_davidson(const macis_b200_hop* op,
 }
 
 }  // extern "C"
+
+extern "C" int macis_b200_form_rdms(macis_b200_ham* h, const uint64_t* dets,
+                                    size_t ndets, const double* C,
+                                    double* ordm, double* trdm,
+                                    unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(h && ordm && (ndets == 0 || C), MACIS_B200_EINVAL,
+               "null argument");
+    require_dets(dets, ndets, flags);
+    const size_t nw = h->nbits / 64, n = size_t(h->norb);
+    const size_t n2 = n * n, n4 = n2 * n2;
+    cudaStream_t s = h->stream;
+    DevBuf<uint64_t> d(dets, ndets * nw, flags, s);
+    DevBuf<double> c(C, ndets, flags, s);
+    DevBuf<double> o(ordm, n2, flags, s);  // accumulated into, as given
+    DevBuf<double>* t = trdm ? new DevBuf<double>(trdm, n4, flags, s) : nullptr;
+    try {
+      form_rdms_device(h, d.d, ndets, c.d, o.d, t ? t->d : nullptr);
+      if(!(flags & MACIS_B200_DEVICE_PTRS)) {
+        MB_CUDA(cudaMemcpyAsync(ordm, o.d, n2 * 8, cudaMemcpyDeviceToHost, s));
+        if(t)
+          MB_CUDA(cudaMemcpyAsync(trdm, t->d, n4 * 8, cudaMemcpyDeviceToHost, s));
+      }
+      MB_CUDA(cudaStreamSynchronize(s));
+    } catch(...) {
+      delete t;
+      throw;
+    }
+    delete t;
+  });
+}

@@ -2168,3 +2168,164 @@ const double* hop_diag(const macis_b200_hop* op) { return op->diag; }
 cudaStream_t hop_stream(const macis_b200_hop* op) { return op->stream; }
 
 }  // namespace mb
+
+// ------------------------------------------------ 1- and 2-RDMs
+namespace mb {
+
+__device__ __forceinline__ void rdm_add(double* a, size_t i, double v) {
+  atomicAdd(a + i, v);
+}
+
+// Contributions of one (bra, ket) pair: rdm_contributions and its parts
+// (include/macis/util/rdms.hpp:15-131), dispatched in the same order (the
+// two-body branches only when trdm is given). ordm(p,q) = ordm[p + q n],
+// trdm(p,q,r,s) = trdm[p + n (q + n (r + n s))].
+template <int NSW>
+__device__ void rdm_pair(Spin<NSW> ba, Spin<NSW> bb, Spin<NSW> ka,
+                         Spin<NSW> kb, double val, int n, double* ordm,
+                         double* trdm) {
+  const int ca = sp_popc(ba ^ ka), cb = sp_popc(bb ^ kb);
+  if(ca + cb > 4) return;
+  auto t4 = [&](int p, int q, int r, int s, double v) {
+    rdm_add(trdm, size_t(p) + size_t(n) * (q + size_t(n) * (r + size_t(n) * s)),
+            v);
+  };
+  if((ca == 4 || cb == 4) && trdm) {  // rdm_contributions_4, :15-25
+    const uint32_t e = ca == 4 ? double_ex(ba, ka) : double_ex(bb, kb);
+    const int o1 = ex_o1(e), v1 = ex_v1(e), o2 = ex_o2(e), v2 = ex_v2(e);
+    const double v = val * (ex_sgn(e) * 0.5);
+    t4(v1, o1, v2, o2, v);
+    t4(v2, o1, v1, o2, -v);
+    t4(v1, o2, v2, o1, -v);
+    t4(v2, o2, v1, o1, v);
+  } else if(ca == 2 && cb == 2 && trdm) {  // rdm_contributions_22, :27-41
+    const uint32_t ea = single_ex(ba, ka), eb = single_ex(bb, kb);
+    const double v = val * (ex_sgn(ea) * ex_sgn(eb) * 0.5);
+    t4(ex_v1(ea), ex_o1(ea), ex_v1(eb), ex_o1(eb), v);
+    t4(ex_v1(eb), ex_o1(eb), ex_v1(ea), ex_o1(ea), v);
+  } else if(ca == 2 || cb == 2) {  // rdm_contributions_2, :43-66
+    const bool a = ca == 2;
+    const uint32_t e = a ? single_ex(ba, ka) : single_ex(bb, kb);
+    const Spin<NSW> occ_s = a ? ba : bb, occ_o = a ? bb : ba;
+    const int o1 = ex_o1(e), v1 = ex_v1(e);
+    const double sg = ex_sgn(e);
+    rdm_add(ordm, size_t(v1) + size_t(n) * o1, sg * val);
+    if(trdm) {
+      const double v = val * (sg * 0.5);
+      for(Spin<NSW> s = occ_s; sp_popc(s);) {
+        const int p = sp_lowest(s);
+        s = sp_flip(s, p);
+        t4(v1, o1, p, p, v);
+        t4(p, p, v1, o1, v);
+        t4(v1, p, p, o1, -v);
+        t4(p, o1, v1, p, -v);
+      }
+      for(Spin<NSW> s = occ_o; sp_popc(s);) {
+        const int p = sp_lowest(s);
+        s = sp_flip(s, p);
+        t4(v1, o1, p, p, v);
+        t4(p, p, v1, o1, v);
+      }
+    }
+  } else {  // rdm_contributions_diag, :68-99
+    for(Spin<NSW> s = ba; sp_popc(s);) {
+      const int p = sp_lowest(s);
+      s = sp_flip(s, p);
+      rdm_add(ordm, size_t(p) * (n + 1), val);
+    }
+    for(Spin<NSW> s = bb; sp_popc(s);) {
+      const int p = sp_lowest(s);
+      s = sp_flip(s, p);
+      rdm_add(ordm, size_t(p) * (n + 1), val);
+    }
+    if(trdm) {
+      const double v = val * 0.5;
+      for(int spin = 0; spin < 2; ++spin) {
+        const Spin<NSW> o = spin ? bb : ba;
+        for(Spin<NSW> sq = o; sp_popc(sq);) {
+          const int q = sp_lowest(sq);
+          sq = sp_flip(sq, q);
+          for(Spin<NSW> sp = o; sp_popc(sp);) {
+            const int p = sp_lowest(sp);
+            sp = sp_flip(sp, p);
+            t4(p, p, q, q, v);
+            t4(p, q, p, q, -v);
+          }
+        }
+      }
+      for(Spin<NSW> sq = bb; sp_popc(sq);) {
+        const int q = sp_lowest(sq);
+        sq = sp_flip(sq, q);
+        for(Spin<NSW> sp = ba; sp_popc(sp);) {
+          const int p = sp_lowest(sp);
+          sp = sp_flip(sp, p);
+          t4(p, p, q, q, v);
+          t4(q, q, p, p, v);
+        }
+      }
+    }
+  }
+}
+
+// form_rdms (double_loop.hpp:117-165) over one determinant list: every
+// (bra, ket) pair within four spin-orbital differences with |C_i C_j| >
+// 1e-16 adds its contributions. One warp per bra row; the pairs come from
+// the general build's enumeration; sums are atomic (order not fixed).
+template <int NBITS>
+__global__ void __launch_bounds__(HB_THREADS)
+    rdm_k(GenData g, const uint64_t* dets, int64_t n, const double* C,
+          int norb, double* ordm, double* trdm) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  extern __shared__ __align__(16) uint8_t gen_ov[];
+  const int wid = threadIdx.x >> 5;
+  const int64_t nwarp = int64_t(gridDim.x) * HB_WARPS;
+  for(int64_t row = int64_t(blockIdx.x) * HB_WARPS + wid; row < n;
+      row += nwarp) {
+    const int32_t rg = g.rowgroup[row];
+    if(rg < 0) continue;
+    const uint64_t* bd = dets + row * D::NW;
+    const Spin<NSW> ba = D::alpha(bd), bb = D::beta(bd);
+    const double ci = C[row];
+    gen_enumerate<NSW>(g, rg, ba, bb, gen_ov + wid * 256,
+                       [&](bool act, int64_t m, int32_t kg, int, int) {
+      if(!act) return;
+      const double val = ci * C[g.sidx[m]];
+      if(!(fabs(val) > 1e-16)) return;
+      rdm_pair<NSW>(ba, bb, ld_spin<NSW>(g.kalpha, kg),
+                    ld_spin<NSW>(g.sbeta, m), val, norb, ordm, trdm);
+    });
+  }
+}
+
+// ordm (n^2) and trdm (n^4, may be null) are device arrays the results are
+// added to; dets and C device arrays of length n.
+void form_rdms_device(macis_b200_ham* h, const uint64_t* dets, size_t n,
+                      const double* C, double* ordm, double* trdm) {
+  if(n == 0) return;
+  MB_REQUIRE(n < (size_t(1) << 31), MACIS_B200_ECAPACITY,
+             "RDMs need < 2^31 determinants");
+  cudaStream_t s = h->stream;
+  Arena A(s);
+  const unsigned gr = grid_for(n, HB_WARPS, size_t(num_sms()) * 16);
+  constexpr int dyn = HB_WARPS * 256;
+#define MB_RDM(NB)                                                          \
+  {                                                                         \
+    const GenData g = gen_plan<NB>(h, dets, n, dets, n, true, 0, A);        \
+    rdm_k<NB><<<gr, HB_THREADS, dyn, s>>>(g, dets, int64_t(n), C, h->norb,  \
+                                         ordm, trdm),                       \
+        note_launch();                                                      \
+  }
+  if(h->nbits == 64) {
+    MB_RDM(64)
+  } else if(h->nbits == 128) {
+    MB_RDM(128)
+  } else {
+    MB_RDM(256)
+  }
+#undef MB_RDM
+  MB_CUDA(cudaGetLastError());
+  MB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace mb

@@ -133,6 +133,11 @@ int davidson_op(const DavOperator& op, int64_t max_m, double tol,
                 bool use_guess, double* X, double* E, int64_t* niter,
                 int restart_keep, int64_t max_iter);
 
+// 1- and 2-RDM over one determinant list (device arrays; results added to
+// ordm / trdm, trdm may be null).
+void form_rdms_device(macis_b200_ham* h, const uint64_t* dets, size_t n,
+                      const double* C, double* ordm, double* trdm);
+
 // Matrix-free H over one determinant list (hbuild.cu).
 macis_b200_hop* hop_create(macis_b200_ham* h, const uint64_t* dets, size_t n,
                            double thresh, bool mixed, bool device_ptrs);

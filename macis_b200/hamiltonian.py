@@ -93,6 +93,28 @@ class HamiltonianGenerator:
             out.ctypes.data, 0))
         return out if len(out) > 1 else float(out[0])
 
+    # -- form_rdms (double_loop.hpp:117-165, bra = ket = dets)
+    def form_rdms(self, dets, C, two=True):
+        """(ordm, trdm) of the wavefunction C over dets: norb x norb and
+        norb^4 arrays indexed as the reference's spans (column-major);
+        trdm is None when two is False. Contributions and their dispatch
+        follow include/macis/util/rdms.hpp:15-131 (with two=False the
+        reference routes higher excitations into its one-body branches,
+        and so does this); sums are atomic, so values agree with the
+        reference to rounding."""
+        d = _host_dets(dets, self.nbits)
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        if len(C) != len(d):
+            raise RuntimeError("C and dets differ in length")
+        n = self.norb
+        o = np.zeros(n * n)
+        t = np.zeros(n ** 4) if two else None
+        check(LIB.macis_b200_form_rdms(self._h, d.ctypes.data, len(d),
+                                       C.ctypes.data, o.ctypes.data,
+                                       t.ctypes.data if two else None, 0))
+        return (o.reshape(n, n, order="F"),
+                t.reshape(n, n, n, n, order="F") if two else None)
+
     # -- CSR build hook (hamiltonian_generator.hpp:143-156)
     def make_csr_hamiltonian_block(self, bra, ket, H_thresh, index_t=np.int32,
                                    value_t=np.float64):

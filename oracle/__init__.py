@@ -273,6 +273,8 @@ class Ref:
         L.mref_ham_create.restype = C.c_void_p
         L.mref_ham_create.argtypes = [C.c_int, C.c_size_t, _pd, _pd]
         L.mref_ham_free.argtypes = [C.c_void_p]
+        L.mref_form_rdms.argtypes = [C.c_void_p, _p64, C.c_size_t, _pd, _pd,
+                                     C.c_void_p]
         L.mref_matrix_element.argtypes = [C.c_void_p, _p64, _p64, C.c_size_t, _pd]
         L.mref_fast_diag.argtypes = [C.c_void_p, C.c_int, _pu32, C.c_size_t,
                                      _pu32, C.c_size_t, _pu32, C.c_double, _pd]
@@ -324,6 +326,18 @@ class Ref:
         if not h:
             raise RuntimeError(self._err())
         return Handle(h, self.L.mref_ham_free, nbits, norb)
+
+    def form_rdms(self, h, dets, C, two=True):
+        """(1-RDM, 2-RDM or None) of C over dets from the reference's
+        form_rdms, both column-major flattened."""
+        dets = _dets(dets, h.nbits)
+        C = np.ascontiguousarray(C, dtype=np.float64).copy()
+        o = np.zeros(h.norb ** 2)
+        t = np.zeros(h.norb ** 4) if two else None
+        self.L.mref_form_rdms(h.p, _ptr(dets, _p64), len(dets), _ptr(C, _pd),
+                              _ptr(o, _pd),
+                              t.ctypes.data if two else None)
+        return o, t
 
     def matrix_element(self, h, bra, ket):
         bra, ket = _dets(bra, h.nbits), _dets(ket, h.nbits)

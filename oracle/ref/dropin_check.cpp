@@ -10,6 +10,7 @@
 #include <spdlog/spdlog.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <macis/asci/grow.hpp>
@@ -66,7 +67,22 @@ int main(int argc, char** argv) {
   const double e_mf =
       macis::davidson(int64_t(dets.size()), 15, mf, D.data(), 1e-8, X4.data())
           .second;
-  // 4. ASCI grow with the shim drivers
+  // 4. form_rdms through the virtual hook on both generators
+  const size_t m = norb;
+  std::vector<double> o1(m * m, 0.0), t1(m * m * m * m, 0.0), o2(o1), t2(t1);
+  cpu.form_rdms(dets.begin(), dets.end(), dets.begin(), dets.end(), C1.data(),
+                macis::matrix_span<double>(o1.data(), m, m),
+                macis::rank4_span<double>(t1.data(), m, m, m, m));
+  static_cast<macis::HamiltonianGenerator<64>&>(gpu).form_rdms(
+      dets.begin(), dets.end(), dets.begin(), dets.end(), C1.data(),
+      macis::matrix_span<double>(o2.data(), m, m),
+      macis::rank4_span<double>(t2.data(), m, m, m, m));
+  double rdm_diff = 0;
+  for(size_t i = 0; i < o1.size(); ++i)
+    rdm_diff = std::max(rdm_diff, std::abs(o1[i] - o2[i]));
+  for(size_t i = 0; i < t1.size(); ++i)
+    rdm_diff = std::max(rdm_diff, std::abs(t1[i] - t2[i]));
+  // 5. ASCI grow with the shim drivers
   macis::ASCISettings as;
   as.ntdets_max = ntdets;
   macis::MCSCFSettings ms;
@@ -79,8 +95,9 @@ int main(int argc, char** argv) {
   std::printf(
       "{\"ndets\": %zu, \"nnz\": %ld, \"csr_equal\": %s, \"e_cpu\": %.15g, "
       "\"e_hook\": %.15g, \"e_gpu\": %.15g, \"e_matrix_free\": %.15g, "
-      "\"asci_e0\": %.15g, \"asci_size\": %zu, \"asci_norm\": %.15g}\n",
+      "\"rdm_max_diff\": %.3g, \"asci_e0\": %.15g, \"asci_size\": %zu, "
+      "\"asci_norm\": %.15g}\n",
       dets.size(), long(Hg.nnz()), csr_equal ? "true" : "false", e_cpu,
-      e_hook, e_gpu, e_mf, E0, w.size(), nrm);
+      e_hook, e_gpu, e_mf, rdm_diff, E0, w.size(), nrm);
   return 0;
 }

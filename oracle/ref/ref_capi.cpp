@@ -193,6 +193,27 @@ void* mref_ham_create(int nbits, size_t norb, const double* T,
 
 void mref_ham_free(void* h) { delete static_cast<HamBase*>(h); }
 
+// DoubleLoopHamiltonianGenerator::form_rdms (double_loop.hpp:117-165) with
+// bra = ket = dets, the compute_casci_rdms form (cas.hpp:52-56); results are
+// added to ordm (norb^2) and trdm (norb^4, or NULL).
+int mref_form_rdms(void* hv, const uint64_t* dets, size_t n, double* C,
+                   double* ordm, double* trdm) {
+  auto* hb = static_cast<HamBase*>(hv);
+  const size_t m = hb->norb;
+  macis::matrix_span<double> o(ordm, m, m);
+  macis::rank4_span<double> t(trdm, m, m, m, m);
+  if(hb->nbits == 64) {
+    auto D = to_dets<64>(dets, n);
+    static_cast<Ham<64>*>(hb)->gen.form_rdms(D.begin(), D.end(), D.begin(),
+                                             D.end(), C, o, t);
+  } else {
+    auto D = to_dets<128>(dets, n);
+    static_cast<Ham<128>*>(hb)->gen.form_rdms(D.begin(), D.end(), D.begin(),
+                                              D.end(), C, o, t);
+  }
+  return 0;
+}
+
 // Batched matrix_element(bra, ket) (hamiltonian_generator/matrix_elements.hpp:15)
 int mref_matrix_element(void* hv, const uint64_t* bra, const uint64_t* ket,
                         size_t n, double* out) {

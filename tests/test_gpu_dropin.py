@@ -32,5 +32,7 @@ def test_reference_templates_with_b200_generator(tmp_path):
     assert abs(r["e_gpu"] - r["e_cpu"]) < 1e-8
     # the reference's davidson on the shim's matrix-free operator
     assert abs(r["e_matrix_free"] - r["e_cpu"]) < 1e-8
+    # form_rdms through the generator hook, against the reference generator
+    assert r["rdm_max_diff"] < 1e-11
     assert r["asci_size"] == 10000 and abs(r["asci_norm"] - 1) < 1e-10
     assert abs(r["asci_e0"] - K["water_asci_grow_e0"]) < 1e-8
