@@ -279,6 +279,32 @@ int macis_b200_asci_search(macis_b200_ham* h,
                            size_t ndets_max, const uint64_t* cdets,
                            size_t ncdets, double E0, const double* C,
                            uint64_t* out_dets, size_t* nout, unsigned flags);
+/* One part of an exact ASCI search split over part_count processes (one
+ * per GPU; no data is exchanged during the search). The candidate
+ * determinants are divided by a hash of their alpha string into 4096 bins;
+ * every part computes the same contribution histogram over the bins and
+ * takes the bins where its cumulative load crosses part_index / part_count
+ * and (part_index + 1) / part_count of the total. The part's result is its
+ * candidates with their scores, core determinants and zero scores removed,
+ * cut at the (ndets_max - ncdets)-th |score| with every tie kept: the union
+ * over all parts, ordered by |score| descending then by determinant
+ * (bitset order) ascending and cut at ndets_max - ncdets, is exactly the
+ * top-k that macis_b200_asci_search returns for the same inputs (it then
+ * lists it in ascending determinant order, followed by the core dets).
+ * This replaces the reference's MPI search, which splits the work by alpha
+ * constraints and selects the top-k with a distributed quickselect
+ * (include/macis/asci/determinant_search.hpp:145-391,
+ * include/macis/util/dist_quickselect.hpp). *nout receives the number of
+ * candidates; macis_b200_asci_part_results copies them (states: nout x
+ * words, scores: nout) to host memory. */
+int macis_b200_asci_search_part(macis_b200_ham* h,
+                                const macis_b200_asci_settings* s,
+                                size_t ndets_max, const uint64_t* cdets,
+                                size_t ncdets, double E0, const double* C,
+                                uint32_t part_index, uint32_t part_count,
+                                size_t* nout, unsigned flags);
+int macis_b200_asci_part_results(const macis_b200_ham* h, uint64_t* states,
+                                 double* scores);
 /* The accumulated (state, score) pairs before the core merge -- the list the
  * reference top-k works on (determinant_search.hpp:498). Two calls: with
  * states == NULL only *npairs is set. States ascend. */

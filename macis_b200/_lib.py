@@ -126,6 +126,11 @@ _SIGS = {
                                                 C.POINTER(_sz)]),
     "macis_b200_form_rdms": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp,
                                        C.c_uint]),
+    "macis_b200_asci_search_part": (C.c_int, [_vp, C.POINTER(AsciSettingsC),
+                                              _sz, _vp, _sz, C.c_double, _vp,
+                                              C.c_uint32, C.c_uint32,
+                                              C.POINTER(_sz), C.c_uint]),
+    "macis_b200_asci_part_results": (C.c_int, [_vp, _vp, _vp]),
     "macis_b200_hop_create": (C.c_int, [_vp, _vp, _sz, C.c_double, C.c_uint,
                                         C.POINTER(_vp)]),
     "macis_b200_hop_destroy": (C.c_int, [_vp]),

@@ -24,6 +24,7 @@ from ._lib import LIB, check
 from .solvers import FP64, selected_ci_diag
 
 __all__ = ["ASCISettings", "MCSCFSettings", "asci_search", "asci_pairs",
+           "asci_search_part", "merge_asci_parts",
            "asci_iter", "asci_grow", "asci_refine", "reorder_ci_on_coeff",
            "last_search_stats"]
 
@@ -109,6 +110,50 @@ def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen,
              st["raw_pairs"], st["unique_pairs"], st["pairs_ms"] / 1e3,
              st["sort_ms"] / 1e3, st["total_ms"] / 1e3)
     return out[:nout.value]
+
+
+def asci_search_part(asci_settings, ndets_max, cdets, E_ASCI, C, norb,
+                     ham_gen, part_index, part_count):
+    """One part of an exact search split over part_count processes
+    (macis_b200_asci_search_part): (states, scores) of the part's candidates,
+    cut at the (ndets_max - ncdets)-th |score| with every tie kept.
+    merge_asci_parts of all parts gives asci_search's result."""
+    cdets = _dets(cdets, ham_gen.nbits)
+    C = np.ascontiguousarray(C, dtype=np.float64)[:len(cdets)]
+    s = asci_settings.c_struct()
+    n = ct.c_size_t()
+    check(LIB.macis_b200_asci_search_part(
+        ham_gen.handle, ct.byref(s), int(ndets_max), cdets.ctypes.data,
+        len(cdets), float(E_ASCI), C.ctypes.data, int(part_index),
+        int(part_count), ct.byref(n), 0))
+    W = ham_gen.nbits // 64
+    st = np.empty((max(n.value, 1), W), dtype=np.uint64)
+    sc = np.empty(max(n.value, 1))
+    check(LIB.macis_b200_asci_part_results(ham_gen.handle, st.ctypes.data,
+                                           sc.ctypes.data))
+    return st[:n.value], sc[:n.value]
+
+
+def merge_asci_parts(parts, ndets_max, cdets, nbits):
+    """asci_search's result from the parts of a split search: the union of
+    the parts' (states, scores) ordered by |score| descending then by
+    determinant ascending (bitset order, most significant word first), cut
+    at ndets_max - ncdets, listed in ascending determinant order, followed by
+    the core determinants in their input order."""
+    W = nbits // 64
+    cdets = _dets(cdets, nbits)
+    st = [np.asarray(p[0], dtype=np.uint64).reshape(-1, W) for p in parts]
+    sc = [np.asarray(p[1], dtype=np.float64).ravel() for p in parts]
+    st = np.concatenate(st) if st else np.zeros((0, W), dtype=np.uint64)
+    sc = np.concatenate(sc) if sc else np.zeros(0)
+    k = int(ndets_max) - len(cdets)
+    if len(sc) > k:
+        # lexsort: the last key is the primary one
+        order = np.lexsort(tuple(st[:, w] for w in range(W)) + (-np.abs(sc),))
+        st = st[order[:k]]
+    if len(st):
+        st = st[np.lexsort(tuple(st[:, w] for w in range(W)))]
+    return np.concatenate([st, cdets]) if len(cdets) else st
 
 
 def asci_pairs(asci_settings, cdets, E_ASCI, C, ham_gen):

@@ -874,7 +874,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
                       const uint64_t* cdets, size_t ncdets, double E0,
                       const double* C, uint64_t* out_dets, size_t* nout,
                       std::vector<uint64_t>* ps, std::vector<double>* pr,
-                      bool pairs_only) {
+                      bool pairs_only, const AsciPart* part) {
   constexpr int NW = DetTraits<NBITS>::NW;
   cudaStream_t s = h->stream;
   Arena A(s);
@@ -1015,16 +1015,51 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     rns.push_back(ns);
     rsub.push_back(sb);
   };
-  if(Ptot <= cap || pairs_only) {  // pairs_only: the full list is the result
-    add_range(0, ASCI_BINS, 0, 0);
-  } else {
-    std::vector<unsigned long long> hh(ASCI_BINS);
+  // a part of a split search owns the bins [bin_lo, bin_hi): the cuts fall
+  // where the cumulative bin load crosses index / count of the total (the
+  // histogram, hence the cut, is the same on every part)
+  uint32_t bin_lo = 0, bin_hi = ASCI_BINS;
+  std::vector<unsigned long long> hh;
+  auto load_hist = [&] {
+    if(!hh.empty()) return;
+    hh.resize(ASCI_BINS);
     MB_CUDA(cudaMemcpyAsync(hh.data(), dhist, ASCI_BINS * 8,
                             cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
-    uint32_t b0 = 0;
+  };
+  uint64_t Ppart = uint64_t(Ptot);
+  if(part && part->count > 1) {
+    load_hist();
+    auto cut = [&](uint32_t r) -> uint32_t {
+      if(r == 0) return 0;
+      if(r >= part->count) return ASCI_BINS;
+      // first bin whose preceding load reaches r / count of the total
+      const long double want =
+          (long double)Ptot * (long double)r / (long double)part->count;
+      unsigned long long c = 0;
+      for(uint32_t b = 0; b < ASCI_BINS; ++b) {
+        if((long double)c >= want) return b;
+        c += hh[b];
+      }
+      return ASCI_BINS;
+    };
+    bin_lo = cut(part->index);
+    bin_hi = std::max(bin_lo, cut(part->index + 1));
+    Ppart = 0;
+    for(uint32_t b = bin_lo; b < bin_hi; ++b) Ppart += hh[b];
+  }
+  if(bin_lo == bin_hi) {
+    // this part owns no bins: nothing to search
+  } else if((Ppart <= uint64_t(cap) || pairs_only) && bin_lo == 0 &&
+            bin_hi == ASCI_BINS) {  // pairs_only: the full list is the result
+    add_range(0, ASCI_BINS, 0, 0);
+  } else if(Ppart <= uint64_t(cap)) {
+    add_range(bin_lo, bin_hi, 0, 0);
+  } else {
+    load_hist();
+    uint32_t b0 = bin_lo;
     unsigned long long acc = 0;
-    for(uint32_t b = 0; b < ASCI_BINS; ++b) {
+    for(uint32_t b = bin_lo; b < bin_hi; ++b) {
       if(hh[b] > uint64_t(cap)) {
         if(acc) add_range(b0, b, 0, 0);
         const uint32_t ns = uint32_t(std::ceil(1.25 * double(hh[b]) / double(cap)));
@@ -1040,7 +1075,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       }
       acc += hh[b];
     }
-    if(b0 < ASCI_BINS) add_range(b0, ASCI_BINS, 0, 0);
+    if(b0 < bin_hi) add_range(b0, bin_hi, 0, 0);
   }
   const uint32_t nr = uint32_t(rlo.size());
   stats.batches = nr;
@@ -1106,7 +1141,9 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     int64_t* rc = ucnt;
     int64_t* off = uout;
     int64_t P = Ptot;
-    if(nr > 1) {
+    // the first count pass covered every bin: a range that does not (one of
+    // several, or the share of a split search) is counted on its own
+    if(nr > 1 || rlo[rr] != 0 || rhi[rr] != ASCI_BINS) {
       rc = B.get<int64_t>(U + 1);
       off = B.get<int64_t>(U + 1);
       units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
@@ -1272,6 +1309,22 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     h->last_asci = stats;
     return;
   }
+  if(part) {
+    // the part's running top-k, ties at its cut included: the union over
+    // the parts holds the whole search's top-k
+    h->part_states.resize(surv.n * NW);
+    h->part_scores.resize(surv.n);
+    if(surv.n) {
+      MB_CUDA(cudaMemcpyAsync(h->part_states.data(), surv.keys,
+                              surv.n * NW * 8, cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaMemcpyAsync(h->part_scores.data(), surv.rv, surv.n * 8,
+                              cudaMemcpyDeviceToHost, s));
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    stats.total_ms = ms_since(t_all);
+    h->last_asci = stats;
+    return;
+  }
 
   // ------------------------------------------------------------- top-k
   // Ties at the topk-th score go to the smaller determinants
@@ -1334,17 +1387,17 @@ void asci_search_device(macis_b200_ham* h, const macis_b200_asci_settings& s,
                         const uint64_t* cdets, size_t ncdets, double E0,
                         const double* C, uint64_t* out_dets, size_t* nout,
                         std::vector<uint64_t>* ps, std::vector<double>* pr,
-                        bool pairs_only) {
+                        bool pairs_only, const AsciPart* part) {
   MB_REQUIRE(h->norb <= MAXORB, MACIS_B200_EINVAL, "norb too large for ASCI");
   if(h->nbits == 64)
     asci_impl<64>(h, s, scr, ndets_max, cdets, ncdets, E0, C, out_dets, nout,
-                  ps, pr, pairs_only);
+                  ps, pr, pairs_only, part);
   else if(h->nbits == 128)
     asci_impl<128>(h, s, scr, ndets_max, cdets, ncdets, E0, C, out_dets, nout,
-                   ps, pr, pairs_only);
+                   ps, pr, pairs_only, part);
   else
     asci_impl<256>(h, s, scr, ndets_max, cdets, ncdets, E0, C, out_dets, nout,
-                   ps, pr, pairs_only);
+                   ps, pr, pairs_only, part);
 }
 
 template <int NBITS>

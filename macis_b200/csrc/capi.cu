@@ -633,3 +633,38 @@ extern "C" int macis_b200_form_rdms(macis_b200_ham* h, const uint64_t* dets,
     delete t;
   });
 }
+
+extern "C" int macis_b200_asci_search_part(
+    macis_b200_ham* h, const macis_b200_asci_settings* s, size_t ndets_max,
+    const uint64_t* cdets, size_t ncdets, double E0, const double* C,
+    uint32_t part_index, uint32_t part_count, size_t* nout, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(h && s && nout, MACIS_B200_EINVAL, "null argument");
+    MB_REQUIRE(part_count >= 1 && part_index < part_count, MACIS_B200_EINVAL,
+               "part_index must be in [0, part_count)");
+    require_dets(cdets, ncdets, flags);
+    const size_t nw = h->nbits / 64;
+    DevBuf<uint64_t> cd(cdets, ncdets * nw, flags, h->stream);
+    DevBuf<double> cc(C, ncdets, flags, h->stream);
+    AsciPart part;
+    part.index = part_index;
+    part.count = part_count;
+    size_t dummy = 0;
+    h->part_states.clear();
+    h->part_scores.clear();
+    asci_search_device(h, *s, nullptr, ndets_max, cd.d, ncdets, E0, cc.d,
+                       nullptr, &dummy, nullptr, nullptr, false, &part);
+    *nout = h->part_scores.size();
+  });
+}
+
+extern "C" int macis_b200_asci_part_results(const macis_b200_ham* h,
+                                            uint64_t* states, double* scores) {
+  return guarded([&] {
+    MB_REQUIRE(h && states && scores, MACIS_B200_EINVAL, "null argument");
+    if(!h->part_scores.empty()) {
+      std::memcpy(states, h->part_states.data(), h->part_states.size() * 8);
+      std::memcpy(scores, h->part_scores.data(), h->part_scores.size() * 8);
+    }
+  });
+}

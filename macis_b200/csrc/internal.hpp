@@ -26,6 +26,9 @@ struct macis_b200_ham {
   // first use by the screened search
   double* pairmax = nullptr;
   macis_b200_asci_stats last_asci{};
+  // result of the last macis_b200_asci_search_part (candidates, scores)
+  std::vector<uint64_t> part_states;
+  std::vector<double> part_scores;
   mb::Ints ints() const {
     return mb::Ints{norb, T, V, G, G_red, V_red, G2_red, V2_red};
   }
@@ -154,12 +157,18 @@ void small_syev_lowest(int k, const double* lower, int nwant, double* W,
 
 // ASCI search on device-resident core dets (see macis_b200_asci_search).
 // scr may be null (exact search, nothing recorded).
+// One part of a search split over `count` parts (index in [0, count)): the
+// part's candidates and scores go to h->part_states / part_scores.
+struct AsciPart {
+  uint32_t index = 0, count = 1;
+};
 void asci_search_device(macis_b200_ham* h, const macis_b200_asci_settings& s,
                         const macis_b200_asci_screen* scr, size_t ndets_max,
                         const uint64_t* cdets, size_t ncdets, double E0,
                         const double* C, uint64_t* out_dets, size_t* nout,
                         std::vector<uint64_t>* pairs_states,
-                        std::vector<double>* pairs_rv, bool pairs_only);
+                        std::vector<double>* pairs_rv, bool pairs_only,
+                        const AsciPart* part = nullptr);
 // Network input rows of units [first, first + n) of the search over the core
 // dets (device X [n][din]); returns the unit count.
 int64_t asci_unit_features_device(macis_b200_ham* h, const uint64_t* cdets,

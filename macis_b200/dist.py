@@ -28,7 +28,8 @@ from ._lib import LIB, check
 __all__ = ["rank_world", "local_rows", "reduce_max", "reduce_sum",
            "allgather_rows", "DistCSR", "make_dist_csr_hamiltonian",
            "RowBlockOperator", "p_gram_schmidt", "p_rayleigh_ritz",
-           "p_davidson", "gather_row_blocks"]
+           "p_davidson", "gather_row_blocks", "merge_search_parts",
+           "asci_search"]
 
 
 def _dist():
@@ -286,3 +287,33 @@ def gather_row_blocks(rowptr, colind, nzval, dst=0, group=None):
         cis.append(ci)
         nzs.append(nz)
     return np.concatenate(rps), np.concatenate(cis), np.concatenate(nzs)
+
+
+def merge_search_parts(part, ndets_max, cdets, nbits, group=None):
+    """All-gather every rank's (states, scores) part of a split ASCI search
+    and merge them (asci.merge_asci_parts) into the whole search's result,
+    the same on every rank."""
+    from .asci import merge_asci_parts
+    r, w = rank_world(group)
+    if w == 1:
+        parts = [part]
+    else:
+        parts = [None] * w
+        _dist().all_gather_object(parts, (np.asarray(part[0]),
+                                          np.asarray(part[1])), group=group)
+    return merge_asci_parts(parts, ndets_max, cdets, nbits)
+
+
+def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen,
+                group=None):
+    """Exact ASCI search split over the ranks of `group`, one GPU each: rank
+    r searches part r of world (asci.asci_search_part: its share of the
+    alpha-string hash bins, cut by the contribution histogram every rank
+    computes alike), then the parts are gathered and merged. The result is
+    asci_search's on one GPU, on every rank (the reference's MPI search,
+    determinant_search.hpp:145-391, splits by alpha constraints instead)."""
+    from .asci import asci_search_part
+    r, w = rank_world(group)
+    part = asci_search_part(asci_settings, ndets_max, cdets, E_ASCI, C, norb,
+                            ham_gen, r, w)
+    return merge_search_parts(part, ndets_max, cdets, ham_gen.nbits, group)

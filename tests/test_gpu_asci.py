@@ -165,3 +165,29 @@ def test_water_grow_refine_golden():
     E, dets, X = mb.asci_refine(s, ci, E, dets, X, H, norb)
     assert len(dets) == 10000
     assert abs(E - K["water_asci_refine_e0"]) < 1e-7
+
+
+@pytest.mark.parametrize("nparts", [1, 2, 4])
+def test_split_search_merges_to_whole(port, wcase, monkeypatch, nparts):
+    """A search split into parts by the alpha-string bins (one process per
+    GPU in a distributed run; run one after another here) merges to the
+    whole search's result exactly -- with one range per part, with several
+    (small range cap), and with a small top-k whose ties are resolved only in
+    the merge."""
+    norb, T, V, hp, cd, cc, E = wcase
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+
+    def split(ndets_max):
+        parts = [mb.asci_search_part(_settings(), ndets_max, cd, E, cc, norb,
+                                     H, i, nparts) for i in range(nparts)]
+        assert sum(len(p[1]) for p in parts) > 0
+        return mb.merge_asci_parts(parts, ndets_max, cd, 64)
+
+    for ndets_max in (5000, len(cd) + 7):
+        whole = mb.asci_search(_settings(), ndets_max, cd, E, cc, norb, H)
+        assert np.array_equal(split(ndets_max), whole)
+    monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", "50000")
+    got = split(5000)
+    assert mb.last_search_stats(H)["batches"] >= 1
+    exp = port.asci_search(hp, oracle.AsciSettings.default(), 5000, cd, E, cc)
+    assert np.array_equal(got, exp)

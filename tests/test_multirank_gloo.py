@@ -40,6 +40,34 @@ def _block_op(port, hp, dets, lo, hi):
     return (rp, ci, nz), mv
 
 
+def _asci_parts(port, world=WORLD, ndets_max=300):
+    """Parts of a split ASCI search built from the oracle's accumulated
+    pairs: core dets and zero scores removed, a disjoint split by a hash of
+    the determinant, each part cut at its (ndets_max - ncore)-th |score|
+    with every tie kept. Returns [(states, scores, core, ndets_max)]."""
+    import oracle
+    T, V, d = fci(7, 3, 3, 64, seed=6)
+    core = d[:40]
+    C = np.random.default_rng(2).standard_normal(len(core))
+    C /= np.linalg.norm(C)
+    hp = port.ham(64, 7, T, V)
+    E0 = float(port.matrix_element(hp, core[:1], core[:1])[0]) - 0.5
+    st, rv = port.asci_pairs(hp, oracle.AsciSettings.default(), core, E0, C)
+    keep = (rv != 0) & ~np.isin(st[:, 0], core[:, 0])
+    st, rv = st[keep], rv[keep]
+    k = ndets_max - len(core)
+    out = []
+    for r in range(world):
+        m = (st[:, 0] * np.uint64(0x9E3779B97F4A7C15) >> np.uint64(61)) % \
+            np.uint64(world) == np.uint64(r)
+        ps, pr = st[m], rv[m]
+        if len(pr) > k:
+            cut = np.sort(np.abs(pr))[::-1][k - 1]
+            ps, pr = ps[np.abs(pr) >= cut], pr[np.abs(pr) >= cut]
+        out.append((ps, pr, core, ndets_max))
+    return out, (st, rv)
+
+
 def _rank_main(rank, port_no, case, q):
     import datetime
 
@@ -81,6 +109,11 @@ def _rank_main(rank, port_no, case, q):
                                   1e-8, X)
             out.update(it=it, E=E, X=md.allgather_rows(X, N).numpy(),
                        guess=g)
+        elif case == "asci":
+            parts_in, _ = _asci_parts(port)
+            states, scores, core, ndets_max = parts_in[rank]
+            out["merged"] = md.merge_search_parts((states, scores), ndets_max,
+                                                  core, 64)
         dist.barrier()
         dist.destroy_process_group()
         q.put(out)
@@ -169,3 +202,16 @@ def test_p_davidson_single_rank_no_group(port):
     with pytest.raises(RuntimeError, match="Did Not Converge"):
         md.p_davidson(N, 3, md.RowBlockOperator(mv, N), torch.from_numpy(D),
                       1e-14, torch.from_numpy(X0.copy()))
+
+
+def test_split_asci_search_merge_two_ranks(port):
+    """merge_search_parts over two gloo ranks returns, on both, the merge of
+    the whole candidate list (the result of the unsplit search)."""
+    from macis_b200.asci import merge_asci_parts
+    res = _run("asci")
+    parts, (st, rv) = _asci_parts(port)
+    _, _, core, ndets_max = parts[0]
+    whole = merge_asci_parts([(st, rv)], ndets_max, core, 64)
+    assert len(whole) == ndets_max
+    for r in range(WORLD):
+        assert np.array_equal(res[r]["merged"], whole)
