@@ -20,6 +20,8 @@
         # the same on n = 64, 16a/16b, bitset<128>; learned_mixed also runs
         # one exact search from its last core set and reports the top-k
         # recall of the screened one
+    python -m macis_b200.profile_cases c5 --ntdets 51200 --refine 1
+        # n = 100, 20a/20b, bitset<256>, exact search, FP64 Davidson
 
 Each case runs its hot call a few times (--reps) and prints one timing line.
 """
@@ -142,14 +144,14 @@ def screen_n48(reps, ncore=10000):
         print(r)
 
 
-def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12):
+def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128):
     """One C3-shaped ASCI run (C4 with n = 64, k = 16); prints one JSON line
     with the per-iteration log, the final energy and the wall time."""
     import json
     import logging
     logging.basicConfig(level=logging.INFO, format="%(name)s %(message)s")
     T, V = mb.synthetic_integrals(n, seed)
-    H = mb.HamiltonianGenerator(T, V, 128)
+    H = mb.HamiltonianGenerator(T, V, nbits)
     s = mb.ASCISettings(ntdets_max=int(ntdets), ntdets_min=100,
                         ncdets_max=int(ncore), grow_factor=8, h_el_tol=1e-8,
                         max_refine_iter=int(refine))
@@ -158,8 +160,9 @@ def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12):
                          precision=mb.MIXED if mode == "learned_mixed" else mb.FP64)
     scr = None
     if mode == "learned_mixed":
-        scr = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=128, seed=seed))
-    hf = mb.canonical_hf_determinant(k, k, 128)
+        scr = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=nbits,
+                                                             seed=seed))
+    hf = mb.canonical_hf_determinant(k, k, nbits)
     E0 = float(H.matrix_element(hf, hf))
     t0 = time.perf_counter()
     E, dets, X = mb.asci_grow(s, m, E0, hf, [1.0], H, n, screen=scr)
@@ -219,6 +222,7 @@ def main():
     ap.add_argument("--ntdets", type=float, default=1e6)
     ap.add_argument("--mode", default="fp64")
     ap.add_argument("--ncore", type=int, default=10000)
+    ap.add_argument("--refine", type=int, default=3)
     a = ap.parse_args()
     if a.case == "hbuild_c1":
         hbuild(10, 5, a.reps)
@@ -246,6 +250,10 @@ def main():
         c3(a.ntdets, a.mode)
     elif a.case == "c4":
         c3(a.ntdets, a.mode, n=64, k=16)
+    elif a.case == "c5":
+        # n = 100, 20a/20b, bitset<256>: exact search only (the network
+        # input of 256-bit dets is wider than the network takes)
+        c3(a.ntdets, "fp64", refine=a.refine, n=100, k=20, nbits=256)
     else:
         raise SystemExit(f"unknown case {a.case}")
 
