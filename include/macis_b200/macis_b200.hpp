@@ -14,7 +14,8 @@
 //   macis_b200::asci_search / asci_iter / asci_grow / asci_refine
 //       include/macis/asci/{determinant_search.hpp:395,iteration.hpp:17,
 //       grow.hpp:17,refine.hpp:15}; the reference drivers call asci_search
-//       and selected_ci_diag directly, so same-signature drivers are shipped
+//       and selected_ci_diag directly, so same-signature drivers are shipped;
+//       a trailing ScreenSettings* adds the learned screening of the search
 //
 // Link with libmacis_b200.so (C ABI in macis_b200.h). MPI world size 1.
 #pragma once
@@ -281,13 +282,118 @@ std::vector<macis::wfn_t<N>> asci_search(
   return out;
 }
 
-// asci_iter (include/macis/asci/iteration.hpp:17-68)
+// Learned screening of the ASCI search (no MACIS counterpart). A search
+// "unit" is one core determinant with one excitation class and, for
+// doubles, one outer (occupied, virtual) pair; the network predicts each
+// unit's largest log |score|, and a screened search scores exactly only the
+// top keep_frac of the units (plus a random explore_frac).
+class ScreeningNetwork {
+  macis_b200_mlp* m_ = nullptr;
+  size_t trained_steps_ = 0;
+
+ public:
+  explicit ScreeningNetwork(int nbits, uint64_t seed = 0) {
+    check(macis_b200_mlp_create(macis_b200_asci_unit_width(nbits), seed, &m_));
+  }
+  ScreeningNetwork(const ScreeningNetwork&) = delete;
+  ScreeningNetwork& operator=(const ScreeningNetwork&) = delete;
+  ~ScreeningNetwork() {
+    if(m_) macis_b200_mlp_destroy(m_);
+  }
+  macis_b200_mlp* handle() const { return m_; }
+  size_t trained_steps() const { return trained_steps_; }
+  // Adam over the samples the last recording search stored; returns the
+  // mean loss of the last epoch.
+  double train_on_samples(int epochs, int batch, double lr, uint64_t seed) {
+    double loss = 0;
+    check(macis_b200_mlp_train(m_, nullptr, nullptr, 0, epochs, batch, lr,
+                               seed, &loss, 0));
+    ++trained_steps_;
+    return loss;
+  }
+  // Raise the stored targets below their q-quantile to that value.
+  float clamp_samples(double q) {
+    float f = 0;
+    check(macis_b200_mlp_clamp_samples(m_, q, &f));
+    return f;
+  }
+};
+
+// How the ASCI drivers use a ScreeningNetwork: every search records
+// samples of the units it scores and the network is retrained after it;
+// searches after the first warmup_searches, with at least min_units units,
+// prune by prediction.
+struct ScreenSettings {
+  ScreeningNetwork* network = nullptr;
+  double keep_frac = 0.2;
+  double explore_frac = 0.02;
+  uint64_t max_samples = 1000000;  // samples recorded per search
+  int epochs = 2;
+  double lr = 1e-3;
+  int batch = 1024;
+  double clamp_quantile = 0.6;  // 0: no clamping
+  uint64_t min_units = 20000;
+  uint64_t warmup_searches = 1;
+  bool train = true;
+  uint64_t seed = 0;
+  uint64_t searches = 0;  // searches run so far (updated)
+
+  bool prune_next() const {
+    return network && network->trained_steps() > 0 &&
+           searches >= warmup_searches;
+  }
+  macis_b200_asci_screen to_c(bool use_net) const {
+    macis_b200_asci_screen c{};
+    c.net = network ? network->handle() : nullptr;
+    c.use_net = use_net;
+    c.keep_frac = keep_frac;
+    c.explore_frac = explore_frac;
+    c.max_samples = train ? max_samples : 0;
+    c.seed = seed + 7919 * searches;
+    return c;
+  }
+};
+
+// asci_search with learned screening (use_net: prune by prediction).
+template <size_t N>
+std::vector<macis::wfn_t<N>> asci_search(
+    macis::ASCISettings asci_settings, size_t ndets_max,
+    macis::wavefunction_iterator_t<N> cdets_begin,
+    macis::wavefunction_iterator_t<N> cdets_end, const double E_ASCI,
+    const std::vector<double>& C, HamiltonianGenerator<N>& ham_gen,
+    ScreenSettings& screen, bool use_net) {
+  if(!screen.network) throw std::logic_error("ScreenSettings without network");
+  const size_t nc = std::distance(cdets_begin, cdets_end);
+  const auto s = to_c(asci_settings);
+  const auto sc = screen.to_c(use_net);
+  std::vector<macis::wfn_t<N>> out(ndets_max + nc);
+  size_t nout = 0;
+  check(macis_b200_asci_search_screened(
+      ham_gen.handle(), &s, &sc, ndets_max,
+      nc ? words<N>(&*cdets_begin) : nullptr, nc, E_ASCI, C.data(),
+      reinterpret_cast<uint64_t*>(out.data()), &nout, 0));
+  ++screen.searches;
+  out.resize(nout);
+  return out;
+}
+
+// Statistics of the last search on a generator.
+template <size_t N>
+macis_b200_asci_stats last_search_stats(const HamiltonianGenerator<N>& h) {
+  macis_b200_asci_stats st{};
+  check(macis_b200_asci_last_stats(h.handle(), &st));
+  return st;
+}
+
+// asci_iter (include/macis/asci/iteration.hpp:17-68). With a screen whose
+// network is set, the search records samples / prunes units and the network
+// is retrained on the recorded samples before the diagonalisation.
 template <size_t N, typename index_t = int32_t>
 auto asci_iter(macis::ASCISettings asci_settings,
                macis::MCSCFSettings mcscf_settings, size_t ndets_max,
                double E0, std::vector<macis::wfn_t<N>> wfn,
                std::vector<double> X, HamiltonianGenerator<N>& ham_gen,
-               size_t norb) {
+               size_t norb, ScreenSettings* screen = nullptr) {
   if(wfn.size() > 1) {  // reorder_ci_on_coeff, ties kept in order
     std::vector<size_t> idx(X.size());
     std::iota(idx.begin(), idx.end(), 0);
@@ -304,9 +410,30 @@ auto asci_iter(macis::ASCISettings asci_settings,
     X = std::move(x2);
   }
   const size_t nkeep = std::min(asci_settings.ncdets_max, wfn.size());
-  wfn = asci_search<N>(asci_settings, ndets_max, wfn.begin(),
-                       wfn.begin() + nkeep, E0, X, norb, nullptr, nullptr,
-                       nullptr, nullptr, nullptr, ham_gen);
+  if(screen && screen->network) {
+    bool use_net = screen->prune_next();
+    if(use_net && screen->min_units) {  // small searches run exact
+      size_t nunits = 0;
+      check(macis_b200_asci_unit_features(ham_gen.handle(), words<N>(&wfn[0]),
+                                          nkeep, E0, X.data(), 0, 0, nullptr,
+                                          &nunits));
+      use_net = nunits >= screen->min_units;
+    }
+    wfn = asci_search<N>(asci_settings, ndets_max, wfn.begin(),
+                         wfn.begin() + nkeep, E0, X, ham_gen, *screen,
+                         use_net);
+    if(screen->train && last_search_stats(ham_gen).samples > 0) {
+      if(screen->clamp_quantile > 0)
+        screen->network->clamp_samples(screen->clamp_quantile);
+      screen->network->train_on_samples(screen->epochs, screen->batch,
+                                        screen->lr,
+                                        screen->seed + screen->searches);
+    }
+  } else {
+    wfn = asci_search<N>(asci_settings, ndets_max, wfn.begin(),
+                         wfn.begin() + nkeep, E0, X, norb, nullptr, nullptr,
+                         nullptr, nullptr, nullptr, ham_gen);
+  }
   std::vector<double> X_local;
   const double E = selected_ci_diag<N, index_t>(
       wfn.begin(), wfn.end(), ham_gen, mcscf_settings.ci_matel_tol,
@@ -319,7 +446,8 @@ template <size_t N, typename index_t = int32_t>
 auto asci_grow(macis::ASCISettings asci_settings,
                macis::MCSCFSettings mcscf_settings, double E0,
                std::vector<macis::wfn_t<N>> wfn, std::vector<double> X,
-               HamiltonianGenerator<N>& ham_gen, size_t norb) {
+               HamiltonianGenerator<N>& ham_gen, size_t norb,
+               ScreenSettings* screen = nullptr) {
   if(asci_settings.grow_with_rot)
     throw std::logic_error("grow_with_rot is not part of the B200 path");
   while(wfn.size() < asci_settings.ntdets_max) {
@@ -330,7 +458,7 @@ auto asci_grow(macis::ASCISettings asci_settings,
     double E;
     std::tie(E, wfn, X) = asci_iter<N, index_t>(
         asci_settings, mcscf_settings, ndets_new, E0, std::move(wfn),
-        std::move(X), ham_gen, norb);
+        std::move(X), ham_gen, norb, screen);
     if(ndets_new > wfn.size())
       throw std::runtime_error("Wavefunction didn't grow enough...");
     E0 = E;
@@ -343,13 +471,15 @@ template <size_t N, typename index_t = int32_t>
 auto asci_refine(macis::ASCISettings asci_settings,
                  macis::MCSCFSettings mcscf_settings, double E0,
                  std::vector<macis::wfn_t<N>> wfn, std::vector<double> X,
-                 HamiltonianGenerator<N>& ham_gen, size_t norb) {
+                 HamiltonianGenerator<N>& ham_gen, size_t norb,
+                 ScreenSettings* screen = nullptr) {
   const size_t ndets = wfn.size();
   for(size_t iter = 0; iter < asci_settings.max_refine_iter; ++iter) {
     double E;
     std::tie(E, wfn, X) =
         asci_iter<N, index_t>(asci_settings, mcscf_settings, ndets, E0,
-                              std::move(wfn), std::move(X), ham_gen, norb);
+                              std::move(wfn), std::move(X), ham_gen, norb,
+                              screen);
     if(wfn.size() != ndets)
       throw std::runtime_error("Wavefunction size can't change in refinement");
     const double dE = E - E0;

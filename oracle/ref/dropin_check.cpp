@@ -92,12 +92,42 @@ int main(int argc, char** argv) {
   std::tie(E0, w, X) = macis_b200::asci_grow<64>(as, ms, E0, w, X, gpu, norb);
   double nrm = 0;
   for(double x : X) nrm += x * x;
+  // 6. the same grow with learned screening: (a) recording and training
+  //    only, which must not change the searches; (b) pruning by prediction
+  //    from the third search on
+  auto screened_grow = [&](macis_b200::ScreenSettings& sc) {
+    std::vector<macis::wfn_t<64>> ws = {hf};
+    std::vector<double> Xs = {1.0};
+    double Es = gpu.matrix_element(hf, hf);
+    std::tie(Es, ws, Xs) =
+        macis_b200::asci_grow<64>(as, ms, Es, ws, Xs, gpu, norb, &sc);
+    return std::make_pair(Es, ws.size());
+  };
+  macis_b200::ScreeningNetwork net_rec(64, 0), net_scr(64, 0);
+  macis_b200::ScreenSettings rec;
+  rec.network = &net_rec;
+  rec.warmup_searches = size_t(-1);
+  const auto [e_rec, n_rec] = screened_grow(rec);
+  macis_b200::ScreenSettings scr;
+  scr.network = &net_scr;
+  scr.keep_frac = 0.5;
+  scr.epochs = 8;
+  scr.min_units = 0;
+  scr.warmup_searches = 2;
+  const auto [e_scr, n_scr] = screened_grow(scr);
+  const auto st = macis_b200::last_search_stats(gpu);
   std::printf(
       "{\"ndets\": %zu, \"nnz\": %ld, \"csr_equal\": %s, \"e_cpu\": %.15g, "
       "\"e_hook\": %.15g, \"e_gpu\": %.15g, \"e_matrix_free\": %.15g, "
       "\"rdm_max_diff\": %.3g, \"asci_e0\": %.15g, \"asci_size\": %zu, "
-      "\"asci_norm\": %.15g}\n",
+      "\"asci_norm\": %.15g, \"rec_e0\": %.15g, \"rec_size\": %zu, "
+      "\"rec_trained\": %zu, \"rec_searches\": %zu, \"scr_e0\": %.15g, "
+      "\"scr_size\": %zu, \"scr_trained\": %zu, \"scr_units_kept\": %llu, "
+      "\"scr_units_total\": %llu}\n",
       dets.size(), long(Hg.nnz()), csr_equal ? "true" : "false", e_cpu,
-      e_hook, e_gpu, e_mf, rdm_diff, E0, w.size(), nrm);
+      e_hook, e_gpu, e_mf, rdm_diff, E0, w.size(), nrm, e_rec, n_rec,
+      net_rec.trained_steps(), size_t(rec.searches), e_scr, n_scr,
+      net_scr.trained_steps(), (unsigned long long)st.units_kept,
+      (unsigned long long)st.units_total);
   return 0;
 }

@@ -36,3 +36,13 @@ def test_reference_templates_with_b200_generator(tmp_path):
     assert r["rdm_max_diff"] < 1e-11
     assert r["asci_size"] == 10000 and abs(r["asci_norm"] - 1) < 1e-10
     assert abs(r["asci_e0"] - K["water_asci_grow_e0"]) < 1e-8
+    # the shim's screened drivers: recording + training leaves every search
+    # as it was; pruning (searches 3 and 4, half the units) still grows the
+    # same state -- the network's accuracy is tested in test_gpu_screening
+    print(f"\nshim screened grow: dE {r['scr_e0'] - r['asci_e0']:.3e} Eh, "
+          f"units {r['scr_units_kept']}/{r['scr_units_total']}")
+    assert r["rec_size"] == 10000 and r["rec_searches"] == 4
+    assert r["rec_trained"] == 4 and abs(r["rec_e0"] - r["asci_e0"]) < 1e-8
+    assert r["scr_size"] == 10000 and r["scr_trained"] == 4
+    assert 0 < r["scr_units_kept"] <= 0.52 * r["scr_units_total"] + 2
+    assert abs(r["scr_e0"] - r["asci_e0"]) < 1e-3   # measured 1.1e-4
