@@ -305,6 +305,23 @@ int macis_b200_asci_search_part(macis_b200_ham* h,
                                 size_t* nout, unsigned flags);
 int macis_b200_asci_part_results(const macis_b200_ham* h, uint64_t* states,
                                  double* scores);
+/* macis_b200_asci_search_part with learned screening / sample recording
+ * (scr as in macis_b200_asci_search_screened; may be NULL). The network
+ * runs over all units on every part, so parts holding equal networks keep
+ * the same units and their union is the screened whole search. A recording
+ * part stores the same sample rows as the whole search, each target taken
+ * over the part's bins only: the elementwise maximum of the parts' targets
+ * (macis_b200_mlp_samples, then macis_b200_mlp_set_sample_targets) is the
+ * whole search's. */
+int macis_b200_asci_search_part_screened(macis_b200_ham* h,
+                                         const macis_b200_asci_settings* s,
+                                         const macis_b200_asci_screen* scr,
+                                         size_t ndets_max,
+                                         const uint64_t* cdets, size_t ncdets,
+                                         double E0, const double* C,
+                                         uint32_t part_index,
+                                         uint32_t part_count, size_t* nout,
+                                         unsigned flags);
 /* The accumulated (state, score) pairs before the core merge -- the list the
  * reference top-k works on (determinant_search.hpp:498). Two calls: with
  * states == NULL only *npairs is set. States ascend. */
@@ -344,6 +361,10 @@ int macis_b200_mlp_train(macis_b200_mlp* m, const uint16_t* X, const float* t,
  * ranking below it does not matter to a search that keeps the top units);
  * *floor = the value (may be NULL). */
 int macis_b200_mlp_clamp_samples(macis_b200_mlp* m, double q, float* floor);
+/* Overwrite the targets of the n recorded samples (n must equal their
+ * count), e.g. with the maximum over the parts of a split search. */
+int macis_b200_mlp_set_sample_targets(macis_b200_mlp* m, const float* t,
+                                      size_t n);
 /* Recorded samples (host copies; X may be NULL to query *n). */
 int macis_b200_mlp_samples(const macis_b200_mlp* m, size_t* n, uint16_t* X,
                            float* t);

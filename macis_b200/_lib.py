@@ -131,6 +131,10 @@ _SIGS = {
                                               C.c_uint32, C.c_uint32,
                                               C.POINTER(_sz), C.c_uint]),
     "macis_b200_asci_part_results": (C.c_int, [_vp, _vp, _vp]),
+    "macis_b200_asci_search_part_screened": (C.c_int, [
+        _vp, C.POINTER(AsciSettingsC), C.POINTER(AsciScreenC), _sz, _vp, _sz,
+        C.c_double, _vp, C.c_uint32, C.c_uint32, C.POINTER(_sz), C.c_uint]),
+    "macis_b200_mlp_set_sample_targets": (C.c_int, [_vp, _vp, _sz]),
     "macis_b200_hop_create": (C.c_int, [_vp, _vp, _sz, C.c_double, C.c_uint,
                                         C.POINTER(_vp)]),
     "macis_b200_hop_destroy": (C.c_int, [_vp]),

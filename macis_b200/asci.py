@@ -113,19 +113,33 @@ def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen,
 
 
 def asci_search_part(asci_settings, ndets_max, cdets, E_ASCI, C, norb,
-                     ham_gen, part_index, part_count):
+                     ham_gen, part_index, part_count, screen=None,
+                     use_net=False):
     """One part of an exact search split over part_count processes
     (macis_b200_asci_search_part): (states, scores) of the part's candidates,
     cut at the (ndets_max - ncdets)-th |score| with every tie kept.
-    merge_asci_parts of all parts gives asci_search's result."""
+    merge_asci_parts of all parts gives asci_search's result.
+
+    screen / use_net as in asci_search: parts whose networks are equal keep
+    the same units, so the merge gives the screened whole search; recorded
+    targets cover the part's bins only (their elementwise maximum over the
+    parts is the whole search's, see dist.merge_sample_targets)."""
     cdets = _dets(cdets, ham_gen.nbits)
     C = np.ascontiguousarray(C, dtype=np.float64)[:len(cdets)]
     s = asci_settings.c_struct()
     n = ct.c_size_t()
-    check(LIB.macis_b200_asci_search_part(
-        ham_gen.handle, ct.byref(s), int(ndets_max), cdets.ctypes.data,
-        len(cdets), float(E_ASCI), C.ctypes.data, int(part_index),
-        int(part_count), ct.byref(n), 0))
+    if screen is not None and screen.network is not None:
+        sc = screen.c_struct(use_net)
+        check(LIB.macis_b200_asci_search_part_screened(
+            ham_gen.handle, ct.byref(s), ct.byref(sc), int(ndets_max),
+            cdets.ctypes.data, len(cdets), float(E_ASCI), C.ctypes.data,
+            int(part_index), int(part_count), ct.byref(n), 0))
+        screen.searches += 1
+    else:
+        check(LIB.macis_b200_asci_search_part(
+            ham_gen.handle, ct.byref(s), int(ndets_max), cdets.ctypes.data,
+            len(cdets), float(E_ASCI), C.ctypes.data, int(part_index),
+            int(part_count), ct.byref(n), 0))
     W = ham_gen.nbits // 64
     st = np.empty((max(n.value, 1), W), dtype=np.uint64)
     sc = np.empty(max(n.value, 1))

@@ -495,6 +495,20 @@ int macis_b200_mlp_clamp_samples(macis_b200_mlp* m, double q, float* floor) {
   });
 }
 
+int macis_b200_mlp_set_sample_targets(macis_b200_mlp* m, const float* t,
+                                      size_t n) {
+  return guarded([&] {
+    MB_REQUIRE(m && (t || n == 0), MACIS_B200_EINVAL, "null argument");
+    MB_REQUIRE(n == m->ns, MACIS_B200_EINVAL,
+               "target count differs from the recorded sample count");
+    if(n) {
+      MB_CUDA(cudaMemcpyAsync(m->ts, t, n * 4, cudaMemcpyHostToDevice,
+                              m->stream));
+      MB_CUDA(cudaStreamSynchronize(m->stream));
+    }
+  });
+}
+
 int macis_b200_mlp_samples(const macis_b200_mlp* m, size_t* n, uint16_t* X,
                            float* t) {
   return guarded([&] {
@@ -638,6 +652,16 @@ extern "C" int macis_b200_asci_search_part(
     macis_b200_ham* h, const macis_b200_asci_settings* s, size_t ndets_max,
     const uint64_t* cdets, size_t ncdets, double E0, const double* C,
     uint32_t part_index, uint32_t part_count, size_t* nout, unsigned flags) {
+  return macis_b200_asci_search_part_screened(h, s, nullptr, ndets_max, cdets,
+                                              ncdets, E0, C, part_index,
+                                              part_count, nout, flags);
+}
+
+extern "C" int macis_b200_asci_search_part_screened(
+    macis_b200_ham* h, const macis_b200_asci_settings* s,
+    const macis_b200_asci_screen* scr, size_t ndets_max, const uint64_t* cdets,
+    size_t ncdets, double E0, const double* C, uint32_t part_index,
+    uint32_t part_count, size_t* nout, unsigned flags) {
   return guarded([&] {
     MB_REQUIRE(h && s && nout, MACIS_B200_EINVAL, "null argument");
     MB_REQUIRE(part_count >= 1 && part_index < part_count, MACIS_B200_EINVAL,
@@ -652,7 +676,7 @@ extern "C" int macis_b200_asci_search_part(
     size_t dummy = 0;
     h->part_states.clear();
     h->part_scores.clear();
-    asci_search_device(h, *s, nullptr, ndets_max, cd.d, ncdets, E0, cc.d,
+    asci_search_device(h, *s, scr, ndets_max, cd.d, ncdets, E0, cc.d,
                        nullptr, &dummy, nullptr, nullptr, false, &part);
     *nout = h->part_scores.size();
   });

@@ -304,16 +304,49 @@ def merge_search_parts(part, ndets_max, cdets, nbits, group=None):
     return merge_asci_parts(parts, ndets_max, cdets, nbits)
 
 
+def merge_sample_targets(t, group=None):
+    """Elementwise maximum over the ranks of the recorded sample targets of
+    a split search (every rank records the same sample rows; each target is
+    the unit's largest score over the rank's bins). float32 in and out."""
+    t = np.ascontiguousarray(t, dtype=np.float32).ravel()
+    r, w = rank_world(group)
+    if w == 1:
+        return t
+    import torch
+    x = torch.from_numpy(t.copy()).to(_device(group))
+    _dist().all_reduce(x, op=_dist().ReduceOp.MAX, group=group)
+    return x.cpu().numpy()
+
+
+def _device(group):
+    """Where collective buffers live: CUDA for NCCL, else the CPU."""
+    return "cuda" if _dist().get_backend(group) == "nccl" else "cpu"
+
+
 def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen,
-                group=None):
+                group=None, screen=None, use_net=False):
     """Exact ASCI search split over the ranks of `group`, one GPU each: rank
     r searches part r of world (asci.asci_search_part: its share of the
     alpha-string hash bins, cut by the contribution histogram every rank
     computes alike), then the parts are gathered and merged. The result is
     asci_search's on one GPU, on every rank (the reference's MPI search,
-    determinant_search.hpp:145-391, splits by alpha constraints instead)."""
+    determinant_search.hpp:145-391, splits by alpha constraints instead).
+
+    screen / use_net: the learned screening (asci.asci_search), with every
+    rank holding an equal network. A recording search merges the parts'
+    targets (merge_sample_targets) into every rank's network, so each holds
+    the one-GPU search's samples and training keeps the networks equal."""
     from .asci import asci_search_part
     r, w = rank_world(group)
     part = asci_search_part(asci_settings, ndets_max, cdets, E_ASCI, C, norb,
-                            ham_gen, r, w)
+                            ham_gen, r, w, screen=screen, use_net=use_net)
+    if (w > 1 and screen is not None and screen.network is not None and
+            screen.train and screen.max_samples > 0):
+        _, t = screen.network.samples()
+        dev = _device(group)
+        n = reduce_max(len(t), group, dev)     # equal on every rank
+        if n != len(t) or reduce_sum(len(t), group, dev) != w * n:
+            raise RuntimeError("ranks recorded different sample counts")
+        if len(t):
+            screen.network.set_sample_targets(merge_sample_targets(t, group))
     return merge_search_parts(part, ndets_max, cdets, ham_gen.nbits, group)

@@ -113,6 +113,12 @@ class ScreeningNetwork:
                                                ct.byref(f)))
         return f.value
 
+    def set_sample_targets(self, t):
+        """Overwrite the targets of the recorded samples (same count)."""
+        t = np.ascontiguousarray(t, dtype=np.float32).ravel()
+        check(LIB.macis_b200_mlp_set_sample_targets(self.handle,
+                                                    t.ctypes.data, t.size))
+
     def samples(self):
         """(X, t) recorded by the last search that recorded samples."""
         n = ct.c_size_t()

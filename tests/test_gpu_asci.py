@@ -191,3 +191,53 @@ def test_split_search_merges_to_whole(port, wcase, monkeypatch, nparts):
     assert mb.last_search_stats(H)["batches"] >= 1
     exp = port.asci_search(hp, oracle.AsciSettings.default(), 5000, cd, E, cc)
     assert np.array_equal(got, exp)
+
+
+def test_screened_split_search_matches_whole(wcase):
+    """Learned screening over a split search (parts run one after another
+    here): a recording part stores the whole search's sample rows, and the
+    elementwise maximum of the parts' targets is the whole search's targets;
+    networks trained on them stay equal to the one-GPU network, and a pruning
+    search split into parts merges to the screened whole search."""
+    norb, T, V, hp, cd, cc, E = wcase
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+    nparts, ndets_max = 3, 5000
+    nets = [mb.ScreeningNetwork(nbits=64, seed=0) for _ in range(nparts + 1)]
+    scr = [mb.ScreenSettings(network=n, max_samples=10 ** 6) for n in nets]
+
+    def split(use_net):
+        parts = [mb.asci_search_part(_settings(), ndets_max, cd, E, cc, norb,
+                                     H, i, nparts, screen=scr[i + 1],
+                                     use_net=use_net) for i in range(nparts)]
+        return mb.merge_asci_parts(parts, ndets_max, cd, 64)
+
+    whole = mb.asci_search(_settings(), ndets_max, cd, E, cc, norb, H,
+                           screen=scr[0])
+    Xw, tw = nets[0].samples()
+    assert len(tw) > 1000
+    assert np.array_equal(split(False), whole)
+    got = [n.samples() for n in nets[1:]]
+    for X, t in got:
+        assert np.array_equal(X, Xw)
+    tmax = np.maximum.reduce([t for _, t in got])
+    assert np.array_equal(tmax, tw)
+    assert not all(np.array_equal(t, tw) for _, t in got)
+    for n in nets[1:]:
+        n.set_sample_targets(tmax)
+    for sc in scr:
+        sc.network.clamp_samples(sc.clamp_quantile)
+        sc.network.train(None, None, sc.epochs, sc.batch, sc.lr,
+                         sc.seed + sc.searches)
+    P0 = nets[0].params
+    for n in nets[1:]:
+        assert np.array_equal(n.params, P0)
+    for sc in scr:
+        sc.train = False
+    whole2 = mb.asci_search(_settings(), ndets_max, cd, E, cc, norb, H,
+                            screen=scr[0], use_net=True)
+    st = mb.last_search_stats(H)
+    assert 0 < st["units_kept"] < st["units_total"]
+    assert not np.array_equal(whole2, whole)
+    assert np.array_equal(split(True), whole2)
+    with pytest.raises(mb.MacisError, match="recorded sample count"):
+        nets[1].set_sample_targets(tmax[:-1])

@@ -68,6 +68,23 @@ def _asci_parts(port, world=WORLD, ndets_max=300):
     return out, (st, rv)
 
 
+def _sample_targets(n=1000, seed=3):
+    """Targets of a whole search's samples and the parts' views of them:
+    each unit's largest score lands in one rank's bins; the other ranks see
+    a smaller one (or none: the floor target (ln 1e-12 + 20) / 5)."""
+    rng = np.random.default_rng(seed)
+    floor = np.float32((np.log(1e-12) + 20) / 5)
+    whole = rng.uniform(floor, 4.0, n).astype(np.float32)
+    owner = rng.integers(0, WORLD, n)
+    parts = []
+    for r in range(WORLD):
+        lower = np.maximum(whole - rng.uniform(0, 1, n).astype(np.float32),
+                           floor)
+        lower[rng.random(n) < 0.3] = floor
+        parts.append(np.where(owner == r, whole, lower).astype(np.float32))
+    return whole, parts
+
+
 def _rank_main(rank, port_no, case, q):
     import datetime
 
@@ -114,6 +131,8 @@ def _rank_main(rank, port_no, case, q):
             states, scores, core, ndets_max = parts_in[rank]
             out["merged"] = md.merge_search_parts((states, scores), ndets_max,
                                                   core, 64)
+            t_whole, t_parts = _sample_targets()
+            out["targets"] = md.merge_sample_targets(t_parts[rank])
         dist.barrier()
         dist.destroy_process_group()
         q.put(out)
@@ -206,7 +225,8 @@ def test_p_davidson_single_rank_no_group(port):
 
 def test_split_asci_search_merge_two_ranks(port):
     """merge_search_parts over two gloo ranks returns, on both, the merge of
-    the whole candidate list (the result of the unsplit search)."""
+    the whole candidate list (the result of the unsplit search), and
+    merge_sample_targets the whole search's recorded targets."""
     from macis_b200.asci import merge_asci_parts
     res = _run("asci")
     parts, (st, rv) = _asci_parts(port)
@@ -215,3 +235,8 @@ def test_split_asci_search_merge_two_ranks(port):
     assert len(whole) == ndets_max
     for r in range(WORLD):
         assert np.array_equal(res[r]["merged"], whole)
+    # recorded sample targets: the elementwise maximum over the ranks
+    t_whole, _ = _sample_targets()
+    for r in range(WORLD):
+        assert res[r]["targets"].dtype == np.float32
+        assert np.array_equal(res[r]["targets"], t_whole)
