@@ -203,6 +203,32 @@ def _screened(screen):
             screen.searches >= screen.warmup_searches)
 
 
+def _use_net(screen, ham_gen, cdets, E0, C):
+    """Whether the next search prunes by prediction: a trained network,
+    past the warm-up searches, and (with min_units) a search large enough
+    for the network to save time."""
+    use_net = _screened(screen)
+    if use_net and screen.min_units:
+        from .screening import unit_features
+        _, nunits = unit_features(ham_gen, cdets, E0, C, 0, 0)
+        use_net = nunits >= screen.min_units
+    return use_net
+
+
+def _train_after_search(screen, stats):
+    """Retrain the network on the samples the search recorded (clamped
+    first); returns the milliseconds it took (0 without training)."""
+    if not (screen is not None and screen.network is not None and
+            screen.train and stats["samples"] > 0):
+        return 0.0
+    tt = time.perf_counter()
+    if screen.clamp_quantile:
+        screen.network.clamp_samples(screen.clamp_quantile)
+    screen.network.train(None, None, screen.epochs, screen.batch, screen.lr,
+                         screen.seed + screen.searches)
+    return (time.perf_counter() - tt) * 1e3
+
+
 def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
               norb, screen=None):
     """One ASCI iteration: reorder, search on the ncdets_max largest, then
@@ -215,25 +241,12 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
         wfn, X = reorder_ci_on_coeff(wfn, X)
     nkeep = min(int(asci_settings.ncdets_max), len(wfn))
     t0 = time.perf_counter()
-    use_net = _screened(screen)
-    if use_net and screen.min_units:
-        # small searches run exact: the network cannot save time there
-        from .screening import unit_features
-        _, nunits = unit_features(ham_gen, wfn[:nkeep], E0, X[:nkeep], 0, 0)
-        use_net = nunits >= screen.min_units
+    use_net = _use_net(screen, ham_gen, wfn[:nkeep], E0, X[:nkeep])
     wfn = asci_search(asci_settings, ndets_max, wfn[:nkeep], E0, X[:nkeep],
                       norb, ham_gen, screen=screen, use_net=use_net)
     st = last_search_stats(ham_gen)
     t1 = time.perf_counter()
-    train_ms = 0.0
-    if screen is not None and screen.network is not None and screen.train \
-            and st["samples"] > 0:
-        tt = time.perf_counter()
-        if screen.clamp_quantile:
-            screen.network.clamp_samples(screen.clamp_quantile)
-        screen.network.train(None, None, screen.epochs, screen.batch,
-                             screen.lr, screen.seed + screen.searches)
-        train_ms = (time.perf_counter() - tt) * 1e3
+    train_ms = _train_after_search(screen, st)
     t1b = time.perf_counter()
     tim = {}
     E, X = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,

@@ -29,7 +29,8 @@ __all__ = ["rank_world", "local_rows", "reduce_max", "reduce_sum",
            "allgather_rows", "DistCSR", "make_dist_csr_hamiltonian",
            "RowBlockOperator", "p_gram_schmidt", "p_rayleigh_ritz",
            "p_davidson", "gather_row_blocks", "merge_search_parts",
-           "asci_search"]
+           "merge_sample_targets", "asci_search", "p_diagonal_guess",
+           "selected_ci_diag", "asci_iter", "asci_grow", "asci_refine"]
 
 
 def _dist():
@@ -320,6 +321,8 @@ def merge_sample_targets(t, group=None):
 
 def _device(group):
     """Where collective buffers live: CUDA for NCCL, else the CPU."""
+    if rank_world(group)[1] == 1:
+        return "cpu"
     return "cuda" if _dist().get_backend(group) == "nccl" else "cpu"
 
 
@@ -350,3 +353,114 @@ def asci_search(asci_settings, ndets_max, cdets, E_ASCI, C, norb, ham_gen,
         if len(t):
             screen.network.set_sample_targets(merge_sample_targets(t, group))
     return merge_search_parts(part, ndets_max, cdets, ham_gen.nbits, group)
+
+
+def p_diagonal_guess(D_local, N, group=None):
+    """p_diagonal_guess (davidson.hpp:72-110): this rank's rows of the unit
+    vector at the first minimum of the full diagonal, which is gathered
+    from every rank's rows."""
+    import torch
+    D = allgather_rows(D_local, N, group)
+    g = int(torch.argmin(D).item())     # the first minimum
+    lo, hi = local_rows(N, group)
+    X = torch.zeros(hi - lo, dtype=torch.float64, device=D_local.device)
+    if lo <= g < hi:
+        X[g - lo] = 1.0
+    return X
+
+
+def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
+                     davidson_res_tol, C_local=None, group=None, log=None):
+    """selected_ci_diag over the ranks of `group` (selected_ci_diag.hpp:
+    125-206 with a communicator, parallel_selected_ci_diag :23-72): this
+    rank's row block of H on its GPU (make_dist_csr_hamiltonian), the guess,
+    then p_davidson (no restarts, as the reference). C_local (this rank's
+    rows) is the guess when max |C| over all ranks exceeds 1/N; else the
+    diagonal guess (p_diagonal_guess). Returns (E0, X_local), X_local this
+    rank's rows of the eigenvector as a CUDA tensor.
+
+    The reference compares each rank's own max |C_local| with 1/len(C_local),
+    so its ranks can disagree, and only some of them then enter the
+    collective p_diagonal_guess; here the test is one over all ranks."""
+    import torch
+    dets = _host_dets(dets, ham_gen.nbits)
+    N = len(dets)
+    A = make_dist_csr_hamiltonian(dets, ham_gen, h_el_tol, group=group)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    D = A.diagonal(dev)
+    use = False
+    if C_local is not None and len(C_local) == A.m_local:
+        c = torch.as_tensor(np.asarray(C_local, dtype=np.float64)).to(dev)
+        mx = float(c.abs().max().item()) if A.m_local else 0.0
+        use = reduce_max(mx, group, _device(group)) > 1.0 / max(N, 1)
+    X = c.clone() if use else p_diagonal_guess(D, N, group)
+    it, E = p_davidson(A.m_local, int(davidson_max_m), A.operator(), D,
+                       davidson_res_tol, X, group, log)
+    return E, X
+
+
+def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
+              norb, group=None, screen=None):
+    """asci_iter with a communicator (iteration.hpp:17-68): reorder on |C|,
+    the split search over the ranks (asci_search above), the distributed
+    rediagonalisation without guess reuse (selected_ci_diag above), and the
+    eigenvector all-gathered to every rank. screen as in asci.asci_iter,
+    with an equal network on every rank. Only the reference solver is
+    distributed: FP64 values, no thick restart."""
+    from .asci import (_dets, _train_after_search, _use_net,
+                       last_search_stats, reorder_ci_on_coeff)
+    from .solvers import FP64
+    if mcscf_settings.precision != FP64 or mcscf_settings.davidson_restart_keep:
+        raise NotImplementedError(
+            "the distributed solve is the reference p_davidson: FP64, no "
+            "restart")
+    wfn = _dets(wfn, ham_gen.nbits)
+    X = np.asarray(X, dtype=np.float64)
+    if len(wfn) > 1:
+        wfn, X = reorder_ci_on_coeff(wfn, X)
+    nkeep = min(int(asci_settings.ncdets_max), len(wfn))
+    use_net = _use_net(screen, ham_gen, wfn[:nkeep], E0, X[:nkeep])
+    wfn = asci_search(asci_settings, ndets_max, wfn[:nkeep], E0, X[:nkeep],
+                      norb, ham_gen, group, screen=screen, use_net=use_net)
+    _train_after_search(screen, last_search_stats(ham_gen))
+    E, X_local = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,
+                                  mcscf_settings.ci_max_subspace,
+                                  mcscf_settings.ci_res_tol, None, group)
+    X = allgather_rows(X_local, len(wfn), group).cpu().numpy()
+    return E, wfn, X
+
+
+def asci_grow(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb,
+              group=None, screen=None):
+    """asci_grow (grow.hpp:17-171, without grow_with_rot) over the ranks:
+    distributed asci_iter until ntdets_max determinants."""
+    from .asci import _dets
+    wfn = _dets(wfn, ham_gen.nbits)
+    if asci_settings.grow_with_rot:
+        raise NotImplementedError("grow_with_rot is outside the GPU path")
+    while len(wfn) < asci_settings.ntdets_max:
+        ndets_new = min(max(asci_settings.ntdets_min,
+                            len(wfn) * asci_settings.grow_factor),
+                        asci_settings.ntdets_max)
+        E, wfn, X = asci_iter(asci_settings, mcscf_settings, ndets_new, E0,
+                              wfn, X, ham_gen, norb, group, screen)
+        if ndets_new > len(wfn):
+            raise RuntimeError("Wavefunction didn't grow enough...")
+        E0 = E
+    return E0, wfn, X
+
+
+def asci_refine(asci_settings, mcscf_settings, E0, wfn, X, ham_gen, norb,
+                group=None, screen=None):
+    """asci_refine (refine.hpp:15-66) over the ranks."""
+    ndets = len(wfn)
+    for _ in range(asci_settings.max_refine_iter):
+        E, wfn, X = asci_iter(asci_settings, mcscf_settings, ndets, E0, wfn,
+                              X, ham_gen, norb, group, screen)
+        if len(wfn) != ndets:
+            raise RuntimeError("Wavefunction size can't change in refinement")
+        dE = E - E0
+        E0 = E
+        if abs(dE) < asci_settings.refine_energy_tol:
+            return E0, wfn, X
+    raise RuntimeError("ACCI Refine did not converge")

@@ -59,3 +59,29 @@ def test_dist_csr_offset_block_diagonal(port):
                                             np.finfo(float).eps)
         D = md.DistCSR(blk, lo, hi, N, bra=dets[lo:hi]).diagonal().numpy()
         assert np.array_equal(D, full[lo:hi])
+
+
+def test_dist_asci_grow_refine_water_golden():
+    """The distributed ASCI drivers at world size 1 (no process group): the
+    split search, the row-block H with p_davidson and the gathered vector
+    reproduce the water grow and refine energies."""
+    from golden_data import constants, water
+
+    from macis_b200 import dist as md
+    K = constants()
+    norb, T, V, _ = water()
+    H = mb.HamiltonianGenerator(T, V, 64, norb)
+    s = mb.ASCISettings()
+    s.ntdets_max = K["water_asci_ntdets_max"]
+    ci = mb.MCSCFSettings()
+    hf = mb.canonical_hf_determinant(5, 5, 64)
+    E0 = H.matrix_element(hf, hf)
+    E, dets, X = md.asci_grow(s, ci, E0, hf, np.ones(1), H, norb)
+    assert len(dets) == 10000 and abs(X @ X - 1) < 1e-10
+    assert abs(E - K["water_asci_grow_e0"]) < 1e-8
+    E, dets, X = md.asci_refine(s, ci, E, dets, X, H, norb)
+    assert len(dets) == 10000
+    assert abs(E - K["water_asci_refine_e0"]) < 1e-7
+    ci.precision = mb.MIXED
+    with pytest.raises(NotImplementedError):
+        md.asci_iter(s, ci, 10000, E, dets, X, H, norb)

@@ -121,6 +121,8 @@ def _rank_main(rank, port_no, case, q):
             X = torch.zeros(hi - lo, dtype=torch.float64)
             if lo <= g < hi:
                 X[g - lo] = 1.0
+            out["guess_equal"] = bool(torch.equal(
+                md.p_diagonal_guess(torch.from_numpy(D), N), X))
             op = md.RowBlockOperator(mv, N)
             it, E = md.p_davidson(hi - lo, 200, op, torch.from_numpy(D),
                                   1e-8, X)
@@ -185,6 +187,7 @@ def test_row_blocks_gather_and_reductions(port):
 
 def test_p_davidson_two_ranks_matches_serial(port):
     res = _run("davidson")
+    assert all(res[r]["guess_equal"] for r in range(WORLD))  # p_diagonal_guess
     T, V, dets = _problem()
     rp, ci, nz = port.build_csr(port.ham(64, 7, T, V), dets, dets,
                                 np.finfo(float).eps)
