@@ -29,7 +29,7 @@ __all__ = ["rank_world", "local_rows", "reduce_max", "reduce_sum",
            "allgather_rows", "DistCSR", "make_dist_csr_hamiltonian",
            "RowBlockOperator", "p_gram_schmidt", "p_rayleigh_ritz",
            "p_davidson", "gather_row_blocks", "merge_search_parts",
-           "merge_sample_targets", "asci_search", "p_diagonal_guess",
+           "merge_sample_targets", "asci_search", "p_diagonal_guess", "reuse_guess",
            "selected_ci_diag", "asci_iter", "asci_grow", "asci_refine"]
 
 
@@ -369,6 +369,16 @@ def p_diagonal_guess(D_local, N, group=None):
     return X
 
 
+def reuse_guess(C_local, N, group=None):
+    """Whether the passed vector is the Davidson guess: max |C| over all
+    ranks above 1/N (selected_ci_diag.hpp:41-52 and :94-101, decided once for
+    all ranks). C_local None or empty counts as zero on this rank."""
+    c = np.abs(np.asarray(C_local, dtype=np.float64)) if C_local is not None \
+        else np.zeros(0)
+    mx = float(c.max()) if c.size else 0.0
+    return reduce_max(mx, group, _device(group)) > 1.0 / max(N, 1)
+
+
 def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
                      davidson_res_tol, C_local=None, group=None, log=None):
     """selected_ci_diag over the ranks of `group` (selected_ci_diag.hpp:
@@ -388,12 +398,11 @@ def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
     A = make_dist_csr_hamiltonian(dets, ham_gen, h_el_tol, group=group)
     dev = torch.device("cuda", torch.cuda.current_device())
     D = A.diagonal(dev)
-    use = False
-    if C_local is not None and len(C_local) == A.m_local:
-        c = torch.as_tensor(np.asarray(C_local, dtype=np.float64)).to(dev)
-        mx = float(c.abs().max().item()) if A.m_local else 0.0
-        use = reduce_max(mx, group, _device(group)) > 1.0 / max(N, 1)
-    X = c.clone() if use else p_diagonal_guess(D, N, group)
+    ok = C_local is not None and len(C_local) == A.m_local
+    if reuse_guess(C_local if ok else None, N, group):
+        X = torch.as_tensor(np.asarray(C_local, dtype=np.float64)).to(dev)
+    else:
+        X = p_diagonal_guess(D, N, group)
     it, E = p_davidson(A.m_local, int(davidson_max_m), A.operator(), D,
                        davidson_res_tol, X, group, log)
     return E, X

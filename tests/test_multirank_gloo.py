@@ -135,6 +135,11 @@ def _rank_main(rank, port_no, case, q):
                                                   core, 64)
             t_whole, t_parts = _sample_targets()
             out["targets"] = md.merge_sample_targets(t_parts[rank])
+            # guess reuse is one decision for all ranks: only rank 0 holds
+            # a coefficient above 1/N = 0.01 in the first case
+            out["reuse"] = (
+                md.reuse_guess([0.5, 0.0] if rank == 0 else [0.0], 100),
+                md.reuse_guess([0.005] if rank == 0 else None, 100))
         dist.barrier()
         dist.destroy_process_group()
         q.put(out)
@@ -238,6 +243,8 @@ def test_split_asci_search_merge_two_ranks(port):
     assert len(whole) == ndets_max
     for r in range(WORLD):
         assert np.array_equal(res[r]["merged"], whole)
+    for r in range(WORLD):
+        assert res[r]["reuse"] == (True, False)
     # recorded sample targets: the elementwise maximum over the ranks
     t_whole, _ = _sample_targets()
     for r in range(WORLD):
