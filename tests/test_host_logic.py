@@ -1,5 +1,6 @@
 """Host-side logic that needs no GPU: determinant spaces, integrals, the
-Rayleigh-Ritz eigensolver, the C ABI surface and the row-block partition."""
+Rayleigh-Ritz eigensolver, the C ABI surface, the row-block partition and
+the drivers' use of the screening settings."""
 import ctypes
 import os
 import re
@@ -133,3 +134,49 @@ def test_settings_defaults_match_reference():
     m = mb.MCSCFSettings()
     assert (m.ci_res_tol, m.ci_max_subspace) == (1e-8, 20)
     assert m.ci_matel_tol == np.finfo(float).eps
+
+
+class _FakeNet:
+    """Stands in for a ScreeningNetwork: records what the drivers ask of it."""
+
+    handle = None
+
+    def __init__(self, trained_steps):
+        self.trained_steps = trained_steps
+        self.calls = []
+
+    def clamp_samples(self, q):
+        self.calls.append(("clamp", q))
+
+    def train(self, X, t, epochs, batch, lr, seed):
+        self.calls.append(("train", X, t, epochs, batch, lr, seed))
+
+
+def test_screening_decision_and_retraining():
+    """The drivers' use of ScreenSettings: no pruning before the network is
+    trained or during the warm-up searches; retraining (clamped first) only
+    after a search that recorded samples, seeded by the search count."""
+    from macis_b200.asci import _train_after_search, _use_net
+    net = _FakeNet(trained_steps=0)
+    sc = mb.ScreenSettings(network=net, min_units=0, warmup_searches=2,
+                           clamp_quantile=0.6, seed=5)
+    assert not _use_net(None, None, None, 0.0, None)
+    assert not _use_net(sc, None, None, 0.0, None)        # untrained
+    net.trained_steps = 1
+    sc.searches = 1
+    assert not _use_net(sc, None, None, 0.0, None)        # warm-up
+    sc.searches = 2
+    assert _use_net(sc, None, None, 0.0, None)
+    assert _train_after_search(sc, {"samples": 0}) == 0.0
+    assert net.calls == []
+    assert _train_after_search(sc, {"samples": 10}) >= 0.0
+    assert net.calls == [("clamp", 0.6),
+                         ("train", None, None, sc.epochs, sc.batch, sc.lr, 7)]
+    sc.train = False
+    net.calls.clear()
+    _train_after_search(sc, {"samples": 10})
+    assert net.calls == []
+    assert sc.c_struct(True).max_samples == 0              # nothing recorded
+    sc.train, sc.clamp_quantile = True, 0.0
+    _train_after_search(sc, {"samples": 10})
+    assert [c[0] for c in net.calls] == ["train"]
