@@ -180,3 +180,14 @@ def test_screening_decision_and_retraining():
     sc.train, sc.clamp_quantile = True, 0.0
     _train_after_search(sc, {"samples": 10})
     assert [c[0] for c in net.calls] == ["train"]
+
+
+def test_product_does_not_use_the_oracle():
+    """The package (the product path) imports neither the oracle nor any
+    working file; only the tests, smoke() and bench.py's baseline legs do."""
+    pat = re.compile(r"^\s*(import|from)\s+(\.*\s*)?(oracle|_work)\b", re.M)
+    pkg = os.path.join(ROOT, "macis_b200")
+    for f in sorted(os.listdir(pkg)):
+        if f.endswith(".py"):
+            with open(os.path.join(pkg, f)) as fh:
+                assert not pat.search(fh.read()), f
