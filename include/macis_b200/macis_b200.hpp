@@ -414,9 +414,9 @@ auto asci_iter(macis::ASCISettings asci_settings,
     bool use_net = screen->prune_next();
     if(use_net && screen->min_units) {  // small searches run exact
       size_t nunits = 0;
-      check(macis_b200_asci_unit_features(ham_gen.handle(), words<N>(&wfn[0]),
-                                          nkeep, E0, X.data(), 0, 0, nullptr,
-                                          &nunits));
+      check(macis_b200_asci_unit_features(
+          ham_gen.handle(), nkeep ? words<N>(wfn.data()) : nullptr, nkeep, E0,
+          X.data(), 0, 0, nullptr, &nunits));
       use_net = nunits >= screen->min_units;
     }
     wfn = asci_search<N>(asci_settings, ndets_max, wfn.begin(),
