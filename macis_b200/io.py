@@ -184,7 +184,10 @@ def write_rdms_binary(fname, norb, ordm, trdm):
 
 def read_rdms_binary(fname, norb):
     """(ordm, trdm) flat column-major from a binary RDM file; the stored
-    norb must match (read_rdms_binary, fcidump.cxx:202-250)."""
+    norb must match (read_rdms_binary, fcidump.cxx:209-250). Both reads go
+    into one zero-initialised norb^4 buffer, as there, so a short file
+    leaves the bytes it lacks as that buffer held them: zeros, or for the
+    2-RDM the 1-RDM bytes read before."""
     n = int(norb)
     with open(fname, "rb") as f:
         head = f.read(4)
@@ -193,6 +196,11 @@ def read_rdms_binary(fname, norb):
         nr = struct.unpack("i", head)[0]
         if nr != n:
             raise RuntimeError(f"NORB in RDM file doesn't match {n} {nr}")
-        o = np.frombuffer(f.read(n * n * 8), dtype=np.float64).copy()
-        t = np.frombuffer(f.read(n ** 4 * 8), dtype=np.float64).copy()
+        raw = bytearray(n ** 4 * 8)
+        b = f.read(n * n * 8)
+        raw[:len(b)] = b
+        o = np.frombuffer(bytes(raw[:n * n * 8]), dtype=np.float64).copy()
+        b = f.read(n ** 4 * 8)
+        raw[:len(b)] = b
+        t = np.frombuffer(bytes(raw), dtype=np.float64).copy()
     return o, t

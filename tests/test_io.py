@@ -82,3 +82,18 @@ def test_rdms_binary_round_trip(tmp_path):
     assert np.array_equal(o2, o) and np.array_equal(t2, t)
     with pytest.raises(RuntimeError, match="NORB in RDM file"):
         mio.read_rdms_binary(f, n + 1)
+    # short files (fcidump.cxx:235-249 reads into one zeroed buffer): a
+    # missing 2-RDM keeps the 1-RDM bytes at its start, the rest is zero
+    f.write_bytes(raw[:4 + 8 * n * n])
+    o3, t3 = mio.read_rdms_binary(f, n)
+    assert np.array_equal(o3, o)
+    assert np.array_equal(t3[:n * n], o) and not t3[n * n:].any()
+    f.write_bytes(raw[:4 + 8 * (n * n + 5)])
+    o4, t4 = mio.read_rdms_binary(f, n)
+    assert np.array_equal(o4, o)
+    assert np.array_equal(t4[:5], t[:5]) and np.array_equal(t4[5:n * n], o[5:])
+    assert not t4[n * n:].any()
+    f.write_bytes(raw[:4 + 8 * 3])
+    o5, t5 = mio.read_rdms_binary(f, n)
+    assert np.array_equal(o5[:3], o[:3]) and not o5[3:].any()
+    assert np.array_equal(t5[:3], o[:3]) and not t5[3:].any()
