@@ -151,17 +151,19 @@ def write_wavefunction(fname, norb, dets, coeffs, nbits=64):
 
 def read_wavefunction(fname, nbits=64):
     """(dets, coeffs) of an ASCII wavefunction file (read_wavefunction,
-    wavefunction_io.hpp:39-74): the header line, then '<COEFF> <STR>'
-    lines."""
+    wavefunction_io.hpp:39-74): the header line, whose four fields must
+    parse as integers, then one '<COEFF> <STR>' line per determinant. As
+    there, every later line is a determinant: a blank one has no
+    coefficient and raises, a missing string is the empty determinant."""
     dets, coeffs = [], []
     with open(fname) as f:
-        f.readline()
+        head = f.readline().split()
+        for tok in (head + [""] * 4)[:4]:
+            _stoi(tok)
         for line in f:
-            tok = line.split()
-            if len(tok) < 2:
-                continue
-            coeffs.append(_stod(tok[0]))
+            tok = line.split() + ["", ""]
             dets.append(from_canonical_string(tok[1], nbits)[0])
+            coeffs.append(_stod(tok[0]))
     W = nbits // 64
     out = (np.asarray(dets, dtype=np.uint64).reshape(-1, W) if dets
            else np.zeros((0, W), dtype=np.uint64))

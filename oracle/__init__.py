@@ -312,6 +312,10 @@ class Ref:
                                          C.c_size_t, _p64]
         L.mref_cisd_space.restype = C.c_size_t
         L.mref_cisd_space.argtypes = L.mref_hilbert_space.argtypes
+        L.mref_read_wavefunction.restype = C.c_long
+        L.mref_read_wavefunction.argtypes = [C.c_char_p, _p64, _pd, C.c_size_t]
+        L.mref_write_wavefunction.argtypes = [C.c_char_p, C.c_size_t, _p64, _pd,
+                                              C.c_size_t, C.c_size_t]
 
     def _err(self):
         return self.L.mref_last_error().decode()
@@ -326,6 +330,26 @@ class Ref:
         if not h:
             raise RuntimeError(self._err())
         return Handle(h, self.L.mref_ham_free, nbits, norb)
+
+    def read_wavefunction(self, fname, cap=1 << 16):
+        """(dets, coeffs) from the reference's read_wavefunction<64>;
+        RuntimeError with its message when it throws."""
+        d = np.zeros(cap, dtype=np.uint64)
+        c = np.zeros(cap)
+        n = self.L.mref_read_wavefunction(str(fname).encode(), _ptr(d, _p64),
+                                          _ptr(c, _pd), cap)
+        if n < 0:
+            raise RuntimeError(self._err())
+        return d[:n].reshape(-1, 1), c[:n]
+
+    def write_wavefunction(self, fname, norb, dets, coeffs):
+        """The reference's write_wavefunction<64>."""
+        d = np.ascontiguousarray(dets, dtype=np.uint64).ravel()
+        c = np.ascontiguousarray(coeffs, dtype=np.float64)
+        if self.L.mref_write_wavefunction(str(fname).encode(), int(norb),
+                                          _ptr(d, _p64), _ptr(c, _pd),
+                                          len(d), len(c)) != 0:
+            raise RuntimeError(self._err())
 
     def form_rdms(self, h, dets, C, two=True):
         """(1-RDM, 2-RDM or None) of C over dets from the reference's

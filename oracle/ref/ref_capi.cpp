@@ -31,6 +31,7 @@
 #include <macis/solvers/davidson.hpp>
 #include <macis/solvers/selected_ci_diag.hpp>
 #include <macis/util/mcscf.hpp>
+#include <macis/wavefunction_io.hpp>
 #include <sparsexx/spblas/spmbv.hpp>
 #include <sparsexx/util/submatrix.hpp>
 #include <atomic>
@@ -474,6 +475,41 @@ size_t mref_cisd_space(int nbits, size_t norb, size_t na, size_t nb,
   auto d = macis::generate_cisd_hilbert_space<128>(norb, hf);
   if(out) from_dets(d, out);
   return d.size();
+}
+
+// read_wavefunction<64> (wavefunction_io.hpp:39-74): the number of
+// determinants (at most cap copied out), or -1 when the reader throws.
+long mref_read_wavefunction(const char* fname, uint64_t* dets, double* coeffs,
+                            size_t cap) {
+  try {
+    std::vector<std::bitset<64>> st;
+    std::vector<double> c;
+    macis::read_wavefunction<64>(fname, st, c);
+    for(size_t i = 0; i < st.size() && i < cap; ++i) {
+      dets[i] = st[i].to_ullong();
+      coeffs[i] = c[i];
+    }
+    return long(st.size());
+  } catch(std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// write_wavefunction<64> (wavefunction_io.hpp:88-114); -1 when it throws.
+int mref_write_wavefunction(const char* fname, size_t norb,
+                            const uint64_t* dets, const double* coeffs,
+                            size_t n, size_t nc) {
+  try {
+    std::vector<std::bitset<64>> st(n);
+    for(size_t i = 0; i < n; ++i) st[i] = std::bitset<64>(dets[i]);
+    std::vector<double> c(coeffs, coeffs + nc);
+    macis::write_wavefunction<64>(fname, norb, st, c);
+    return 0;
+  } catch(std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
 }
 
 }  // extern "C"

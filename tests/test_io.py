@@ -69,6 +69,41 @@ def test_wavefunction_round_trip(tmp_path, nbits):
         mio.write_wavefunction(f, 6, dets, c[:-1], nbits)
 
 
+def test_wavefunction_reader_rules(tmp_path, ref):
+    """wavefunction_io.hpp:39-74: stoi of the four header fields, then
+    every line a determinant (stod of its coefficient) -- checked against
+    the compiled reference reader on the same files."""
+    f = tmp_path / "wfn.dat"
+
+    def both(text):
+        f.write_text(text)
+        return mio.read_wavefunction(f), ref.read_wavefunction(f)
+
+    (d, c), (dr, cr) = both("2 4 1 1\n  0.5e0 2000 \n-0.25 ud\n")
+    assert np.array_equal(c, [0.5, -0.25])
+    assert np.array_equal(d[:, 0], [1 | (1 << 32), 1 | (2 << 32)])
+    assert np.array_equal(d, dr) and np.array_equal(c, cr)
+    # no string: the empty determinant; extra tokens ignored
+    (d, c), (dr, cr) = both("2 4 1 1\n0.5 2000 x y\n0.7\n")
+    assert d[1, 0] == 0 and c[1] == 0.7
+    assert np.array_equal(d, dr) and np.array_equal(c, cr)
+    # the writers agree byte for byte (64-bit determinants)
+    dets = mb.generate_hilbert_space(6, 3, 2, 64)[:25]
+    cf = np.random.default_rng(2).standard_normal(len(dets)) * 1e-3
+    mio.write_wavefunction(tmp_path / "a.dat", 6, dets, cf)
+    ref.write_wavefunction(tmp_path / "b.dat", 6, dets, cf)
+    assert (tmp_path / "a.dat").read_bytes() == (tmp_path / "b.dat").read_bytes()
+    with pytest.raises(RuntimeError, match="Invalid Wave Function"):
+        ref.write_wavefunction(tmp_path / "b.dat", 6, dets, cf[:-1])
+    # a blank line, a short header: both readers raise
+    for text in ("2 4 1 1\n0.5 2000\n\n0.1 ud\n", "2 4 1\n0.5 2000\n"):
+        f.write_text(text)
+        with pytest.raises(ValueError):
+            mio.read_wavefunction(f)
+        with pytest.raises(RuntimeError):
+            ref.read_wavefunction(f)
+
+
 def test_rdms_binary_round_trip(tmp_path):
     n = 4
     rng = np.random.default_rng(1)
