@@ -316,6 +316,10 @@ class Ref:
         L.mref_read_wavefunction.argtypes = [C.c_char_p, _p64, _pd, C.c_size_t]
         L.mref_write_wavefunction.argtypes = [C.c_char_p, C.c_size_t, _p64, _pd,
                                               C.c_size_t, C.c_size_t]
+        L.mref_read_fcidump.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), _pd,
+                                        _pd, _pd]
+        L.mref_write_fcidump.argtypes = [C.c_char_p, C.c_size_t, _pd, _pd,
+                                         C.c_double]
 
     def _err(self):
         return self.L.mref_last_error().decode()
@@ -341,6 +345,29 @@ class Ref:
         if n < 0:
             raise RuntimeError(self._err())
         return d[:n].reshape(-1, 1), c[:n]
+
+    def read_fcidump(self, fname):
+        """(norb, T, V, E_core) from the reference's FCIDUMP readers (flat
+        column-major, zero where the file has no line)."""
+        n = C.c_uint32()
+        if self.L.mref_read_fcidump(str(fname).encode(), C.byref(n), None,
+                                    None, None) != 0:
+            raise RuntimeError(self._err())
+        T, V, core = np.zeros(n.value ** 2), np.zeros(n.value ** 4), C.c_double()
+        if self.L.mref_read_fcidump(str(fname).encode(), C.byref(n),
+                                    _ptr(T, _pd), _ptr(V, _pd),
+                                    C.byref(core)) != 0:
+            raise RuntimeError(self._err())
+        return n.value, T, V, core.value
+
+    def write_fcidump(self, fname, norb, T, V, E_core):
+        """The reference's write_fcidump."""
+        T = np.ascontiguousarray(T, dtype=np.float64).ravel(order="K")
+        V = np.ascontiguousarray(V, dtype=np.float64).ravel(order="K")
+        if self.L.mref_write_fcidump(str(fname).encode(), int(norb),
+                                     _ptr(T, _pd), _ptr(V, _pd),
+                                     float(E_core)) != 0:
+            raise RuntimeError(self._err())
 
     def write_wavefunction(self, fname, norb, dets, coeffs):
         """The reference's write_wavefunction<64>."""

@@ -31,6 +31,7 @@
 #include <macis/solvers/davidson.hpp>
 #include <macis/solvers/selected_ci_diag.hpp>
 #include <macis/util/mcscf.hpp>
+#include <macis/util/fcidump.hpp>
 #include <macis/wavefunction_io.hpp>
 #include <sparsexx/spblas/spmbv.hpp>
 #include <sparsexx/util/submatrix.hpp>
@@ -491,6 +492,41 @@ long mref_read_wavefunction(const char* fname, uint64_t* dets, double* coeffs,
     }
     return long(st.size());
   } catch(std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// read_fcidump_norb / _core / _1body / _2body (fcidump.cxx:78-182): with
+// T == NULL only *norb; else T (norb^2) and V (norb^4) must be zeroed by the
+// caller, leading dimensions norb. -1 when the reader throws.
+int mref_read_fcidump(const char* fname, uint32_t* norb, double* T, double* V,
+                      double* core) {
+  try {
+    *norb = macis::read_fcidump_norb(fname);
+    if(T) {
+      *core = macis::read_fcidump_core(fname);
+      macis::read_fcidump_1body(fname, T, *norb);
+      macis::read_fcidump_2body(fname, V, *norb);
+    }
+    return 0;
+  } catch(std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// write_fcidump (fcidump.cxx:184-207). The writer registers an spdlog
+// logger named "fcidump"; it is dropped afterwards, which closes the file
+// and lets the next call register it again.
+int mref_write_fcidump(const char* fname, size_t norb, const double* T,
+                       const double* V, double core) {
+  try {
+    macis::write_fcidump(fname, norb, T, norb, V, norb, core);
+    spdlog::drop("fcidump");
+    return 0;
+  } catch(std::exception& e) {
+    spdlog::drop("fcidump");
     g_err = e.what();
     return -1;
   }

@@ -11,10 +11,13 @@ from macis_b200 import io as mio
 from golden_data import water
 
 
-def test_fcidump_round_trip_water(tmp_path):
+def test_fcidump_round_trip_water(tmp_path, ref):
     norb, T, V, ecore = water()
     f = tmp_path / "FCIDUMP"
     mio.write_fcidump(f, norb, T, V, ecore)
+    # the reference's writer (fcidump.cxx:184-207) writes the same bytes
+    ref.write_fcidump(tmp_path / "FCIDUMP.ref", norb, T, V, ecore)
+    assert f.read_bytes() == (tmp_path / "FCIDUMP.ref").read_bytes()
     n, T2, V2, e2 = mio.read_fcidump(f)
     assert n == norb and e2 == ecore
     assert np.array_equal(T2, np.asarray(T).ravel(order="F"))
@@ -25,7 +28,7 @@ def test_fcidump_round_trip_water(tmp_path):
     assert lines[-1].split()[:4] == ["0", "0", "0", "0"]
 
 
-def test_fcidump_reader_rules(tmp_path):
+def test_fcidump_reader_rules(tmp_path, ref):
     f = tmp_path / "FCIDUMP"
     f.write_text(
         " &FCI NORB=  3,NELEC=2,MS2=0,\n"
@@ -46,10 +49,16 @@ def test_fcidump_reader_rules(tmp_path):
     assert Vm[0, 0, 1, 1] == Vm[1, 1, 0, 0] == 0.5
     assert Vm[2, 2, 0, 0] == Vm[0, 0, 2, 2] == 0.25
     assert np.count_nonzero(V) == 4
+    # the same file through the reference's readers (fcidump.cxx:78-182)
+    nr, Tr, Vr, er = ref.read_fcidump(f)
+    assert (nr, er) == (n, e)
+    assert np.array_equal(Tr, T) and np.array_equal(Vr, V)
     bad = tmp_path / "BAD"
     bad.write_text("1.0 1 1 1 2.0\n")     # value at both ends
     with pytest.raises(RuntimeError, match="Invalid FCIDUMP Line"):
         mio.read_fcidump(bad)
+    with pytest.raises(RuntimeError, match="Invalid FCIDUMP Line"):
+        ref.read_fcidump(bad)
 
 
 @pytest.mark.parametrize("nbits", [64, 128, 256])
