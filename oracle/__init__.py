@@ -320,6 +320,8 @@ class Ref:
                                         _pd, _pd]
         L.mref_write_fcidump.argtypes = [C.c_char_p, C.c_size_t, _pd, _pd,
                                          C.c_double]
+        L.mref_read_rdms_binary.argtypes = [C.c_char_p, C.c_size_t, _pd, _pd]
+        L.mref_write_rdms_binary.argtypes = [C.c_char_p, C.c_size_t, _pd, _pd]
 
     def _err(self):
         return self.L.mref_last_error().decode()
@@ -367,6 +369,22 @@ class Ref:
         if self.L.mref_write_fcidump(str(fname).encode(), int(norb),
                                      _ptr(T, _pd), _ptr(V, _pd),
                                      float(E_core)) != 0:
+            raise RuntimeError(self._err())
+
+    def read_rdms_binary(self, fname, norb):
+        """(ordm, trdm) from the reference's read_rdms_binary."""
+        o, t = np.zeros(norb ** 2), np.zeros(norb ** 4)
+        if self.L.mref_read_rdms_binary(str(fname).encode(), int(norb),
+                                        _ptr(o, _pd), _ptr(t, _pd)) != 0:
+            raise RuntimeError(self._err())
+        return o, t
+
+    def write_rdms_binary(self, fname, norb, ordm, trdm):
+        """The reference's write_rdms_binary."""
+        o = np.ascontiguousarray(ordm, dtype=np.float64).ravel(order="K")
+        t = np.ascontiguousarray(trdm, dtype=np.float64).ravel(order="K")
+        if self.L.mref_write_rdms_binary(str(fname).encode(), int(norb),
+                                         _ptr(o, _pd), _ptr(t, _pd)) != 0:
             raise RuntimeError(self._err())
 
     def write_wavefunction(self, fname, norb, dets, coeffs):

@@ -31,6 +31,7 @@
 #include <macis/solvers/davidson.hpp>
 #include <macis/solvers/selected_ci_diag.hpp>
 #include <macis/util/mcscf.hpp>
+#include <macis/util/binary_rdms.hpp>
 #include <macis/util/fcidump.hpp>
 #include <macis/wavefunction_io.hpp>
 #include <sparsexx/spblas/spmbv.hpp>
@@ -527,6 +528,30 @@ int mref_write_fcidump(const char* fname, size_t norb, const double* T,
     return 0;
   } catch(std::exception& e) {
     spdlog::drop("fcidump");
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// read_rdms_binary / write_rdms_binary (fcidump.cxx:209-276), leading
+// dimensions norb; -1 when they throw.
+int mref_read_rdms_binary(const char* fname, size_t norb, double* ORDM,
+                          double* TRDM) {
+  try {
+    macis::read_rdms_binary(fname, norb, ORDM, norb, TRDM, norb);
+    return 0;
+  } catch(std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+int mref_write_rdms_binary(const char* fname, size_t norb, const double* ORDM,
+                           const double* TRDM) {
+  try {
+    macis::write_rdms_binary(fname, norb, ORDM, norb, TRDM, norb);
+    return 0;
+  } catch(std::exception& e) {
     g_err = e.what();
     return -1;
   }

@@ -113,13 +113,15 @@ def test_wavefunction_reader_rules(tmp_path, ref):
             ref.read_wavefunction(f)
 
 
-def test_rdms_binary_round_trip(tmp_path):
+def test_rdms_binary_round_trip(tmp_path, ref):
     n = 4
     rng = np.random.default_rng(1)
     o, t = rng.standard_normal(n * n), rng.standard_normal(n ** 4)
     f = tmp_path / "rdms.bin"
     mio.write_rdms_binary(f, n, o, t)
     raw = f.read_bytes()
+    ref.write_rdms_binary(tmp_path / "rdms.ref", n, o, t)
+    assert (tmp_path / "rdms.ref").read_bytes() == raw
     assert struct.unpack("i", raw[:4])[0] == n
     assert len(raw) == 4 + 8 * (n * n + n ** 4)
     o2, t2 = mio.read_rdms_binary(f, n)
@@ -141,3 +143,11 @@ def test_rdms_binary_round_trip(tmp_path):
     o5, t5 = mio.read_rdms_binary(f, n)
     assert np.array_equal(o5[:3], o[:3]) and not o5[3:].any()
     assert np.array_equal(t5[:3], o[:3]) and not t5[3:].any()
+    # the reference reader on the same short files
+    for k in (4 + 8 * n * n, 4 + 8 * (n * n + 5), 4 + 8 * 3, len(raw)):
+        f.write_bytes(raw[:k])
+        ours, theirs = mio.read_rdms_binary(f, n), ref.read_rdms_binary(f, n)
+        assert np.array_equal(ours[0], theirs[0])
+        assert np.array_equal(ours[1], theirs[1])
+    with pytest.raises(RuntimeError, match="NORB in RDM file"):
+        ref.read_rdms_binary(f, n + 1)
