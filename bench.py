@@ -69,6 +69,71 @@ def peaks():
         return 6650.0, "fallback"
 
 
+class NvmlClocks:
+    """SM clock and clock-event reasons of the CUDA device, read through NVML
+    every few milliseconds in a thread (reading only: nothing is set), so
+    that a timed region of tens of milliseconds still gets several samples.
+    The device is matched by UUID, which holds under CUDA_VISIBLE_DEVICES."""
+
+    def __init__(self, cuda_index, period_s=0.005):
+        import threading
+
+        import pynvml as nv
+        import torch
+        nv.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(cuda_index).uuid)
+        self.nv = nv
+        self.h = nv.nvmlDeviceGetHandleByUUID(
+            uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        self.smax = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        self.reason_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                                 None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        self.bits = {
+            "hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+            "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+            "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+            "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        self.sm, self.reasons = [], set()
+        self.done = threading.Event()
+        self.period = period_s
+        self.sample()                     # fails here, not in the thread
+        self.t = threading.Thread(target=self.run, daemon=True)
+        self.t.start()
+
+    def sample(self):
+        nv = self.nv
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        r = int(self.reason_fn(self.h))
+        self.reasons.update(k for k, b in self.bits.items() if r & b)
+
+    def run(self):
+        while not self.done.wait(self.period):
+            try:
+                self.sample()
+            except Exception:
+                return
+
+    def stop(self):
+        self.done.set()
+        self.t.join(timeout=5)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.smax,
+                "samples": len(self.sm), "reasons": sorted(self.reasons),
+                "source": "nvml"}
+
+
+def start_clocks(cuda_index):
+    """NVML sampling when the bindings and the driver answer, else the
+    nvidia-smi sampler."""
+    try:
+        return NvmlClocks(cuda_index)
+    except Exception:
+        return Clocks(cuda_index)
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -235,7 +300,7 @@ def run_ours(args, rank, world, local_rank):
         A = build_device()
         del A
     barrier()
-    clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    clocks = start_clocks(torch.cuda.current_device()) if rank == 0 else None
     launches0 = LIB.macis_b200_launch_count()
     step_ms, fill_ms, nnz = [], [], 0
     st = _lib.BuildStatsC()
