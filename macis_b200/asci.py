@@ -153,7 +153,10 @@ def merge_asci_parts(parts, ndets_max, cdets, nbits):
     the parts' (states, scores) ordered by |score| descending then by
     determinant ascending (bitset order, most significant word first), cut
     at ndets_max - ncdets, listed in ascending determinant order, followed by
-    the core determinants in their input order."""
+    the core determinants in their input order. ndets_max - ncdets is size_t
+    arithmetic, as in the search: with fewer slots than core determinants
+    nothing is cut, and a result beyond ndets_max raises ECAPACITY, as the
+    search does."""
     W = nbits // 64
     cdets = _dets(cdets, nbits)
     st = [np.asarray(p[0], dtype=np.uint64).reshape(-1, W) for p in parts]
@@ -161,10 +164,15 @@ def merge_asci_parts(parts, ndets_max, cdets, nbits):
     st = np.concatenate(st) if st else np.zeros((0, W), dtype=np.uint64)
     sc = np.concatenate(sc) if sc else np.zeros(0)
     k = int(ndets_max) - len(cdets)
+    if k < 0:
+        k += 1 << 64   # size_t arithmetic, as the search (determinant_search.hpp:547)
     if len(sc) > k:
         # lexsort: the last key is the primary one
         order = np.lexsort(tuple(st[:, w] for w in range(W)) + (-np.abs(sc),))
         st = st[order[:k]]
+    if len(st) > int(ndets_max):
+        raise _lib.MacisError(_lib.ECAPACITY, "ASCI search result exceeds "
+                              "ndets_max + ncdets determinants")
     if len(st):
         st = st[np.lexsort(tuple(st[:, w] for w in range(W)))]
     return np.concatenate([st, cdets]) if len(cdets) else st

@@ -191,3 +191,25 @@ def test_product_does_not_use_the_oracle():
         if f.endswith(".py"):
             with open(os.path.join(pkg, f)) as fh:
                 assert not pat.search(fh.read()), f
+
+
+def test_merge_asci_parts_topk_rules():
+    """merge_asci_parts: |score| descending then determinant ascending, cut
+    at ndets_max - ncdets (determinant_search.hpp:547, size_t): fewer slots
+    than core determinants cut nothing, and a result beyond ndets_max is
+    refused as by the search."""
+    from macis_b200.asci import merge_asci_parts
+    u = lambda *v: np.array(v, dtype=np.uint64).reshape(-1, 1)
+    parts = [(u(5, 1, 9), np.array([-0.5, -0.2, -0.5])),
+             (u(3, 7), np.array([-0.5, -0.1]))]
+    core = u(200, 100)
+    assert merge_asci_parts(parts, 5, core, 64)[:, 0].tolist() == \
+        [3, 5, 9, 200, 100]
+    assert merge_asci_parts(parts, 4, core, 64)[:, 0].tolist() == \
+        [3, 5, 200, 100]                       # tie at the cut: smaller dets
+    assert merge_asci_parts(parts, 7, core, 64)[:, 0].tolist() == \
+        [1, 3, 5, 7, 9, 200, 100]
+    with pytest.raises(mb.MacisError, match="exceeds ndets_max"):
+        merge_asci_parts(parts, 1, core, 64)    # 1 - 2 wraps: nothing cut
+    empty = [(np.zeros((0, 1), dtype=np.uint64), np.zeros(0))]
+    assert merge_asci_parts(empty, 1, core, 64)[:, 0].tolist() == [200, 100]
