@@ -85,6 +85,50 @@ def _sample_targets(n=1000, seed=3):
     return whole, parts
 
 
+class _FakeNet:
+    """Network stand-in: the samples a part search recorded."""
+    handle = None
+
+    def __init__(self, X, t):
+        self.X, self.t = X, t
+
+    def samples(self):
+        return self.X, self.t
+
+    def set_sample_targets(self, t):
+        self.t = np.asarray(t, dtype=np.float32)
+
+
+def _screened_split(rank, parts_in):
+    import macis_b200 as mb
+    from macis_b200 import asci as masci
+    from macis_b200 import dist as md
+    states, scores, core, ndets_max = parts_in[rank]
+    _, t_parts = _sample_targets()
+    X = np.arange(len(t_parts[rank]) * 3, dtype=np.uint16).reshape(-1, 3)
+    net = _FakeNet(X, t_parts[rank])
+    sc = mb.ScreenSettings(network=net)
+    seen = {}
+
+    def part_search(s, nmax, cd, E, C, norb, H, index, count, screen=None,
+                    use_net=False):
+        seen.update(index=index, count=count, screen=screen, use_net=use_net)
+        return states, scores
+
+    class _Ham:
+        nbits = 64
+    orig = masci.asci_search_part
+    masci.asci_search_part = part_search
+    try:
+        got = md.asci_search(mb.ASCISettings(), ndets_max, core, 0.0,
+                             np.ones(len(core)), 7, _Ham(), screen=sc,
+                             use_net=True)
+    finally:
+        masci.asci_search_part = orig
+    return dict(merged=got, targets=net.t, part=(seen["index"], seen["count"]),
+                passed=(seen["screen"] is sc, seen["use_net"]))
+
+
 def _rank_main(rank, port_no, case, q):
     import datetime
 
@@ -135,6 +179,11 @@ def _rank_main(rank, port_no, case, q):
                                                   core, 64)
             t_whole, t_parts = _sample_targets()
             out["targets"] = md.merge_sample_targets(t_parts[rank])
+            # the whole split search with screening: each rank's part search
+            # (standing in: the oracle parts) records the same sample rows
+            # with its partial targets; every rank ends with the merged
+            # result and the whole search's targets in its network
+            out["screened"] = _screened_split(rank, parts_in)
             # guess reuse is one decision for all ranks: only rank 0 holds
             # a coefficient above 1/N = 0.01 in the first case
             out["reuse"] = (
@@ -245,6 +294,10 @@ def test_split_asci_search_merge_two_ranks(port):
         assert np.array_equal(res[r]["merged"], whole)
     for r in range(WORLD):
         assert res[r]["reuse"] == (True, False)
+        scr = res[r]["screened"]
+        assert scr["part"] == (r, WORLD) and scr["passed"] == (True, True)
+        assert np.array_equal(scr["merged"], whole)
+        assert np.array_equal(scr["targets"], _sample_targets()[0])
     # recorded sample targets: the elementwise maximum over the ranks
     t_whole, _ = _sample_targets()
     for r in range(WORLD):
