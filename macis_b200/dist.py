@@ -104,6 +104,12 @@ class DistCSR:
     def m_local(self):
         return self.hi - self.lo
 
+    @property
+    def device(self):
+        """Where the block's vectors live: this rank's CUDA device."""
+        import torch
+        return torch.device("cuda", torch.cuda.current_device())
+
     def nnz_total(self, device="cpu"):
         return int(reduce_sum(self.local.nnz, self.group, device))
 
@@ -396,7 +402,7 @@ def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
     dets = _host_dets(dets, ham_gen.nbits)
     N = len(dets)
     A = make_dist_csr_hamiltonian(dets, ham_gen, h_el_tol, group=group)
-    dev = torch.device("cuda", torch.cuda.current_device())
+    dev = A.device
     D = A.diagonal(dev)
     ok = C_local is not None and len(C_local) == A.m_local
     if reuse_guess(C_local if ok else None, N, group):
@@ -431,7 +437,8 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
     use_net = _use_net(screen, ham_gen, wfn[:nkeep], E0, X[:nkeep])
     wfn = asci_search(asci_settings, ndets_max, wfn[:nkeep], E0, X[:nkeep],
                       norb, ham_gen, group, screen=screen, use_net=use_net)
-    _train_after_search(screen, last_search_stats(ham_gen))
+    if screen is not None:
+        _train_after_search(screen, last_search_stats(ham_gen))
     E, X_local = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,
                                   mcscf_settings.ci_max_subspace,
                                   mcscf_settings.ci_res_tol, None, group)

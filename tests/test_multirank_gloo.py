@@ -85,6 +85,61 @@ def _sample_targets(n=1000, seed=3):
     return whole, parts
 
 
+class _FakeBlock:
+    """A rank's H block on the CPU (the oracle's rows) in place of DistCSR."""
+
+    def __init__(self, md, lo, hi, N, D, mv):
+        import torch
+        self.md, self.lo, self.hi, self.N = md, lo, hi, N
+        self.D, self.mv = torch.from_numpy(D), mv
+        self.device = torch.device("cpu")
+        self.m_local = hi - lo
+
+    def diagonal(self, device=None):
+        return self.D
+
+    def operator(self):
+        return self.md.RowBlockOperator(self.mv, self.N)
+
+
+class _Ham64:
+    nbits = 64
+
+
+def _dist_iter(md, dets, lo, hi, rp, ci, nz, mv):
+    """dist.asci_iter's host flow on the CPU: reorder, the search (standing
+    in: returns the whole space, records what it was given), the
+    distributed solve over the rank's oracle block, the gathered vector."""
+    import macis_b200 as mb
+    N = len(dets)
+    D = np.empty(hi - lo)
+    rows = np.repeat(np.arange(hi - lo), np.diff(rp))
+    on = ci == rows + lo
+    D[rows[on]] = nz[on]
+    seen = {}
+
+    def search(s, nmax, cd, E, C, norb, H, group=None, screen=None,
+               use_net=False):
+        seen.update(cd=np.array(cd), C=np.array(C), nmax=nmax)
+        return dets
+
+    def build(d, H, tol, group=None):
+        assert len(d) == N and tol == np.finfo(float).eps
+        return _FakeBlock(md, lo, hi, N, D, mv)
+    saved = md.asci_search, md.make_dist_csr_hamiltonian
+    md.asci_search, md.make_dist_csr_hamiltonian = search, build
+    try:
+        s = mb.ASCISettings()
+        s.ncdets_max = 20
+        m = mb.MCSCFSettings()
+        m.ci_max_subspace = 200
+        X0 = np.random.default_rng(5).standard_normal(50)
+        E, wfn, X = md.asci_iter(s, m, N, -1.0, dets[:50], X0, _Ham64(), 7)
+    finally:
+        md.asci_search, md.make_dist_csr_hamiltonian = saved
+    return dict(E=E, X=X, nwfn=len(wfn), seen=seen)
+
+
 class _FakeNet:
     """Network stand-in: the samples a part search recorded."""
     handle = None
@@ -172,6 +227,8 @@ def _rank_main(rank, port_no, case, q):
                                   1e-8, X)
             out.update(it=it, E=E, X=md.allgather_rows(X, N).numpy(),
                        guess=g)
+        elif case == "dist_iter":
+            out.update(_dist_iter(md, dets, lo, hi, rp, ci, nz, mv))
         elif case == "asci":
             parts_in, _ = _asci_parts(port)
             states, scores, core, ndets_max = parts_in[rank]
@@ -303,3 +360,30 @@ def test_split_asci_search_merge_two_ranks(port):
     for r in range(WORLD):
         assert res[r]["targets"].dtype == np.float32
         assert np.array_equal(res[r]["targets"], t_whole)
+
+
+def test_dist_asci_iter_two_ranks(port):
+    """dist.asci_iter over two gloo ranks (the search and the H blocks stood
+    in on the CPU): the search gets the ncdets_max largest |C| in order, the
+    distributed solve with the p_diagonal_guess start matches the serial
+    Davidson, and every rank holds the same gathered eigenvector."""
+    res = _run("dist_iter")
+    T, V, dets = _problem()
+    X0 = np.random.default_rng(5).standard_normal(50)
+    order = np.argsort(-np.abs(X0), kind="stable")[:20]
+    rp, ci, nz = port.build_csr(port.ham(64, 7, T, V), dets, dets,
+                                np.finfo(float).eps)
+    rows = np.repeat(np.arange(len(dets)), np.diff(rp))
+    D = nz[ci == rows]
+    G = np.zeros(len(dets))
+    G[int(np.argmin(D))] = 1.0
+    E, it, X = port.davidson(rp, ci, nz, 200, 1e-8, G)
+    for r in range(WORLD):
+        o = res[r]
+        assert np.array_equal(o["seen"]["cd"], dets[:50][order])
+        assert np.array_equal(o["seen"]["C"], X0[order])
+        assert o["seen"]["nmax"] == len(dets) and o["nwfn"] == len(dets)
+        assert o["E"] == res[0]["E"] and abs(o["E"] - E) < 1e-9
+        assert np.array_equal(o["X"], res[0]["X"])
+        assert abs(abs(o["X"] @ X) / (np.linalg.norm(o["X"]) *
+                                      np.linalg.norm(X)) - 1.0) < 1e-10
