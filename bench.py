@@ -36,6 +36,9 @@ METRIC = ("ASCI time & H-build nnz/s: learned+mixed vs plain FP64, one GPU, "
 WORKLOAD = ("CAS(12e,12o) full-CI CSR Hamiltonian build: 853,776 dets "
             "(bitset<64>), synthetic integrals seed 0, FP64 values, int32 "
             "indices, |h| > DBL_EPSILON")
+DATA = ("synthetic: seeded integrals (seed 0; orbital energies on a ramp, "
+        "N(0, 0.02^2) off-diagonal one-body terms, two-body terms as sums of "
+        "products of symmetric random factors), no dataset")
 NORB, NA, NB, SEED = 12, 6, 6, 0
 THRESH = float(np.finfo(np.float64).eps)
 
@@ -247,7 +250,7 @@ def run_reference(args, rank, world):
            "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
            "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic (seeded integrals, BASELINE recipe)",
+           "data": DATA,
            "config": {"workload": WORKLOAD, "sample_rows": rows},
            "cpu_baseline": {"value": value, "unit": "nnz/s",
                             "cores": nthreads, "kind": "reference",
@@ -342,7 +345,7 @@ def run_ours(args, rank, world, local_rank):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded integrals, BASELINE recipe, seed 0)",
+            "data": DATA,
             "config": {"workload": WORKLOAD, "ndets": N, "nnz": int(nnz_all),
                        "rows_per_rank": hi - lo, "direct_product_path": direct,
                        "l2": "256 MB flush between steps; output 18.6 GB > L2",
