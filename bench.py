@@ -57,6 +57,53 @@ def c2_inputs():
     return T, V, dets
 
 
+def c2_inputs_reference(R):
+    """The same workload for the reference arm without importing the package
+    (whose import loads the CUDA library): the integral recipe from
+    macis_b200/integrals.py loaded by path (numpy only), the determinant list
+    from the reference's own generate_hilbert_space<64>."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "macis_b200_integrals", os.path.join(ROOT, "macis_b200", "integrals.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    T, V = mod.synthetic_integrals(NORB, SEED)
+    return T, V, R.hilbert_space(64, NORB, NA, NB)
+
+
+def bench_config(ndets, world):
+    """`config` of both arms (the workload, not how either arm samples it)."""
+    return {"workload": WORKLOAD, "ndets": ndets,
+            "l2": "256 MB flush between steps; output 18.6 GB > L2",
+            "parallelism": f"row-block x{world}"}
+
+
+def sample_blocks(N, rows, nblocks=32):
+    """`nblocks` row blocks of about rows / nblocks rows each, spread evenly
+    over the N rows (a sample of the whole matrix, not of its first rows)."""
+    nblocks = max(1, min(nblocks, rows))
+    b = max(1, rows // nblocks)
+    starts = np.linspace(0, N - b, nblocks).astype(np.int64)
+    return [(int(r), int(r) + b) for r in starts]
+
+
+def _bra_of(dets, blocks):
+    return np.ascontiguousarray(np.concatenate([dets[a:b] for a, b in blocks]))
+
+
+def reference_sample(R, h, dets, target_s, nthreads):
+    """Row blocks whose reference build takes about target_s seconds on
+    nthreads threads (probed on a small sample)."""
+    N = len(dets)
+    probe = sample_blocks(N, max(512, 64 * nthreads), 16)
+    bra = _bra_of(dets, probe)
+    t = time.perf_counter()
+    R.csr(h, bra, dets, THRESH, nthreads=nthreads)
+    per_row = (time.perf_counter() - t) / len(bra)
+    rows = int(min(N, max(len(bra), target_s / max(per_row, 1e-9))))
+    return sample_blocks(N, rows)
+
+
 def alg_bytes(nnz, nrows, nbra, nket, idx_b=4, val_b=8, det_b=8):
     """Algorithmic bytes of one build: CSR written once, dets read once."""
     return nnz * (idx_b + val_b) + (nrows + 1) * idx_b + (nbra + nket) * det_b
@@ -186,28 +233,51 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def cpu_reference_rate(T, V, dets, target_s=12.0, nthreads=None):
+def cpu_reference_rate(T, V, dets, target_s=10.0, nthreads=None):
     """Reference MACIS (compiled oracle/_ref) H build over a bounded sample of
-    rows, all host threads: nnz/s."""
+    rows spread over the matrix, all host threads: nnz/s. Also returns the
+    sample's row blocks and its CSR arrays for the parity check of the
+    device-built matrix."""
     import oracle
     R = oracle.ref()
     nthreads = nthreads or os.cpu_count() or 1
     R.set_threads(1)
     h = R.ham(64, NORB, T, V)
-    rows = max(nthreads * 4, 64)
+    blocks = reference_sample(R, h, dets, target_s, nthreads)
+    bra = _bra_of(dets, blocks)
     t = time.perf_counter()
-    A = R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
+    A = R.csr(h, bra, dets, THRESH, nthreads=nthreads)
     dt = time.perf_counter() - t
-    per_row = dt / rows
-    rows = int(min(len(dets), max(rows, target_s / max(per_row, 1e-9))))
-    t = time.perf_counter()
-    A = R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
-    dt = time.perf_counter() - t
-    return {"value": A.nnz / dt, "unit": "nnz/s", "cores": nthreads,
-            "kind": "reference", "rows": rows, "seconds": dt, "nnz": A.nnz,
-            "sample": f"reference DoubleLoop make_csr_hamiltonian_block on "
-                      f"rows [0,{rows}) x all {len(dets)} kets of the same "
-                      f"matrix, {nthreads} threads over row blocks"}
+    out = {"value": A.nnz / dt, "unit": "nnz/s", "cores": nthreads,
+           "kind": "reference", "rows": len(bra), "seconds": dt, "nnz": A.nnz,
+           "sample": f"reference DoubleLoop make_csr_hamiltonian_block on "
+                     f"{len(bra)} rows ({len(blocks)} row blocks spread over "
+                     f"the {len(dets)} rows) x all {len(dets)} kets of the "
+                     f"same matrix, {nthreads} threads over row blocks (the "
+                     f"reference build loop itself is single-threaded)"}
+    return out, blocks, A.arrays()
+
+
+def csr_parity(A, blocks, ref_arrays):
+    """The device-built matrix's rows of the sampled blocks against the
+    reference's CSR of the same rows: rowptr, colind and nzval bit for bit."""
+    rr, rc, rz = ref_arrays
+    off, exact, nnz = 0, True, 0
+    for a, b in blocks:
+        rp, ci, nz = A.rows(a, b)
+        lo, hi = int(rr[off]), int(rr[off + b - a])
+        exact &= bool(np.array_equal(rp.astype(np.int64),
+                                     rr[off:off + b - a + 1].astype(np.int64) - lo))
+        exact &= bool(np.array_equal(ci.astype(np.int64),
+                                     rc[lo:hi].astype(np.int64)))
+        exact &= bool(np.array_equal(nz, rz[lo:hi]))
+        nnz += hi - lo
+        off += b - a
+    return {"rows": off, "blocks": len(blocks), "nnz": nnz,
+            "bit_exact": exact,
+            "against": "compiled reference make_csr_hamiltonian_block "
+                       "(DoubleLoopHamiltonianGenerator), the cpu_baseline "
+                       "sample's rows"}
 
 
 # ---------------------------------------------------------------- reference
@@ -220,28 +290,28 @@ def run_reference(args, rank, world):
                           "compiled reference oracle/_ref/libmacis_ref.so "
                           "missing"}))
         return 0
-    T, V, dets = c2_inputs()
     nthreads = os.cpu_count() or 1
     R = oracle.ref()
     R.set_threads(1)
+    T, V, dets = c2_inputs_reference(R)
     h = R.ham(64, NORB, T, V)
-    # size each step to about 6 s of host work
-    probe = max(64, 4 * nthreads)
-    t = time.perf_counter()
-    R.csr(h, dets[:probe], dets, THRESH, nthreads=nthreads)
-    per_row = (time.perf_counter() - t) / probe
-    rows = int(min(len(dets), max(probe, 6.0 / max(per_row, 1e-9))))
+    # each step about 5 s of host work: the whole --steps/--warmup run stays
+    # within a few minutes
+    blocks = reference_sample(R, h, dets, 5.0, nthreads)
+    bra = _bra_of(dets, blocks)
     for _ in range(args.warmup):
-        R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
+        R.csr(h, bra, dets, THRESH, nthreads=nthreads)
     times, nnz = [], 0
     for _ in range(args.steps):
         t = time.perf_counter()
-        A = R.csr(h, dets[:rows], dets, THRESH, nthreads=nthreads)
+        A = R.csr(h, bra, dets, THRESH, nthreads=nthreads)
         times.append(time.perf_counter() - t)
         nnz = A.nnz
+        del A
     tot = sum(times)
     value = nnz * len(times) / tot
-    sample = (f"rows [0,{rows}) of the {len(dets)}-row matrix per step "
+    sample = (f"{len(bra)} rows per step ({len(blocks)} row blocks spread "
+              f"over the {len(dets)}-row matrix) x all {len(dets)} kets "
               f"(DoubleLoopHamiltonianGenerator via make_csr_hamiltonian_block,"
               f" {nthreads} threads over row blocks; the reference build loop "
               f"itself is single-threaded)")
@@ -251,7 +321,8 @@ def run_reference(args, rank, world):
            "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f64",
            "data": DATA,
-           "config": {"workload": WORKLOAD, "sample_rows": rows},
+           "config": bench_config(len(dets), world),
+           "sample_rows": len(bra),
            "cpu_baseline": {"value": value, "unit": "nnz/s",
                             "cores": nthreads, "kind": "reference",
                             "sample": sample},
@@ -346,10 +417,9 @@ def run_ours(args, rank, world, local_rank):
             "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": DATA,
-            "config": {"workload": WORKLOAD, "ndets": N, "nnz": int(nnz_all),
-                       "rows_per_rank": hi - lo, "direct_product_path": direct,
-                       "l2": "256 MB flush between steps; output 18.6 GB > L2",
-                       "parallelism": f"row-block x{world}"},
+            "config": bench_config(N, world),
+            "matrix": {"nnz": int(nnz_all), "rows_per_rank": hi - lo,
+                       "direct_product_path": direct},
             "clocks": ck,
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "dp_fill_k",
@@ -370,7 +440,11 @@ def run_ours(args, rank, world, local_rank):
             res["extras"] = extras(mb, H, dets, torch)
         if world == 1 and not args.no_cpu:
             try:
-                res["cpu_baseline"] = cpu_reference_rate(T, V, dets)
+                res["cpu_baseline"], blocks, ref_arrays = cpu_reference_rate(
+                    T, V, dets)
+                A = build_device()
+                res["parity"] = csr_parity(A, blocks, ref_arrays)
+                del A, ref_arrays
             except Exception as e:  # noqa: BLE001
                 res["cpu_baseline"] = {"unavailable": str(e)}
         print(json.dumps(res))

@@ -3,7 +3,7 @@
  * Plain pointers and sizes only. Each entry point names the reference MACIS
  * interface it replaces (paths relative to the MACIS source tree). The C++
  * drop-in shim include/macis_b200/macis_b200.hpp wraps these calls behind
- * the reference's own template API; INTEGRATION.md shows the bindings.
+ * the reference's own template API.
  *
  * Determinants: arrays of little-endian uint64 words, nbits/64 words per
  * determinant, in the std::bitset<nbits> layout (nbits = 64, 128 or 256):
@@ -145,6 +145,14 @@ int macis_b200_csr_info(const macis_b200_csr* A, int64_t* m, int64_t* n,
  * NULL to skip that array. */
 int macis_b200_csr_download(const macis_b200_csr* A, void* rowptr,
                             void* colind, void* nzval, unsigned flags);
+/* Copy rows [r0, r1) out: rowptr gets the r1 - r0 + 1 stored offsets
+ * rowptr[r0..r1] (absolute, as in the whole matrix), colind and nzval the
+ * entries rowptr[r0] .. rowptr[r1] - 1. The row block that
+ * make_dist_csr_hamiltonian gives one rank (csr_hamiltonian.hpp:49-82),
+ * read out of a matrix built whole. Any pointer may be NULL. */
+int macis_b200_csr_download_rows(const macis_b200_csr* A, int64_t r0,
+                                 int64_t r1, void* rowptr, void* colind,
+                                 void* nzval, unsigned flags);
 /* Diagonal of the matrix, FP64 (sparsexx/util/submatrix.hpp:264-292). */
 int macis_b200_csr_diagonal(const macis_b200_csr* A, double* D,
                             unsigned flags);

@@ -83,6 +83,8 @@ _SIGS = {
                                       C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "macis_b200_csr_download": (C.c_int, [_vp, _vp, _vp, _vp, C.c_uint]),
+    "macis_b200_csr_download_rows": (C.c_int, [_vp, C.c_int64, C.c_int64,
+                                               _vp, _vp, _vp, C.c_uint]),
     "macis_b200_csr_diagonal": (C.c_int, [_vp, _vp, C.c_uint]),
     "macis_b200_spmv": (C.c_int, [_vp, C.c_int64, C.c_double, _vp, C.c_int64,
                                   C.c_double, _vp, C.c_int64, C.c_uint]),

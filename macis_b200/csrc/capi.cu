@@ -199,6 +199,42 @@ int macis_b200_csr_download(const macis_b200_csr* A, void* rowptr,
   });
 }
 
+int macis_b200_csr_download_rows(const macis_b200_csr* A, int64_t r0,
+                                 int64_t r1, void* rowptr, void* colind,
+                                 void* nzval, unsigned flags) {
+  return guarded([&] {
+    MB_REQUIRE(A, MACIS_B200_EINVAL, "null handle");
+    MB_REQUIRE(0 <= r0 && r0 <= r1 && r1 <= A->m, MACIS_B200_EINVAL,
+               "row range outside the matrix");
+    const cudaMemcpyKind k = (flags & MACIS_B200_DEVICE_PTRS)
+                                 ? cudaMemcpyDeviceToDevice
+                                 : cudaMemcpyDeviceToHost;
+    const size_t ib = size_t(A->idx_bytes);
+    // the two bounding row offsets, as stored (int32 or int64)
+    int64_t lo = 0, hi = 0;
+    MB_CUDA(cudaMemcpyAsync(&lo, static_cast<char*>(A->rowptr) + r0 * ib, ib,
+                            cudaMemcpyDeviceToHost, A->stream));
+    MB_CUDA(cudaMemcpyAsync(&hi, static_cast<char*>(A->rowptr) + r1 * ib, ib,
+                            cudaMemcpyDeviceToHost, A->stream));
+    MB_CUDA(cudaStreamSynchronize(A->stream));
+    if(ib == 4) {  // little-endian: the low word holds the int32 value
+      lo = int64_t(int32_t(uint32_t(lo)));
+      hi = int64_t(int32_t(uint32_t(hi)));
+    }
+    if(rowptr)
+      MB_CUDA(cudaMemcpyAsync(rowptr, static_cast<char*>(A->rowptr) + r0 * ib,
+                              size_t(r1 - r0 + 1) * ib, k, A->stream));
+    if(colind && hi > lo)
+      MB_CUDA(cudaMemcpyAsync(colind, static_cast<char*>(A->colind) + lo * ib,
+                              size_t(hi - lo) * ib, k, A->stream));
+    if(nzval && hi > lo)
+      MB_CUDA(cudaMemcpyAsync(
+          nzval, static_cast<char*>(A->nzval) + lo * A->val_bytes,
+          size_t(hi - lo) * A->val_bytes, k, A->stream));
+    MB_CUDA(cudaStreamSynchronize(A->stream));
+  });
+}
+
 int macis_b200_csr_diagonal(const macis_b200_csr* A, double* D,
                             unsigned flags) {
   return guarded([&] {

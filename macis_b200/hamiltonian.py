@@ -182,6 +182,22 @@ class DeviceCSR:
                                           ci.ctypes.data, nz.ctypes.data, 0))
         return rp, ci[:self.nnz], nz[:self.nnz]
 
+    def rows(self, r0, r1):
+        """(rowptr, colind, nzval) of rows [r0, r1) as numpy arrays, rowptr
+        rebased to start at 0 (the local CSR of that row block)."""
+        if not 0 <= r0 <= r1 <= self.m:
+            raise ValueError("row range outside the matrix")
+        rp = np.empty(r1 - r0 + 1, dtype=self.index_t)
+        check(LIB.macis_b200_csr_download_rows(self._c, r0, r1, rp.ctypes.data,
+                                               None, None, 0))
+        k = int(rp[-1] - rp[0])
+        ci = np.empty(max(k, 1), dtype=self.index_t)
+        nz = np.empty(max(k, 1), dtype=self.value_t)
+        check(LIB.macis_b200_csr_download_rows(self._c, r0, r1, None,
+                                               ci.ctypes.data, nz.ctypes.data,
+                                               0))
+        return rp - rp[0], ci[:k], nz[:k]
+
     def diagonal(self):
         """extract_diagonal_elements (sparsexx/util/submatrix.hpp:264-292)."""
         d = np.empty(self.m)

@@ -31,3 +31,43 @@ def assert_csr_equal(a, b, exact=True):
                               np.asarray(zb, np.float64))
     else:
         np.testing.assert_allclose(za, zb, rtol=1e-12, atol=1e-14)
+
+
+def core_set(norb, nel, ncore, nbits=128, seed=0, nalpha=60, top=30):
+    """A core set shaped like the ASCI core of a large active space: the HF
+    determinant of `nel` alpha and `nel` beta electrons in `norb` orbitals
+    and products of its low single / double excitations, ordered by total
+    excitation degree, with decaying normalised coefficients. Returns
+    (dets, C)."""
+    rng = np.random.default_rng(seed)
+    hf = (1 << nel) - 1
+    strings = {hf}
+    while len(strings) < nalpha:
+        a = hf
+        for _ in range(int(rng.integers(1, 3))):
+            i, v = int(rng.integers(0, nel)), int(rng.integers(nel, norb))
+            if a >> i & 1 and not a >> v & 1:
+                a ^= (1 << i) ^ (1 << v)
+        strings.add(a)
+    strings = sorted(strings, key=lambda x: (bin(x ^ hf).count("1"), x))
+    deg = lambda ab: (bin(ab[0] ^ hf).count("1") + bin(ab[1] ^ hf).count("1"),
+                      ab)
+    pairs = sorted(((a, b) for a in strings[:top] for b in strings[:top]),
+                   key=deg)[:ncore]
+    dets = make_dets([a for a, _ in pairs], [b for _, b in pairs], nbits)
+    C = np.exp(-0.5 * np.arange(len(dets)) / 10.0)
+    return dets, C / np.linalg.norm(C)
+
+
+def abs_sums(states, rv):
+    """Unique states of a raw contribution list in ascending bitset order
+    (the order of sort_and_accumulate_asci_pairs) and, per state, the sum of
+    |rv| over its contributions: the scale of the rounding error of any
+    summation order of that state's score."""
+    nw = states.shape[1]
+    order = np.lexsort(tuple(states[:, w] for w in range(nw)))
+    s, a = states[order], np.abs(rv[order])
+    new = np.ones(len(s), dtype=bool)
+    new[1:] = np.any(s[1:] != s[:-1], axis=1)
+    idx = np.flatnonzero(new)
+    return s[idx], np.add.reduceat(a, idx) if len(a) else a
