@@ -438,6 +438,11 @@ def run_ours(args, rank, world, local_rank):
         res["e2e"] = e2e
         if world == 1 and not args.no_extras:
             res["extras"] = extras(mb, H, dets, torch)
+        if world == 1 and not args.no_asci:
+            try:
+                res["asci"] = asci_iteration(mb, peaks()[0])
+            except Exception as e:  # noqa: BLE001
+                res["asci"] = {"error": str(e)}
         if world == 1 and not args.no_cpu:
             try:
                 res["cpu_baseline"], blocks, ref_arrays = cpu_reference_rate(
@@ -529,43 +534,57 @@ def extras(mb, H, dets, torch):
         out[f"spmv_{prec}"] = {"ms": ms, "GBps": B / ms / 1e6,
                                "frac_of_measured_hbm": B / ms / 1e6 / peak,
                                "nnz": A.nnz}
+        if prec == "fp64":
+            # warm-up solve: the timed solves below run warm
+            try:
+                mb.davidson(N, 40, mb.SparseMatrixOperator(A), None, 1e-8,
+                            np.zeros(N), use_guess=False, restart_keep=8,
+                            max_iter=3000)
+            except RuntimeError:
+                pass
         X = np.zeros(N)
         t = time.perf_counter()
         try:
             it, E = mb.davidson(N, 40, mb.SparseMatrixOperator(A), None, 1e-8,
                                 X, use_guess=False, restart_keep=8,
                                 max_iter=3000)
-            out[f"davidson_{prec}"] = {"seconds": time.perf_counter() - t,
-                                       "iterations": it, "E0": E,
-                                       "max_m": 40, "restart_keep": 8,
-                                       "tol": 1e-8}
+            secs = time.perf_counter() - t
+            ds = mb.davidson_stats()
+            vec_ms = ds["rayleigh_ms"] + ds["residual_ms"] + ds["ortho_ms"]
+            out[f"davidson_{prec}"] = {
+                "seconds": secs, "iterations": it, "E0": E, "max_m": 40,
+                "restart_keep": 8, "tol": 1e-8,
+                "device_ms": {k: ds[k] for k in ("apply_ms", "rayleigh_ms",
+                                                 "residual_ms", "ortho_ms")},
+                "host_ms": ds["wall_ms"] - ds["apply_ms"] - vec_ms,
+                "vector_kernels": {
+                    "GBps": ds["vector_bytes"] / max(vec_ms, 1e-9) / 1e6,
+                    "frac_of_measured_hbm": ds["vector_bytes"] / max(
+                        vec_ms, 1e-9) / 1e6 / peak,
+                    "alg_bytes": ds["vector_bytes"],
+                    "basis": "multi-dot, Ritz/residual and CGS2 kernels: "
+                             "every V / AV column read once per pass"}}
         except RuntimeError as e:
             out[f"davidson_{prec}"] = {"error": str(e)}
         del A
     if "E0" in out.get("davidson_fp64", {}) and "E0" in out.get("davidson_mixed", {}):
         out["mixed_dE_Eh"] = out["davidson_mixed"]["E0"] - out["davidson_fp64"]["E0"]
-    try:
-        out["asci_search_n48"] = asci_extra(mb)
-    except Exception as e:  # noqa: BLE001
-        out["asci_search_n48"] = {"error": str(e)}
-    try:
-        out["asci_screened_n48"] = screen_extra(mb)
-    except Exception as e:  # noqa: BLE001
-        out["asci_screened_n48"] = {"error": str(e)}
     return out
 
 
 def _n48_core(mb, ncore, seed=0):
-    """n = 48 orbitals, 12 alpha / 12 beta, bitset<128>: HF plus its lowest
-    singles / doubles as the core set with decaying coefficients
+    """n = 48 orbitals, 12 alpha / 12 beta, bitset<128>: HF plus products of
+    its low single / double alpha and beta excitations, ordered by total
+    excitation degree, as the core set, with decaying coefficients
     (C3-shaped)."""
     n, k = 48, 12
     T, V = mb.synthetic_integrals(n, seed)
     H = mb.HamiltonianGenerator(T, V, 128)
     rng = np.random.default_rng(seed)
+    top = max(200, int(np.ceil(np.sqrt(ncore))) + 8)
     hf = (1 << k) - 1
     alphas = {hf}
-    while len(alphas) < 400:
+    while len(alphas) < 2 * top:
         a = hf
         for _ in range(rng.integers(1, 3)):
             i = int(rng.integers(0, k))
@@ -574,7 +593,7 @@ def _n48_core(mb, ncore, seed=0):
                 a ^= (1 << i) ^ (1 << v)
         alphas.add(a)
     alphas = sorted(alphas, key=lambda x: bin(x ^ hf).count("1"))
-    pairs = [(a, b) for a in alphas[:200] for b in alphas[:200]]
+    pairs = [(a, b) for a in alphas[:top] for b in alphas[:top]]
     pairs.sort(key=lambda ab: bin(ab[0] ^ hf).count("1") + bin(ab[1] ^ hf).count("1"))
     pairs = pairs[:ncore]
     core = mb.sd.make_dets([a for a, _ in pairs], [b for _, b in pairs], 128)
@@ -584,75 +603,170 @@ def _n48_core(mb, ncore, seed=0):
     return n, H, core, C, hd - 0.5
 
 
-def asci_extra(mb, ncore=10000, ndets_max=1000000, seed=0):
-    """One exact FP64 asci_search on the n = 48 core set."""
-    n, H, core, C, E0 = _n48_core(mb, ncore, seed)
-    s = mb.ASCISettings()
-    # a warm-up search of the same size grows the memory pool, as the
-    # previous iteration of a refine loop would
-    mb.asci_search(s, ndets_max, core, E0, C, n, H)
-    t = time.perf_counter()
-    out = mb.asci_search(s, ndets_max, core, E0, C, n, H)
-    dt = time.perf_counter() - t
-    st = mb.last_search_stats(H)
-    return {"seconds": dt, "ncdets": len(core), "ndets_max": ndets_max,
-            "returned": len(out), "raw_pairs": st["raw_pairs"],
-            "unique_pairs": st["unique_pairs"], "batches": st["batches"],
-            "raw_pairs_per_s": st["raw_pairs"] / dt,
-            "phase_ms": {k2: st[k2] for k2 in ("pairs_ms", "sort_ms",
-                                               "keep_ms", "topk_ms")}}
+def asci_rooflines(st, nbits, peak):
+    """HBM rooflines of the exact search's two dominant phases from its
+    statistics: contribution generation (units_k count and fill passes:
+    every raw record written once) and the candidate sort (lower bound: one
+    read and one write of every record; per pass: the digit passes run)."""
+    rec = 8 * (nbits // 64) + 8
+    gen_b = st["raw_pairs"] * rec
+    gen = gen_b / (st["pairs_ms"] * 1e-3) / 1e9
+    lb_b = 2 * st["raw_pairs"] * rec
+    pass_b = 2 * st["sort_pass_items"] * rec
+    sort_lb = lb_b / (st["sort_ms"] * 1e-3) / 1e9
+    sort_pass = pass_b / (st["sort_ms"] * 1e-3) / 1e9
+    return {
+        "units_k": {"bound": "hbm", "achieved": gen, "peak": peak,
+                    "unit": "GB/s", "frac": gen / peak,
+                    "alg_bytes": gen_b, "ms": st["pairs_ms"],
+                    "basis": f"raw contributions x {rec} B written, over the "
+                             "count + generation passes"},
+        "sort": {"bound": "hbm", "achieved": sort_lb, "peak": peak,
+                 "unit": "GB/s", "frac": sort_lb / peak, "alg_bytes": lb_b,
+                 "ms": st["sort_ms"],
+                 "per_pass_GBps": sort_pass, "per_pass_frac": sort_pass / peak,
+                 "digit_passes": st["sort_pass_items"] / max(st["raw_pairs"], 1),
+                 "basis": "lower bound 2 x raw contributions x record (one "
+                          "read + one write); per pass: 2 x record x records "
+                          "per digit pass, summed over passes"}}
 
 
-def screen_extra(mb, ncore=10000, ndets_max=1000000, seed=0, keep=0.2,
-                 batch=None, lr=None, epochs=None):
-    """Learned screening on the n = 48 core set: the network is trained on
-    the exact search over the leading ncore/4 core dets (the previous
-    iteration's data), then the search over all ncore dets runs exact and
-    screened (top `keep` of the units). Reports both times, the training
-    time, top-k recall of the screened selection and the network forward
-    throughput (tensor-pipe work)."""
+def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
+                   cpu_ncore=50, cpu_ndets=20000):
+    """One C3-shaped ASCI iteration (asci_iter, iteration.hpp:17-68) both
+    ways on n = 48, 12 alpha / 12 beta, bitset<128>: `ncore` core
+    determinants -> `ndets` determinants -> rediagonalisation.
+
+    exact_fp64: the exact asci_search, then the FP64 CSR H and Davidson.
+    learned_mixed: the network trained (timed) on the samples the previous
+    iteration's search recorded (a recording search over the leading
+    ncore / 4 core determinants, not timed), the screened search (top 20 %
+    of the units by prediction plus 2 % random), then the FP32-H CSR and
+    the mixed-precision Davidson (FP64 residual, CGS2, Rayleigh-Ritz).
+    dE = E(learned_mixed) - E(exact_fp64) at equal determinant count; the
+    learned run's wavefunction is also evaluated with the FP64 H.
+    cpu_baseline: the compiled reference asci_search (serial,
+    determinant_search.hpp:395-663) and the GPU search on a matched small
+    core set."""
+    from macis_b200.solvers import FP64, MIXED
     n, H, core, C, E0 = _n48_core(mb, ncore, seed)
     s = mb.ASCISettings()
-    net = mb.ScreeningNetwork(nbits=128, seed=seed)
-    scr = mb.ScreenSettings(network=net, max_samples=1000000)
-    scr.batch = batch or scr.batch
-    scr.lr = lr or scr.lr
-    scr.epochs = epochs or scr.epochs
-    nprev = max(1, ncore // 4)
-    mb.asci_search(s, ndets_max // 4, core[:nprev], E0, C[:nprev], n, H,
-                   screen=scr)
-    st_p = mb.last_search_stats(H)
-    t = time.perf_counter()
-    net.clamp_samples(scr.clamp_quantile)
-    loss = net.train(None, None, scr.epochs, scr.batch, scr.lr, seed)
-    t_train = time.perf_counter() - t
-    t = time.perf_counter()
-    exact = mb.asci_search(s, ndets_max, core, E0, C, n, H)
-    t_exact = time.perf_counter() - t
+    dav = dict(restart_keep=8, max_iter=4000)
+    # warm-up: a search of the same size grows the memory pool, as the
+    # previous iteration of a refine loop would; a small solve loads the
+    # solver kernels
+    warm = mb.asci_search(s, ndets, core, E0, C, n, H)
+    mb.selected_ci_diag(warm[:20000], H, THRESH, 40, 1e-8, **dav)
+    mb.selected_ci_diag(warm[:20000], H, THRESH, 40, 1e-8, precision=MIXED,
+                        **dav)
+    del warm
+    # exact search + FP64
+    t0 = time.perf_counter()
+    dets_e = mb.asci_search(s, ndets, core, E0, C, n, H)
+    t_se = time.perf_counter() - t0
     st_e = mb.last_search_stats(H)
-    sc = mb.ScreenSettings(network=net, keep_frac=keep, explore_frac=0.0,
-                           train=False)
-    mb.asci_search(s, ndets_max, core, E0, C, n, H, screen=sc, use_net=True)
-    t = time.perf_counter()
-    scrd = mb.asci_search(s, ndets_max, core, E0, C, n, H, screen=sc,
-                          use_net=True)
-    t_scr = time.perf_counter() - t
-    st_s = mb.last_search_stats(H)
-    ea = set(map(bytes, exact))
-    recall = sum(1 for d in scrd if bytes(d) in ea) / max(len(exact), 1)
-    din = mb.unit_width(128)
-    flop = 2.0 * (din * 256 + 256 * 256 + 256) * st_s["units_total"]
-    return {"ncdets": len(core), "ndets_max": ndets_max, "keep_frac": keep,
-            "batch": scr.batch, "lr": scr.lr, "epochs": scr.epochs,
-            "train_samples": st_p["samples"],
-            "exact_s": t_exact, "screened_s": t_scr, "train_s": t_train,
-            "train_loss": loss, "speedup_search": t_exact / t_scr,
-            "topk_recall": recall,
-            "units": [st_s["units_kept"], st_s["units_total"]],
-            "raw_pairs": [st_s["raw_pairs"], st_e["raw_pairs"]],
-            "predict_ms": st_s["predict_ms"],
-            "predict_tflops": flop / (st_s["predict_ms"] * 1e-3) / 1e12,
-            "screen_ms": st_s["screen_ms"]}
+    te = {}
+    E_e, X_e = mb.selected_ci_diag(dets_e, H, THRESH, 40, 1e-8,
+                                   precision=FP64, timings=te, **dav)
+    t_exact = time.perf_counter() - t0
+    del X_e
+    # learned: the previous iteration's recording search (untimed)
+    nprev = max(1, ncore // 4)
+    net = mb.ScreeningNetwork(nbits=128, seed=seed)
+    rec = mb.ScreenSettings(network=net, max_samples=1000000)
+    mb.asci_search(s, ndets // 4, core[:nprev], E0, C[:nprev], n, H,
+                   screen=rec)
+    sc = mb.ScreenSettings(network=net, keep_frac=0.2, explore_frac=0.02,
+                           train=False, seed=seed)
+    mb.asci_search(s, 1000, core[:200], E0, C[:200], n, H, screen=sc,
+                   use_net=True)                  # loads the network kernels
+    t0 = time.perf_counter()
+    net.clamp_samples(rec.clamp_quantile)
+    loss = net.train(None, None, rec.epochs, rec.batch, rec.lr, seed)
+    t_train = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    dets_l = mb.asci_search(s, ndets, core, E0, C, n, H, screen=sc,
+                            use_net=True)
+    t_sl = time.perf_counter() - t1
+    st_l = mb.last_search_stats(H)
+    tl = {}
+    E_l, X_l = mb.selected_ci_diag(dets_l, H, THRESH, 40, 1e-8,
+                                   precision=MIXED, timings=tl, **dav)
+    t_learned = time.perf_counter() - t0
+    A = mb.make_csr_hamiltonian(dets_l, H, THRESH, np.int64)
+    E_l64 = float(X_l @ A.spmv(X_l)) / float(X_l @ X_l)
+    del A
+    ea = set(map(bytes, dets_e[:len(dets_e) - len(core)]))
+    recall = sum(1 for d in dets_l[:len(dets_l) - len(core)]
+                 if bytes(d) in ea) / max(len(ea), 1)
+    out = {
+        "workload": f"ASCI iteration: n = 48, 12a/12b, bitset<128>, "
+                    f"{len(core)} core dets -> {len(dets_e)} dets, synthetic "
+                    f"integrals seed {seed}; Davidson to 1e-8 (max_m 40, "
+                    f"thick restart 8)",
+        "exact_fp64": {"seconds": t_exact, "search_s": t_se,
+                       "h_build_s": te["h_ms"] / 1e3,
+                       "davidson_s": te["dav_ms"] / 1e3,
+                       "davidson_iterations": te["niter"], "E": E_e,
+                       "ndets": len(dets_e), "raw_pairs": st_e["raw_pairs"],
+                       "unique_pairs": st_e["unique_pairs"],
+                       "phase_ms": {k: st_e[k] for k in
+                                    ("pairs_ms", "sort_ms", "keep_ms")}},
+        "learned_mixed": {"seconds": t_learned, "train_s": t_train,
+                          "train_loss": loss, "search_s": t_sl,
+                          "h_build_s": tl["h_ms"] / 1e3,
+                          "davidson_s": tl["dav_ms"] / 1e3,
+                          "davidson_iterations": tl["niter"], "E": E_l,
+                          "E_with_fp64_H": E_l64, "ndets": len(dets_l),
+                          "raw_pairs": st_l["raw_pairs"],
+                          "units_kept": [st_l["units_kept"],
+                                         st_l["units_total"]],
+                          "predict_ms": st_l["predict_ms"],
+                          "topk_recall": recall},
+        "speedup": t_exact / t_learned,
+        "dE_Eh": E_l - E_e,
+        "dE_target_Eh": 1e-4,
+        "within_target": abs(E_l - E_e) <= 1e-4,
+        "roofline": asci_rooflines(st_e, 128, peak),
+    }
+    del dets_e, dets_l, X_l
+    out["cpu_baseline"] = asci_cpu_baseline(mb, n, H, core[:cpu_ncore],
+                                            C[:cpu_ncore], E0, cpu_ndets, seed)
+    return out
+
+
+def asci_cpu_baseline(mb, n, H, core, C, E0, ndets, seed):
+    """The compiled reference asci_search (one thread: its contribution loop
+    and sort are serial, determinant_search.hpp:54-141 / determinant_sort.hpp:
+    40-83) and the GPU search on the same small core set."""
+    try:
+        import oracle
+        if not oracle.ref_available():
+            return {"unavailable": "compiled reference oracle/_ref missing"}
+        R = oracle.ref()
+        T, V = mb.synthetic_integrals(n, seed)
+        hr = R.ham(128, n, T, V)
+        so = oracle.AsciSettings.default()
+        t = time.perf_counter()
+        r = R.asci_search(hr, so, ndets, core, float(E0), C)
+        t_ref = time.perf_counter() - t
+        s = mb.ASCISettings()
+        mb.asci_search(s, ndets, core, E0, C, n, H)
+        t = time.perf_counter()
+        g = mb.asci_search(s, ndets, core, E0, C, n, H)
+        t_gpu = time.perf_counter() - t
+        st = mb.last_search_stats(H)
+        same = len(set(map(bytes, r)) ^ set(map(bytes, g)))
+        return {"value": t_ref, "unit": "s", "cores": 1, "kind": "reference",
+                "gpu_s": t_gpu, "raw_pairs": st["raw_pairs"],
+                "ref_raw_pairs_per_s": st["raw_pairs"] / t_ref,
+                "gpu_raw_pairs_per_s": st["raw_pairs"] / t_gpu,
+                "selection_differences": same,
+                "sample": f"asci_search, n = 48 12a/12b bitset<128>, "
+                          f"{len(core)} core dets -> {ndets} dets, the same "
+                          f"inputs on both sides"}
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": str(e)}
 
 
 def main():
@@ -664,6 +778,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-asci", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
     rank = env_int("RANK", 0)

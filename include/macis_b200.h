@@ -75,6 +75,9 @@ typedef struct {
   uint64_t samples;       /* training samples recorded into the network */
   double screen_ms;       /* prediction + selection + recording */
   double predict_ms;      /* network forward over all units (device time) */
+  uint64_t sort_pass_items; /* sum over the sorted candidate ranges of
+                               (radix digit passes x records): each pass
+                               reads and writes every record once */
 } macis_b200_asci_stats;
 
 /* Learned screening (no MACIS counterpart). A "unit" of the ASCI search is
@@ -170,12 +173,17 @@ int macis_b200_spmv(const macis_b200_csr* A, int64_t K, double alpha,
  * reference. It is meant for callers that may not allocate device memory
  * once they run -- for instance a service whose memory manager takes all of
  * HBM at start-up -- and it produces the same result as macis_b200_spmv.
- * x and y are device pointers on the matrix's device. The FP32 copy of x is
- * kept in a fixed array compiled into the library (4,194,304 entries, 16 MiB
- * on every GPU that loads the library, held until exit): matrices with more
- * columns are rejected with MACIS_B200_ECAPACITY. The first call on a device
- * looks up that array's device address; make that first call before any
- * stream capture. Every call reuses the same array, so calls that overlap on
+ * x and y are device pointers on the matrix's device; the call runs on that
+ * device whatever device is current and restores the caller's device. The
+ * FP32 copy of x is kept in a fixed array compiled into the library
+ * (4,194,304 entries, 16 MiB): matrices with more columns are rejected with
+ * MACIS_B200_ECAPACITY. The array and the SpMV code are made resident on a
+ * device by the first use of the library's SpMV there (CUDA loads device
+ * modules lazily), which can allocate device memory and looks up the
+ * array's device address: make that first call during set-up, before the
+ * caller's memory manager takes HBM and before any stream capture. Later
+ * calls allocate nothing, and the array then stays on that device until the
+ * process exits. Every call reuses the same array, so calls that overlap on
  * the GPU (from several host threads or handles at once) race; calls return
  * after the product completes. */
 int macis_b200_spmv_mixed_noalloc(const macis_b200_csr* A, double alpha,
@@ -192,6 +200,21 @@ int macis_b200_spmv_mixed_noalloc(const macis_b200_csr* A, double alpha,
 int macis_b200_davidson(const macis_b200_csr* A, int64_t max_m, double tol,
                         int use_guess, double* X, double* E, int64_t* niter,
                         unsigned flags);
+
+/* Device time per phase of the last Davidson solve on the calling thread
+ * (CSR or matrix-free; diagnostics, no reference counterpart): the H
+ * products, the new row of the Rayleigh matrix (multi-dot), the Ritz vector
+ * with residual and preconditioned correction, and CGS2 with the thick-
+ * restart rotations; wall_ms is the host time of the whole solve (the
+ * difference is host work: the k x k eigensolve and synchronisation).
+ * vector_bytes: algorithmic bytes of the Rayleigh, residual and CGS2 phases
+ * (each column of V / AV read once per pass, vectors read / written once). */
+typedef struct {
+  int64_t iterations;
+  double apply_ms, rayleigh_ms, residual_ms, ortho_ms, wall_ms;
+  double vector_bytes;
+} macis_b200_davidson_stats;
+int macis_b200_davidson_last_stats(macis_b200_davidson_stats* out);
 
 /* Davidson options beyond the reference signature. restart_keep = 0 keeps
  * the reference behaviour (no restart: stop after max_m basis vectors);

@@ -28,7 +28,7 @@ from .sd import (canonical_hf_determinant, from_canonical_string,  # noqa
                  generate_cisd_hilbert_space, generate_hilbert_space,
                  to_canonical_string)
 from .solvers import (FP64, MIXED, SparseMatrixOperator,  # noqa: F401
-                      davidson, diagonal_guess, selected_ci_diag,
-                      small_syev)
+                      davidson, davidson_stats, diagonal_guess,
+                      selected_ci_diag, small_syev)
 
 __version__ = "0.1.0"

@@ -37,7 +37,8 @@ class AsciStatsC(C.Structure):
                 ("keep_ms", C.c_double), ("topk_ms", C.c_double),
                 ("total_ms", C.c_double), ("units_total", C.c_uint64),
                 ("units_kept", C.c_uint64), ("samples", C.c_uint64),
-                ("screen_ms", C.c_double), ("predict_ms", C.c_double)]
+                ("screen_ms", C.c_double), ("predict_ms", C.c_double),
+                ("sort_pass_items", C.c_uint64)]
 
 
 class AsciScreenC(C.Structure):
@@ -51,6 +52,13 @@ class DavidsonOptsC(C.Structure):
     _fields_ = [("max_m", C.c_int64), ("tol", C.c_double),
                 ("use_guess", C.c_int32), ("restart_keep", C.c_int32),
                 ("max_iter", C.c_int64)]
+
+
+class DavidsonStatsC(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("apply_ms", C.c_double),
+                ("rayleigh_ms", C.c_double), ("residual_ms", C.c_double),
+                ("ortho_ms", C.c_double), ("wall_ms", C.c_double),
+                ("vector_bytes", C.c_double)]
 
 
 class BuildStatsC(C.Structure):
@@ -96,6 +104,7 @@ _SIGS = {
     "macis_b200_davidson_ex": (C.c_int, [_vp, C.POINTER(DavidsonOptsC), _vp,
                                          C.POINTER(C.c_double),
                                          C.POINTER(C.c_int64), C.c_uint]),
+    "macis_b200_davidson_last_stats": (C.c_int, [C.POINTER(DavidsonStatsC)]),
     "macis_b200_small_syev": (C.c_int, [C.c_int, _vp, C.c_int, _vp, _vp]),
     "macis_b200_csr_build_stats": (C.c_int, [_vp, C.POINTER(BuildStatsC)]),
     "macis_b200_asci_search": (C.c_int, [_vp, C.POINTER(AsciSettingsC), _sz,

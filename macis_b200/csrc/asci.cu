@@ -1171,7 +1171,9 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     if(P) {
       k2 = B.get<uint64_t>(size_t(P) * NW + NW);
       r2 = B.get<double>(size_t(P) + 1);
-      radix_sort<NW, double>(keys, rv, k2, r2, size_t(P), B);
+      stats.sort_pass_items +=
+          uint64_t(radix_sort<NW, double>(keys, rv, k2, r2, size_t(P), B)) *
+          uint64_t(P);
       uint32_t* f = B.get<uint32_t>(size_t(P) + 1);
       uint32_t* fx = B.get<uint32_t>(size_t(P) + 1);
       seg_flags_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(

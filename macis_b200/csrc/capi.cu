@@ -313,6 +313,13 @@ int macis_b200_davidson_ex(const macis_b200_csr* A,
   return rc;
 }
 
+int macis_b200_davidson_last_stats(macis_b200_davidson_stats* out) {
+  return guarded([&] {
+    MB_REQUIRE(out, MACIS_B200_EINVAL, "null argument");
+    *out = davidson_last_stats();
+  });
+}
+
 int macis_b200_small_syev(int k, const double* lower, int nwant, double* W,
                           double* Vec) {
   return guarded([&] {

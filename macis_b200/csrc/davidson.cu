@@ -12,6 +12,7 @@
 // and the entries of earlier rows do not change, so only the new row is
 // formed. Reductions are two-stage with a fixed order (deterministic).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <vector>
 
@@ -272,7 +273,46 @@ __global__ void basis_rotate_k(const double* __restrict__ A, int64_t n, int k,
   }
 }
 
+// Phase timings of the last solve on this host thread
+// (macis_b200_davidson_last_stats).
+static thread_local macis_b200_davidson_stats g_dav_stats{};
+const macis_b200_davidson_stats& davidson_last_stats() { return g_dav_stats; }
+
 namespace {
+// Device time of one phase, accumulated over the solve: events recorded on
+// the solver stream around the phase, read at the next synchronisation.
+struct PhaseTimer {
+  cudaEvent_t e[2];
+  cudaStream_t s;
+  double* acc = nullptr;
+  bool open = false;
+  explicit PhaseTimer(cudaStream_t st) : s(st) {
+    cudaEventCreate(&e[0]);
+    cudaEventCreate(&e[1]);
+  }
+  ~PhaseTimer() {
+    cudaEventDestroy(e[0]);
+    cudaEventDestroy(e[1]);
+  }
+  void begin(double* into) {
+    collect();
+    acc = into;
+    cudaEventRecord(e[0], s);
+  }
+  void end() {
+    cudaEventRecord(e[1], s);
+    open = true;
+  }
+  // after a stream synchronisation (or at the end of the solve)
+  void collect() {
+    if(!open) return;
+    float ms = 0.f;
+    cudaEventSynchronize(e[1]);
+    if(cudaEventElapsedTime(&ms, e[0], e[1]) == cudaSuccess) *acc += ms;
+    open = false;
+  }
+};
+
 struct DavCtx {
   cudaStream_t s;
   int64_t n;
@@ -333,6 +373,9 @@ int davidson_op(const DavOperator& op, int64_t max_m, double tol,
              "Davidson: restart_keep must be in [0, max_m)");
   cudaStream_t s = op.s;
   Arena Ar(s);
+  const auto t_wall = std::chrono::steady_clock::now();
+  macis_b200_davidson_stats st{};
+  PhaseTimer t_op(s), t_ray(s), t_res(s), t_cgs(s);
   max_m = std::min<int64_t>(max_m, N);
   if(restart_keep >= max_m) restart_keep = int(max_m) - 1;
   const double* D = op.diag;
@@ -372,9 +415,14 @@ int davidson_op(const DavOperator& op, int64_t max_m, double tol,
   int64_t i = 1;  // index of the newest basis vector (AV_i not yet formed)
   for(;; ++iter) {
     const int k = int(i + 1);
+    t_op.begin(&st.apply_ms);
     op.apply(V + i * N, AV + i * N);
+    t_op.end();
     // new row of V^T AV: V_i . AV_c for c <= i (lower triangle)
+    t_ray.begin(&st.rayleigh_ms);
     ctx.multidot(AV, N, k, V + i * N, ctx.dots);
+    t_ray.end();
+    st.vector_bytes += double(N) * (k + 1) * 8;
     MB_CUDA(cudaMemcpyAsync(rowdots.data(), ctx.dots, k * 8,
                             cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
@@ -389,9 +437,12 @@ int davidson_op(const DavOperator& op, int64_t max_m, double tol,
     MB_CUDA(cudaMemcpyAsync(d_c, Vec.data(), size_t(k) * nwant * 8,
                             cudaMemcpyHostToDevice, s));
     double* R = V + size_t(k) * N;
+    t_res.begin(&st.residual_ms);
     ritz_residual_k<<<ctx.nb, DV_THREADS, 0, s>>>(V, AV, N, k, d_c, lam0, D,
                                                   X, R, ctx.partial), note_launch();
     reduce_partials_k<<<1, 32, 0, s>>>(ctx.partial, ctx.nb, 1, ctx.dots + 1200), note_launch();
+    t_res.end();
+    st.vector_bytes += double(N) * (2.0 * k + 3) * 8;
     double rn2 = 0;
     MB_CUDA(cudaMemcpyAsync(&rn2, ctx.dots + 1200, 8, cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
@@ -405,6 +456,11 @@ int davidson_op(const DavOperator& op, int64_t max_m, double tol,
       // thick restart: keep the lowest restart_keep Ritz vectors
       const int keep = restart_keep;
       const unsigned g = grid_for(size_t(N), 256, size_t(num_sms()) * 8);
+      t_cgs.begin(&st.ortho_ms);
+      // two rotations (read k columns, write keep), the copies back and
+      // of R, then CGS2 over keep columns
+      st.vector_bytes += double(N) * (2.0 * k + 6.0 * keep + 2) * 8 +
+                         double(N) * (4.0 * keep + 9) * 8;
       basis_rotate_k<<<g, 256, 0, s>>>(V, N, k, d_c, keep, tmp), note_launch();
       MB_CUDA(cudaMemcpyAsync(V, tmp, size_t(N) * keep * 8,
                               cudaMemcpyDeviceToDevice, s));
@@ -416,15 +472,25 @@ int davidson_op(const DavOperator& op, int64_t max_m, double tol,
       std::fill(Cl.begin(), Cl.end(), 0.0);
       for(int c = 0; c < keep; ++c) Cl[c + size_t(c) * ld] = W[c];
       ctx.cgs2(V, keep, V + size_t(keep) * N);
+      t_cgs.end();
       i = keep;
       continue;
     }
     if(max_iter > 0 && iter >= max_iter) break;
+    t_cgs.begin(&st.ortho_ms);
     ctx.cgs2(V, k, R);
+    t_cgs.end();
+    st.vector_bytes += double(N) * (4.0 * k + 9) * 8;
     i = k;
   }
   MB_CUDA(cudaGetLastError());
   MB_CUDA(cudaStreamSynchronize(s));
+  for(PhaseTimer* t : {&t_op, &t_ray, &t_res, &t_cgs}) t->collect();
+  st.iterations = iter;
+  st.wall_ms = std::chrono::duration<double, std::milli>(
+                   std::chrono::steady_clock::now() - t_wall)
+                   .count();
+  g_dav_stats = st;
   *E = lam0;
   *niter = iter;
   return converged ? 0 : MACIS_B200_ENOCONV;

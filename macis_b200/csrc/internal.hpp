@@ -135,6 +135,7 @@ struct DavOperator {
 int davidson_op(const DavOperator& op, int64_t max_m, double tol,
                 bool use_guess, double* X, double* E, int64_t* niter,
                 int restart_keep, int64_t max_iter);
+const macis_b200_davidson_stats& davidson_last_stats();
 
 // 1- and 2-RDM over one determinant list (device arrays; results added to
 // ordm / trdm, trdm may be null).

@@ -11,7 +11,9 @@
 // product formed exactly in FP64 (24x24-bit mantissas fit in 53 bits) and
 // summed in FP64, plus the FP64 diagonal times the FP64 x. The Davidson
 // solver uses the same kernel with the FP64 x (spmv_device_x64).
+#include <exception>
 #include <mutex>
+#include <new>
 
 #include "internal.hpp"
 #include "primitives.cuh"
@@ -137,8 +139,12 @@ void spmv_device_x64(const macis_b200_csr* A, double alpha, const double* x,
 // forbids cudaMalloc afterwards, or a host program whose memory budget is
 // fixed when it links this library. For them the FP32 copy of x that the
 // mixed-precision product needs lives in the file-scope array below instead
-// of a stream-ordered allocation. Every GPU that loads the library holds
-// this array (16 MiB) until the process exits.
+// of a stream-ordered allocation. The array (16 MiB) belongs to this file's
+// device module: with CUDA's lazy module loading the module, and with it the
+// array and the kernel code, is made resident on a device by the first use
+// of this file's code there (any SpMV, or the first allocation-free call),
+// and stays until the process exits. That first use may allocate device
+// memory; later allocation-free calls allocate nothing.
 namespace mb {
 namespace {
 
@@ -157,17 +163,37 @@ float* noalloc_scratch(int dev) {
   MB_REQUIRE(dev >= 0 && dev < kMaxDevices, MACIS_B200_EINVAL,
              "device ordinal out of range");
   if(!g_noalloc_ptr[dev]) {
-    int cur = -1;
-    MB_CUDA(cudaGetDevice(&cur));
-    if(cur != dev) MB_CUDA(cudaSetDevice(dev));
+    // the caller holds `dev` current (DeviceScope)
     void* p = nullptr;
-    const cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_x32);
-    if(cur != dev) cudaSetDevice(cur);
-    MB_CUDA(rc);
+    MB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_x32));
     g_noalloc_ptr[dev] = static_cast<float*>(p);
   }
   return g_noalloc_ptr[dev];
 }
+
+}  // namespace
+}  // namespace mb
+
+namespace mb {
+namespace {
+
+// Makes `dev` current for the life of the guard and restores the caller's
+// device afterwards (the handle's stream and the scratch address belong to
+// the matrix's device, whatever device the caller has current).
+struct DeviceScope {
+  int prev = -1;
+  bool switched = false;
+  explicit DeviceScope(int dev) {
+    MB_CUDA(cudaGetDevice(&prev));
+    if(prev != dev) {
+      MB_CUDA(cudaSetDevice(dev));
+      switched = true;
+    }
+  }
+  ~DeviceScope() {
+    if(switched) cudaSetDevice(prev);
+  }
+};
 
 }  // namespace
 }  // namespace mb
@@ -182,6 +208,7 @@ extern "C" int macis_b200_spmv_mixed_noalloc(const macis_b200_csr* A,
     MB_REQUIRE(A->n <= mb::kNoAllocMaxN, MACIS_B200_ECAPACITY,
                "matrix has more columns than the allocation-free scratch "
                "holds (4,194,304)");
+    mb::DeviceScope on(A->device);
     float* x32 = mb::noalloc_scratch(A->device);
     const int64_t m = A->m;
     cudaStream_t s = A->stream;
@@ -207,6 +234,11 @@ extern "C" int macis_b200_spmv_mixed_noalloc(const macis_b200_csr* A,
   } catch(const mb::Error& e) {
     mb::set_error(e.what());
     return e.code;
+  } catch(const std::bad_alloc&) {
+    mb::set_error("host allocation failed");
+    return MACIS_B200_ENOMEM;
+  } catch(const std::exception& e) {  // e.g. std::system_error of the mutex
+    mb::set_error(e.what());
+    return MACIS_B200_EINVAL;
   }
 }
-

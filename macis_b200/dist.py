@@ -392,7 +392,8 @@ def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
     rank's row block of H on its GPU (make_dist_csr_hamiltonian), the guess,
     then p_davidson (no restarts, as the reference). C_local (this rank's
     rows) is the guess when max |C| over all ranks exceeds 1/N; else the
-    diagonal guess (p_diagonal_guess). Returns (E0, X_local), X_local this
+    diagonal guess (p_diagonal_guess), also when any rank lacks its rows of
+    C (None or the wrong length). Returns (E0, X_local), X_local this
     rank's rows of the eigenvector as a CUDA tensor.
 
     The reference compares each rank's own max |C_local| with 1/len(C_local),
@@ -405,7 +406,11 @@ def selected_ci_diag(dets, ham_gen, h_el_tol, davidson_max_m,
     dev = A.device
     D = A.diagonal(dev)
     ok = C_local is not None and len(C_local) == A.m_local
-    if reuse_guess(C_local if ok else None, N, group):
+    # one branch on every rank: the guess is reused only when every rank
+    # holds its rows of it (else a rank without them would fail while the
+    # others wait in p_davidson's collectives)
+    all_ok = reduce_max(0.0 if ok else 1.0, group, dev) == 0.0
+    if reuse_guess(C_local if ok else None, N, group) and all_ok:
         X = torch.as_tensor(np.asarray(C_local, dtype=np.float64)).to(dev)
     else:
         X = p_diagonal_guess(D, N, group)

@@ -18,7 +18,8 @@ from .hamiltonian import (DeviceCSR, MatrixFreeHamiltonian,
                           make_csr_hamiltonian)
 
 __all__ = ["SparseMatrixOperator", "diagonal_guess", "davidson",
-           "selected_ci_diag", "small_syev", "FP64", "MIXED"]
+           "selected_ci_diag", "small_syev", "davidson_stats", "FP64",
+           "MIXED"]
 
 FP64 = "fp64"
 MIXED = "mixed"
@@ -72,6 +73,16 @@ def davidson(N, max_m, op, D, tol, X, use_guess=True, restart_keep=0,
     logging.getLogger("davidson").info("Davidson Converged! iter = %d E0 = %.12e",
                                        it.value, E.value)
     return it.value, E.value
+
+
+def davidson_stats():
+    """Per-phase device times (ms) of the last Davidson solve on this thread:
+    apply (H products), rayleigh, residual, ortho (CGS2 and restarts), wall
+    (host), and vector_bytes, the algorithmic bytes of the non-product
+    phases."""
+    st = _lib.DavidsonStatsC()
+    check(LIB.macis_b200_davidson_last_stats(C.byref(st)))
+    return {k: getattr(st, k) for k, _ in st._fields_}
 
 
 def small_syev(lower, nwant=1):

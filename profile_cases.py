@@ -1,36 +1,40 @@
 """Small, self-contained workloads for kernel profiling (ncu) and timing.
 
-    python -m macis_b200.profile_cases hbuild_c1   # CAS(10e,10o) CSR build
-    python -m macis_b200.profile_cases hbuild_c2   # CAS(12e,12o) CSR build
-    python -m macis_b200.profile_cases hbuild_c2s  # 12 orbitals, 3a/6b: the
+    python profile_cases.py hbuild_c1   # CAS(10e,10o) CSR build
+    python profile_cases.py hbuild_c2   # CAS(12e,12o) CSR build
+    python profile_cases.py hbuild_c2s  # 12 orbitals, 3a/6b: the
         # beta lists of CAS(12e,12o) at a quarter of its output (3.3 GB)
-    python -m macis_b200.profile_cases spmv_c1     # FP64 SpMV on CAS(10e,10o)
-    python -m macis_b200.profile_cases hop_c2      # matrix-free H x, CAS(12e,12o)
-    python -m macis_b200.profile_cases hbuild_sel  # selected (shuffled) space
-    python -m macis_b200.profile_cases asci_n48    # one ASCI search, n = 48
+    python profile_cases.py spmv_c1     # FP64 SpMV on CAS(10e,10o)
+    python profile_cases.py hop_c2      # matrix-free H x, CAS(12e,12o)
+    python profile_cases.py hbuild_sel  # selected (shuffled) space
+    python profile_cases.py asci_n48    # one ASCI search, n = 48
         # (--ncore core determinants, default 10000)
-    python -m macis_b200.profile_cases mlp_fwd     # network forward, 2M rows
-    python -m macis_b200.profile_cases mlp_train   # one training epoch
-    python -m macis_b200.profile_cases screen_n48  # screened search, n = 48
-    python -m macis_b200.profile_cases c3 --ntdets 1000000 --mode fp64
+    python profile_cases.py mlp_fwd     # network forward, 2M rows
+    python profile_cases.py mlp_train   # one training epoch
+    python profile_cases.py asci_iter_n48 --ncore 100000 --ntdets 1e6
+        # one ASCI iteration, n = 48: exact FP64 against learned + mixed
+    python profile_cases.py c3 --ntdets 1000000 --mode fp64
         # ASCI n = 48, 12a/12b, bitset<128>: grow from HF (factor 8, <= 1e5
         # core dets) then 3 refine iterations; --mode fp64 (exact search,
         # FP64 Davidson) or learned_mixed (screened search, FP32-H Davidson)
-    python -m macis_b200.profile_cases c4 --ntdets 1000000 --mode ...
+    python profile_cases.py c4 --ntdets 1000000 --mode ...
         # the same on n = 64, 16a/16b, bitset<128>; learned_mixed also runs
         # one exact search from its last core set and reports the top-k
         # recall of the screened one
-    python -m macis_b200.profile_cases c5 --ntdets 51200 --refine 1
+    python profile_cases.py c5 --ntdets 51200 --refine 1
         # n = 100, 20a/20b, bitset<256>, exact search, FP64 Davidson
 
 Each case runs its hot call a few times (--reps) and prints one timing line.
 """
 import argparse
+import os
+import sys
 import time
 
 import numpy as np
 
-import macis_b200 as mb
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import macis_b200 as mb  # noqa: E402
 
 EPS = float(np.finfo(np.float64).eps)
 
@@ -65,19 +69,32 @@ def spmv(norb, k, reps):
         print(f"spmv host-staged {1e3 * (time.perf_counter() - t):.3f} ms")
 
 
-def asci_n48(reps, ncore=10000):
+def _bench():
     import importlib.util
-    import os
     spec = importlib.util.spec_from_file_location(
-        "bench", os.path.join(os.path.dirname(os.path.dirname(
-            os.path.abspath(__file__))), "bench.py"))
+        "bench", os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                              "bench.py"))
     bench = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(bench)
+    return bench
+
+
+def asci_n48(reps, ncore=10000, ndets=200000):
+    """One exact ASCI search on the bench's n = 48 core set (the first run
+    grows the memory pool)."""
+    bench = _bench()
+    n, H, core, C, E0 = bench._n48_core(mb, ncore)
+    s = mb.ASCISettings()
     for _ in range(reps):
-        r = bench.asci_extra(mb, ncore=ncore, ndets_max=200000)
-        print(f"asci {r['seconds']:.3f} s raw={r['raw_pairs']} "
-              f"unique={r['unique_pairs']} batches={r['batches']} "
-              f"phases={r['phase_ms']}")
+        t = time.perf_counter()
+        mb.asci_search(s, ndets, core, E0, C, n, H)
+        dt = time.perf_counter() - t
+        st = mb.last_search_stats(H)
+        print(f"asci {dt:.3f} s raw={st['raw_pairs']} "
+              f"unique={st['unique_pairs']} batches={st['batches']} "
+              f"pairs_ms={st['pairs_ms']:.1f} sort_ms={st['sort_ms']:.1f} "
+              f"keep_ms={st['keep_ms']:.1f} "
+              f"passes={st['sort_pass_items'] / max(st['raw_pairs'], 1):.2f}")
 
 
 def hop(norb, k, reps):
@@ -131,17 +148,13 @@ def mlp_train(reps, n=1 << 18, batch=256):
               f"({dt * 1e6 / (n / batch):.1f} us/step) loss {loss:.4f}")
 
 
-def screen_n48(reps, ncore=10000):
-    import importlib.util
-    import os
-    spec = importlib.util.spec_from_file_location(
-        "bench", os.path.join(os.path.dirname(os.path.dirname(
-            os.path.abspath(__file__))), "bench.py"))
-    bench = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(bench)
-    for _ in range(reps):
-        r = bench.screen_extra(mb, ncore=ncore, ndets_max=200000)
-        print(r)
+def asci_iter_n48(ncore=100000, ndets=1000000):
+    """The bench's C3-shaped ASCI iteration (exact FP64 against learned +
+    mixed) on its own."""
+    import json
+    bench = _bench()
+    print(json.dumps(bench.asci_iteration(mb, bench.peaks()[0], ncore=ncore,
+                                          ndets=ndets), default=float))
 
 
 def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128):
@@ -244,8 +257,9 @@ def main():
         mlp_fwd(a.reps)
     elif a.case == "mlp_train":
         mlp_train(a.reps)
-    elif a.case == "screen_n48":
-        screen_n48(a.reps)
+    elif a.case == "asci_iter_n48":
+        asci_iter_n48(a.ncore if a.ncore != 10000 else 100000,
+                      int(a.ntdets))
     elif a.case == "c3":
         c3(a.ntdets, a.mode)
     elif a.case == "c4":

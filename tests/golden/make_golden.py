@@ -2,7 +2,9 @@
 
 Run in a container that has the reference mounted (it is read here only):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <path to the MACIS source tree>
+
+or with the path in the environment variable MACIS_REFERENCE_DIR.
 
 Outputs (all under tests/golden/):
 
@@ -80,4 +82,9 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+        "MACIS_REFERENCE_DIR")
+    if not src:
+        sys.exit("usage: make_golden.py <path to the MACIS source tree> "
+                 "(or set MACIS_REFERENCE_DIR)")
+    main(src)

@@ -140,6 +140,28 @@ def _dist_iter(md, dets, lo, hi, rp, ci, nz, mv):
     return dict(E=E, X=X, nwfn=len(wfn), seen=seen)
 
 
+def _dist_sci_partial_guess(md, dets, lo, hi, rp, ci, nz, mv, rank):
+    """dist.selected_ci_diag where only rank 0 passes its rows of a guess
+    (rank 1 passes None): every rank must take the diagonal guess."""
+    N = len(dets)
+    D = np.empty(hi - lo)
+    rows = np.repeat(np.arange(hi - lo), np.diff(rp))
+    on = ci == rows + lo
+    D[rows[on]] = nz[on]
+
+    def build(d, H, tol, group=None):
+        return _FakeBlock(md, lo, hi, N, D, mv)
+    saved = md.make_dist_csr_hamiltonian
+    md.make_dist_csr_hamiltonian = build
+    try:
+        C_local = np.full(hi - lo, 0.9) if rank == 0 else None
+        E, X = md.selected_ci_diag(dets, _Ham64(), np.finfo(float).eps, 200,
+                                   1e-8, C_local=C_local)
+    finally:
+        md.make_dist_csr_hamiltonian = saved
+    return dict(E=E, X=md.allgather_rows(X, N).numpy())
+
+
 class _FakeNet:
     """Network stand-in: the samples a part search recorded."""
     handle = None
@@ -229,6 +251,9 @@ def _rank_main(rank, port_no, case, q):
                        guess=g)
         elif case == "dist_iter":
             out.update(_dist_iter(md, dets, lo, hi, rp, ci, nz, mv))
+        elif case == "sci_partial_guess":
+            out.update(_dist_sci_partial_guess(md, dets, lo, hi, rp, ci, nz,
+                                               mv, rank))
         elif case == "asci":
             parts_in, _ = _asci_parts(port)
             states, scores, core, ndets_max = parts_in[rank]
@@ -387,3 +412,22 @@ def test_dist_asci_iter_two_ranks(port):
         assert np.array_equal(o["X"], res[0]["X"])
         assert abs(abs(o["X"] @ X) / (np.linalg.norm(o["X"]) *
                                       np.linalg.norm(X)) - 1.0) < 1e-10
+
+
+def test_dist_selected_ci_diag_guess_on_one_rank_only(port):
+    """Only rank 0 passes its rows of the guess: both ranks fall back to the
+    p_diagonal_guess start together (no rank fails alone while the other
+    waits in a collective) and match the serial Davidson from that start."""
+    res = _run("sci_partial_guess")
+    T, V, dets = _problem()
+    rp, ci, nz = port.build_csr(port.ham(64, 7, T, V), dets, dets,
+                                np.finfo(float).eps)
+    rows = np.repeat(np.arange(len(dets)), np.diff(rp))
+    D = nz[ci == rows]
+    G = np.zeros(len(dets))
+    G[int(np.argmin(D))] = 1.0
+    E, it, X = port.davidson(rp, ci, nz, 200, 1e-8, G)
+    for r in range(WORLD):
+        o = res[r]
+        assert o["E"] == res[0]["E"] and abs(o["E"] - E) < 1e-9
+        assert np.array_equal(o["X"], res[0]["X"])
