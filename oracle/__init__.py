@@ -23,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libmacis_ref.so")
+REFC_PATH = os.path.join(HERE, "_ref", "libmacis_ref_constraint.so")
 
 _p64 = C.POINTER(C.c_uint64)
 _pd = C.POINTER(C.c_double)
@@ -553,8 +554,57 @@ class RefCsr:
             self.c = None
 
 
+class RefConstraint:
+    """The reference's MPI-only constraint-partitioned ASCI contributions
+    (asci_contributions_constraint, determinant_search.hpp:143-391), compiled
+    against a serial MPI stand-in so that one call runs one rank of a job of
+    `world` ranks (_ref/libmacis_ref_constraint.so, bitset<64/128>)."""
+
+    def __init__(self, path=REFC_PATH):
+        L = C.CDLL(path)
+        L.mrefc_last_error.restype = C.c_char_p
+        L.mrefc_ham_create.restype = C.c_void_p
+        L.mrefc_ham_create.argtypes = [C.c_int, C.c_size_t, _pd, _pd]
+        L.mrefc_ham_free.argtypes = [C.c_void_p]
+        L.mrefc_asci_pairs.restype = C.c_void_p
+        L.mrefc_asci_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _p64,
+                                       C.c_size_t, C.c_double, _pd, C.c_int,
+                                       C.c_int]
+        L.mrefc_pairs_size.restype = C.c_size_t
+        L.mrefc_pairs_size.argtypes = [C.c_void_p]
+        L.mrefc_pairs_copy.argtypes = [C.c_void_p, _p64, _pd]
+        L.mrefc_pairs_free.argtypes = [C.c_void_p]
+        self.L = L
+
+    def ham(self, nbits, norb, T, V):
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        p = self.L.mrefc_ham_create(nbits, norb, _ptr(T, _pd), _ptr(V, _pd))
+        if not p:
+            raise RuntimeError(self.L.mrefc_last_error().decode())
+        return Handle(p, self.L.mrefc_ham_free, nbits, norb)
+
+    def asci_pairs(self, h, s, cdets, E0, Cv, rank, world, constraint_level=2):
+        """This rank's accumulated (state, rv) pairs, per constraint in the
+        reference's order (each constraint's block sorted on its own)."""
+        cdets = _dets(cdets, h.nbits)
+        Cv = np.ascontiguousarray(Cv, dtype=np.float64)
+        p = self.L.mrefc_asci_pairs(h.p, C.byref(s), int(constraint_level),
+                                    _ptr(cdets, _p64), len(cdets), E0,
+                                    _ptr(Cv, _pd), int(rank), int(world))
+        if not p:
+            raise RuntimeError(self.L.mrefc_last_error().decode())
+        n = self.L.mrefc_pairs_size(p)
+        st = np.empty((max(n, 1), h.nbits // 64), dtype=np.uint64)
+        rv = np.empty(max(n, 1))
+        self.L.mrefc_pairs_copy(p, _ptr(st, _p64), _ptr(rv, _pd))
+        self.L.mrefc_pairs_free(p)
+        return st[:n], rv[:n]
+
+
 _port = None
 _ref = None
+_refc = None
 
 
 def port():
@@ -573,3 +623,14 @@ def ref():
     if _ref is None:
         _ref = Ref()
     return _ref
+
+
+def ref_constraint_available():
+    return os.path.exists(REFC_PATH)
+
+
+def ref_constraint():
+    global _refc
+    if _refc is None:
+        _refc = RefConstraint()
+    return _refc

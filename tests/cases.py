@@ -71,3 +71,33 @@ def abs_sums(states, rv):
     new[1:] = np.any(s[1:] != s[:-1], axis=1)
     idx = np.flatnonzero(new)
     return s[idx], np.add.reduceat(a, idx) if len(a) else a
+
+
+def reference_mpi_selection(parts, cdets, ndets_max):
+    """The selection of the reference's MPI asci_search (world size > 1,
+    include/macis/asci/determinant_search.hpp:528-654) from every rank's
+    accumulated (states, rv) pairs: per rank, rv -> -|rv| and the core
+    determinants are dropped (keep_only_largest_copy_asci_pairs + partition);
+    the k-th largest |rv| over all ranks (dist_quickselect,
+    util/dist_quickselect.hpp) with k = ndets_max - ncore; every rank keeps
+    its pairs with |rv| >= that score; the gathered states (rank order) are
+    cut at k when ties at the score overflow it; the core determinants
+    follow. Returns the determinant array."""
+    cdets = np.ascontiguousarray(cdets)
+    vt = np.dtype((np.void, cdets.shape[1] * 8))
+    core = cdets.view(vt).ravel()
+    kept = []
+    for st, rv in parts:
+        st = np.ascontiguousarray(st)
+        keep = ~np.isin(st.view(vt).ravel(), core)
+        kept.append((st[keep], np.abs(rv[keep])))
+    k = ndets_max - len(cdets)
+    allv = np.concatenate([v for _, v in kept])
+    if len(allv) <= k:
+        sel = [s for s, _ in kept]
+    else:
+        kth = np.sort(allv)[::-1][k - 1]
+        sel = [s[v >= kth] for s, v in kept]
+    sel = np.concatenate(sel)[:k] if sel else np.zeros((0, cdets.shape[1]),
+                                                        dtype=np.uint64)
+    return np.concatenate([sel, np.ascontiguousarray(cdets)])

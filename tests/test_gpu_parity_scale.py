@@ -29,7 +29,8 @@ import pytest
 
 import macis_b200 as mb
 import oracle
-from cases import abs_sums, assert_csr_equal, core_set, shuffled
+from cases import (abs_sums, assert_csr_equal, core_set,
+                   reference_mpi_selection, shuffled)
 
 pytestmark = pytest.mark.gpu
 
@@ -94,6 +95,41 @@ def test_search_matches_port_and_reference(shape, pairs, port, ref):
         idx = {t: i for i, t in enumerate(map(tuple, gs.tolist()))}
         kth = min(abs(gr[idx[t]])
                   for t in key(got[:NDETS - len(shape["cd"])]))
+        for t in diff:
+            i = idx[t]
+            assert abs(abs(gr[i]) - kth) <= 2e-13 * scale[i] + 1e-14 * kth
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_split_search_matches_reference_constraint_partition(shape, pairs,
+                                                             world):
+    """The hash-bin split search over `world` parts, merged, against the
+    reference's MPI search over `world` ranks: each rank's pairs from the
+    reference's own constraint-partitioned path (asci_contributions_
+    constraint, determinant_search.hpp:143-391, rank split of
+    dist_constraint_general) and the reference's distributed top-k over
+    them (determinant_search.hpp:528-654). Identical selections outside
+    near-ties at the k-th score."""
+    if not oracle.ref_constraint_available():
+        pytest.skip("compiled reference oracle/_ref not built")
+    refc = oracle.ref_constraint()
+    n, cd, C, E0, H = (shape[k] for k in ("n", "cd", "C", "E0", "H"))
+    parts = [mb.asci_search_part(_settings(), NDETS, cd, E0, C, n, H, i,
+                                 world) for i in range(world)]
+    got = mb.merge_asci_parts(parts, NDETS, cd, 128)
+    hc = refc.ham(128, n, shape["T"], shape["V"])
+    so = oracle.AsciSettings.default()
+    rparts = [refc.asci_pairs(hc, so, cd, E0, C, r, world)
+              for r in range(world)]
+    exp = reference_mpi_selection(rparts, cd, NDETS)
+    assert len(got) == len(exp) == NDETS
+    assert np.array_equal(got[NDETS - len(cd):], cd)
+    key = lambda a: set(map(tuple, np.asarray(a).tolist()))
+    diff = key(got) ^ key(exp)
+    if diff:
+        (gs, gr), _, _, _, scale = pairs
+        idx = {t: i for i, t in enumerate(map(tuple, gs.tolist()))}
+        kth = min(abs(gr[idx[t]]) for t in key(got[:NDETS - len(cd)]))
         for t in diff:
             i = idx[t]
             assert abs(abs(gr[i]) - kth) <= 2e-13 * scale[i] + 1e-14 * kth
