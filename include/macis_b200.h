@@ -108,6 +108,25 @@ int macis_b200_version(void);
 /* Number of kernels this library has launched in the process (benchmark
  * diagnostics; no reference counterpart). */
 unsigned long long macis_b200_launch_count(void);
+/* Time limit, in nanoseconds, of every barrier wait inside the tensor-core
+ * kernels of the screening network (0 restores the default of 2 s; no
+ * reference counterpart). A wait that runs out makes the call return
+ * MACIS_B200_ETIMEOUT after the kernel has drained its copies and MMAs in
+ * flight and freed its tensor memory; later calls run normally. A limit far
+ * below a kernel's own waits forces that path, which the tests use. */
+int macis_b200_set_wait_limit_ns(uint64_t ns);
+/* Host-side fault injection for tests of the error paths (no reference
+ * counterpart; the C++ shim maps the resulting codes to the reference's
+ * exceptions). MACIS_B200_FAULT_ALLOC: after `arg` more successful device
+ * allocations by the library, the next one reports out-of-memory
+ * (MACIS_B200_ENOMEM), once. MACIS_B200_FAULT_INT32_LIMIT: CSR builds with
+ * int32 indices reject more than `arg` nonzeros (MACIS_B200_ECAPACITY).
+ * MACIS_B200_FAULT_NONE clears both. Process-wide; nothing fails on the
+ * device. */
+#define MACIS_B200_FAULT_NONE 0
+#define MACIS_B200_FAULT_ALLOC 1
+#define MACIS_B200_FAULT_INT32_LIMIT 2
+int macis_b200_inject_fault(int kind, int64_t arg);
 
 /* --- Hamiltonian generator ------------------------------------------------
  * Replaces the HamiltonianGenerator<N> constructor and

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libmacis_b200.so")
 
 OK, EINVAL, ENOMEM, ECAPACITY, ETIMEOUT, ENOCONV, ECUDA, ENOGROW = range(8)
 DEVICE_PTRS = 1
+FAULT_NONE, FAULT_ALLOC, FAULT_INT32_LIMIT = 0, 1, 2
 HOP_FP32 = 2  # matrix-free H: off-diagonal elements rounded to FP32
 FP64, MIXED = 0, 1
 
@@ -77,6 +78,8 @@ _SIGS = {
     "macis_b200_last_error": (C.c_char_p, []),
     "macis_b200_version": (C.c_int, []),
     "macis_b200_launch_count": (C.c_ulonglong, []),
+    "macis_b200_set_wait_limit_ns": (C.c_int, [C.c_uint64]),
+    "macis_b200_inject_fault": (C.c_int, [C.c_int, C.c_int64]),
     "macis_b200_ham_create": (C.c_int, [C.c_int, _sz, _pd, _sz, _pd, _sz,
                                         C.POINTER(_vp)]),
     "macis_b200_ham_destroy": (C.c_int, [_vp]),

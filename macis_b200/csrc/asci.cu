@@ -836,7 +836,7 @@ static int64_t core_setup(macis_b200_ham* h, Arena& A, const uint64_t* cdets,
   cd.uoff = A.get<int64_t>(ncdets + 1);
   if(!h->pairmax) {
     const size_t n2 = size_t(n) * n;
-    MB_CUDA(cudaMalloc(&h->pairmax, 2 * n2 * sizeof(double)));
+    MB_CUDA(dev_malloc(&h->pairmax, 2 * n2 * sizeof(double)));
     pairmax_g_k<<<grid_for(n2 * 32, 256, 16 * sms), 256, 0, s>>>(
         h->G, n, h->pairmax), note_launch();
     pairmax_v_k<<<grid_for(n2, 128, 4 * sms), 128, 0, s>>>(
@@ -864,6 +864,10 @@ static void check_net(const macis_b200_mlp* net, cudaStream_t s) {
   int e = 0;
   MB_CUDA(cudaMemcpyAsync(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
+  if(e) {  // cleared, so that the next call starts clean
+    MB_CUDA(cudaMemsetAsync(net->err, 0, sizeof(int), s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
   MB_REQUIRE(e == 0, MACIS_B200_ETIMEOUT,
              "screening network kernel timed out waiting on a barrier");
 }
@@ -919,7 +923,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     MB_CUDA(cudaEventRecord(ev[0], s));
     kern<<<unsigned(std::min<int64_t>(tiles, sms)), MLP_TM, smem, s>>>(
         mlp_weights(net), UnitRows<NBITS>{cd, E0}, U, pred, MlpTaps{},
-        net->err), note_launch();
+        net->err, wait_limit_ns()), note_launch();
     MB_CUDA(cudaGetLastError());
     MB_CUDA(cudaEventRecord(ev[1], s));
     MB_CUDA(cudaEventSynchronize(ev[1]));

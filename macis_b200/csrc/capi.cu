@@ -42,7 +42,7 @@ struct DevBuf {
     if(flags & MACIS_B200_DEVICE_PTRS) {
       d = const_cast<T*>(p);
     } else {
-      MB_CUDA(cudaMallocAsync(&d, n * sizeof(T) + 16, s));
+      MB_CUDA(dev_malloc_async(&d, n * sizeof(T) + 16, s));
       owned = true;
       if(n && p)
         MB_CUDA(cudaMemcpyAsync(d, p, n * sizeof(T), cudaMemcpyHostToDevice, s));
@@ -108,7 +108,7 @@ int macis_b200_matrix_element(macis_b200_ham* h, const uint64_t* bra,
     DevBuf<double> o(out, 0, flags | MACIS_B200_DEVICE_PTRS, h->stream);
     double* dout = out;
     if(!(flags & MACIS_B200_DEVICE_PTRS))
-      MB_CUDA(cudaMallocAsync(&dout, n * 8 + 8, h->stream));
+      MB_CUDA(dev_malloc_async(&dout, n * 8 + 8, h->stream));
     matrix_elements_device(h, b.d, k.d, n, dout);
     if(!(flags & MACIS_B200_DEVICE_PTRS)) {
       MB_CUDA(cudaMemcpyAsync(out, dout, n * 8, cudaMemcpyDeviceToHost, h->stream));
@@ -166,6 +166,33 @@ int macis_b200_csr_destroy(macis_b200_csr* A) {
 }
 
 unsigned long long macis_b200_launch_count(void) { return launch_counter(); }
+
+int macis_b200_inject_fault(int kind, int64_t arg) {
+  return guarded([&] {
+    switch(kind) {
+      case MACIS_B200_FAULT_NONE:
+        faults().alloc_countdown.store(-1);
+        faults().int32_limit.store(INT32_MAX);
+        break;
+      case MACIS_B200_FAULT_ALLOC:
+        MB_REQUIRE(arg >= 0, MACIS_B200_EINVAL, "allocation count must be >= 0");
+        faults().alloc_countdown.store(arg);
+        break;
+      case MACIS_B200_FAULT_INT32_LIMIT:
+        MB_REQUIRE(arg >= 0 && arg <= INT32_MAX, MACIS_B200_EINVAL,
+                   "int32 limit must be in [0, 2^31 - 1]");
+        faults().int32_limit.store(arg);
+        break;
+      default:
+        MB_REQUIRE(false, MACIS_B200_EINVAL, "unknown fault kind");
+    }
+  });
+}
+
+int macis_b200_set_wait_limit_ns(uint64_t ns) {
+  wait_limit_slot().store(ns ? ns : kDefaultWaitLimitNs);
+  return MACIS_B200_OK;
+}
 
 int macis_b200_csr_info(const macis_b200_csr* A, int64_t* m, int64_t* n,
                         int64_t* nnz, int* idx_bytes, int* val_bytes) {
@@ -367,7 +394,7 @@ int macis_b200_asci_search_screened(macis_b200_ham* h,
     const size_t cap = ndets_max + ncdets;
     uint64_t* od = out_dets;
     if(!(flags & MACIS_B200_DEVICE_PTRS))
-      MB_CUDA(cudaMallocAsync(&od, cap * nw * 8 + 32, h->stream));
+      MB_CUDA(dev_malloc_async(&od, cap * nw * 8 + 32, h->stream));
     try {
       asci_search_device(h, *s, scr, ndets_max, cd.d, ncdets, E0, cc.d, od,
                          nout, nullptr, nullptr, false);

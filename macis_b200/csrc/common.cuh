@@ -7,6 +7,8 @@
 // alpha in word 0 and beta in word 1; NBITS=256 has alpha in words 0-1 and
 // beta in words 2-3. Spin strings are handled as Spin<NSW> (1 or 2 words).
 #pragma once
+#include <atomic>
+#include <climits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -318,6 +320,54 @@ inline unsigned long long& launch_counter() {
   return n;
 }
 inline void note_launch() { ++launch_counter(); }
+
+// ------------------------------------------------------- fault injection
+// Host-side failures for the tests of the error paths
+// (macis_b200_inject_fault): the (k+1)-th next device allocation made by the
+// library reports out-of-memory (once), or CSR builds with int32 indices
+// accept fewer nonzeros. Nothing is made to fail on the device.
+struct FaultInjection {
+  std::atomic<int64_t> alloc_countdown{-1};  // -1: off
+  std::atomic<int64_t> int32_limit{INT32_MAX};
+};
+inline FaultInjection& faults() {
+  static FaultInjection f;
+  return f;
+}
+inline bool take_injected_alloc_failure() {
+  auto& c = faults().alloc_countdown;
+  const int64_t v = c.load(std::memory_order_relaxed);
+  if(v < 0) return false;
+  c.store(v - 1, std::memory_order_relaxed);  // 0 -> -1: fires once
+  return v == 0;
+}
+// Every device allocation of the library goes through these two.
+template <typename T>
+inline cudaError_t dev_malloc_async(T** p, size_t bytes, cudaStream_t s) {
+  if(take_injected_alloc_failure()) return cudaErrorMemoryAllocation;
+  return cudaMallocAsync(reinterpret_cast<void**>(p), bytes, s);
+}
+template <typename T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  if(take_injected_alloc_failure()) return cudaErrorMemoryAllocation;
+  return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+inline int64_t int32_index_limit() {
+  return faults().int32_limit.load(std::memory_order_relaxed);
+}
+
+// Time limit of every barrier wait in the tensor-core kernels, nanoseconds
+// (macis_b200_set_wait_limit_ns; 2 s by default). A wait that runs out makes
+// the kernel record an error, drain its copies and MMAs in flight (fixed
+// 100 ms bounds), free its TMEM and return; the call reports ETIMEOUT.
+constexpr uint64_t kDefaultWaitLimitNs = 2000000000ull;
+inline std::atomic<uint64_t>& wait_limit_slot() {
+  static std::atomic<uint64_t> v{kDefaultWaitLimitNs};
+  return v;
+}
+inline uint64_t wait_limit_ns() {
+  return wait_limit_slot().load(std::memory_order_relaxed);
+}
 
 inline int num_sms() {
   static int n = 0;

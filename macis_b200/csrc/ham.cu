@@ -92,13 +92,13 @@ void ham_create(macis_b200_ham* h, int nbits, size_t norb, const double* T,
       for(size_t q = 0; q < n; ++q)
         for(size_t p = 0; p < n; ++p)
           v[p + n * (q + n * (r + n * s))] = V[p + LDV * (q + LDV * (r + LDV * s))];
-  MB_CUDA(cudaMalloc(&h->T, n2 * 8));
-  MB_CUDA(cudaMalloc(&h->V, n4 * 8));
-  MB_CUDA(cudaMalloc(&h->G, n4 * 8));
-  MB_CUDA(cudaMalloc(&h->G_red, n3 * 8));
-  MB_CUDA(cudaMalloc(&h->V_red, n3 * 8));
-  MB_CUDA(cudaMalloc(&h->G2_red, n2 * 8));
-  MB_CUDA(cudaMalloc(&h->V2_red, n2 * 8));
+  MB_CUDA(dev_malloc(&h->T, n2 * 8));
+  MB_CUDA(dev_malloc(&h->V, n4 * 8));
+  MB_CUDA(dev_malloc(&h->G, n4 * 8));
+  MB_CUDA(dev_malloc(&h->G_red, n3 * 8));
+  MB_CUDA(dev_malloc(&h->V_red, n3 * 8));
+  MB_CUDA(dev_malloc(&h->G2_red, n2 * 8));
+  MB_CUDA(dev_malloc(&h->V2_red, n2 * 8));
   MB_CUDA(cudaMemcpyAsync(h->T, t.data(), n2 * 8, cudaMemcpyHostToDevice, h->stream));
   MB_CUDA(cudaMemcpyAsync(h->V, v.data(), n4 * 8, cudaMemcpyHostToDevice, h->stream));
   g_from_v_k<<<grid_for(n4, 256, 8 * num_sms()), 256, 0, h->stream>>>(h->V, h->G, int(n)), note_launch();

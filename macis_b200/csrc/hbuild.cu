@@ -1623,7 +1623,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
 
   out->m = int64_t(nbra);
   out->n = int64_t(nket);
-  MB_CUDA(cudaMallocAsync(&out->diag, std::max<size_t>(nbra, 1) * 8, s));
+  MB_CUDA(dev_malloc_async(&out->diag, std::max<size_t>(nbra, 1) * 8, s));
   MB_CUDA(cudaMemsetAsync(out->diag, 0, std::max<size_t>(nbra, 1) * 8, s));
   int64_t* rowptr64 = A.get<int64_t>(nbra + 1);
   int64_t* rowcnt = A.get<int64_t>(nbra + 1);
@@ -1638,10 +1638,10 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
   } ev;
   if(nbra == 0 || nket == 0) {
     out->nnz = 0;
-    MB_CUDA(cudaMallocAsync(&out->rowptr, (nbra + 1) * sizeof(CI), s));
+    MB_CUDA(dev_malloc_async(&out->rowptr, (nbra + 1) * sizeof(CI), s));
     MB_CUDA(cudaMemsetAsync(out->rowptr, 0, (nbra + 1) * sizeof(CI), s));
-    MB_CUDA(cudaMallocAsync(&out->colind, 256, s));
-    MB_CUDA(cudaMallocAsync(&out->nzval, 256, s));
+    MB_CUDA(dev_malloc_async(&out->colind, 256, s));
+    MB_CUDA(dev_malloc_async(&out->nzval, 256, s));
     MB_CUDA(cudaStreamSynchronize(s));
     return;
   }
@@ -1725,8 +1725,8 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     exclusive_scan<int64_t, int64_t>(rowcnt, rowptr64, nbra, rowptr64 + nbra, A);
     nnz_ub = to_host(rowptr64 + nbra, s);
     out->nnz_candidates = nnz_ub;
-    MB_CUDA(cudaMallocAsync(&colind, std::max<int64_t>(nnz_ub, 1) * sizeof(CI), s));
-    MB_CUDA(cudaMallocAsync(&nzval, std::max<int64_t>(nnz_ub, 1) * sizeof(VT), s));
+    MB_CUDA(dev_malloc_async(&colind, std::max<int64_t>(nnz_ub, 1) * sizeof(CI), s));
+    MB_CUDA(dev_malloc_async(&nzval, std::max<int64_t>(nnz_ub, 1) * sizeof(VT), s));
     {
       const int nn0 = h->norb;
       const int64_t na_ = to_host(aoff + UA, s), n2_ = to_host(l2off + UB, s),
@@ -1823,7 +1823,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     const unsigned g = unsigned(std::max(1, per_sm) * sms);
     if(!h->VT) {
       const size_t n4 = size_t(nn) * nn * nn * nn;
-      MB_CUDA(cudaMalloc(&h->VT, n4 * 8));
+      MB_CUDA(dev_malloc(&h->VT, n4 * 8));
       v_pair_transpose_k<<<grid_for(n4, 256, 8 * sms), 256, 0, s>>>(h->V, h->VT, nn), note_launch();
     }
     cudaEventRecord(ev[0], s);
@@ -1840,8 +1840,8 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     exclusive_scan<int64_t, int64_t>(rowcnt, rowptr64, nbra, rowptr64 + nbra, A);
     nnz_ub = to_host(rowptr64 + nbra, s);
     out->nnz_candidates = nnz_ub;
-    MB_CUDA(cudaMallocAsync(&colind, std::max<int64_t>(nnz_ub, 1) * sizeof(CI), s));
-    MB_CUDA(cudaMallocAsync(&nzval, std::max<int64_t>(nnz_ub, 1) * sizeof(VT), s));
+    MB_CUDA(dev_malloc_async(&colind, std::max<int64_t>(nnz_ub, 1) * sizeof(CI), s));
+    MB_CUDA(dev_malloc_async(&nzval, std::max<int64_t>(nnz_ub, 1) * sizeof(VT), s));
     // long rows
     uint32_t* lf = A.get<uint32_t>(nbra + 1);
     uint32_t* lpos = A.get<uint32_t>(nbra + 1);
@@ -1927,13 +1927,13 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
   const int64_t nnz = to_host(newptr + nbra, s);
   out->nnz = nnz;
   if(sizeof(CI) == 4)
-    MB_REQUIRE(nnz <= int64_t(INT32_MAX), MACIS_B200_ECAPACITY,
+    MB_REQUIRE(nnz <= int32_index_limit(), MACIS_B200_ECAPACITY,
                "nnz exceeds the int32 index range; use 64-bit indices");
   if(nnz != nnz_ub) {
     CI* ci2 = nullptr;
     VT* nz2 = nullptr;
-    MB_CUDA(cudaMallocAsync(&ci2, std::max<int64_t>(nnz, 1) * sizeof(CI), s));
-    MB_CUDA(cudaMallocAsync(&nz2, std::max<int64_t>(nnz, 1) * sizeof(VT), s));
+    MB_CUDA(dev_malloc_async(&ci2, std::max<int64_t>(nnz, 1) * sizeof(CI), s));
+    MB_CUDA(dev_malloc_async(&nz2, std::max<int64_t>(nnz, 1) * sizeof(VT), s));
     if(direct)
       compact_marked_k<CI, VT><<<grid_for(nbra * 32, 256, 16 * sms), 256, 0, s>>>(
           rowptr64, newptr, nbra, colind, nzval, ci2, nz2), note_launch();
@@ -1945,7 +1945,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
     colind = ci2;
     nzval = nz2;
   }
-  MB_CUDA(cudaMallocAsync(&out->rowptr, (nbra + 1) * sizeof(CI), s));
+  MB_CUDA(dev_malloc_async(&out->rowptr, (nbra + 1) * sizeof(CI), s));
   rowptr_cast_k<CI><<<grid_for(nbra + 1, 256, 8 * sms), 256, 0, s>>>(
       newptr, nbra + 1, static_cast<CI*>(out->rowptr)), note_launch();
   out->colind = colind;

@@ -44,19 +44,21 @@ struct GemmOut {
 template <int MODE>
 __global__ void __launch_bounds__(128)
     gemm_tc_k(const __nv_bfloat16* A, int64_t lda, const __nv_bfloat16* B,
-              int64_t ldb, int64_t K, GemmOut o, int* err) {
+              int64_t ldb, int64_t K, GemmOut o, int* err, uint64_t limit_ns) {
   constexpr int ABYTES = GT_M * GT_K * 2;  // 16 KB
   constexpr int BBYTES = GT_N * GT_K * 2;  // 8 KB
   constexpr uint32_t A_LBO = GT_M * 16, B_LBO = GT_N * 16;
   constexpr uint32_t IDESC = tc::idesc_bf16(GT_M, GT_N);
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t bar[2];
+  __shared__ uint64_t drain;  // used once, by the timeout path only
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t m0 = int64_t(blockIdx.y) * GT_M, n0 = int64_t(blockIdx.x) * GT_N;
   if(tid == 0) {
     tc::mbar_init(&bar[0], 1);
     tc::mbar_init(&bar[1], 1);
+    tc::mbar_init(&drain, 1);
     tc::mbar_init_fence();
   }
   if(warp == 0) tc::tmem_alloc(&tslot, GT_N);
@@ -71,7 +73,8 @@ __global__ void __launch_bounds__(128)
     uint8_t* as = smem + s * (ABYTES + BBYTES);
     uint8_t* bs = as + ABYTES;
     // the MMAs of chunk c-2 read this stage
-    if(c >= 2 && !tc::mbar_wait(&bar[s], uint32_t(((c - 2) >> 1) & 1)))
+    if(c >= 2 &&
+       !tc::mbar_wait(&bar[s], uint32_t(((c - 2) >> 1) & 1), limit_ns))
       fail = true;
     if(__syncthreads_or(fail)) {
       abort = true;
@@ -110,7 +113,8 @@ __global__ void __launch_bounds__(128)
   // the last commit covers every MMA of this tile
   if(!abort && nk > 0) {
     const int64_t c = nk - 1;
-    if(!tc::mbar_wait(&bar[c & 1], uint32_t((c >> 1) & 1))) fail = true;
+    if(!tc::mbar_wait(&bar[c & 1], uint32_t((c >> 1) & 1), limit_ns))
+      fail = true;
   }
   if(__syncthreads_or(fail)) abort = true;
   if(!abort) {
@@ -147,6 +151,11 @@ __global__ void __launch_bounds__(128)
     }
   } else if(tid == 0) {
     atomicExch(err, 1);
+    // wait (bounded) for every MMA this thread issued before TMEM is freed
+    // and the operand tiles are released: a commit on the unused drain
+    // barrier completes its phase 0 after all of them
+    tc::mma_commit(&drain);
+    tc::mbar_wait(&drain, 0u, 100000000ull);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -286,7 +295,7 @@ double uniform01(uint64_t& s) { return double(splitmix(s) >> 11) * 0x1.0p-53; }
 template <typename T>
 T* dalloc(size_t n) {
   void* p = nullptr;
-  MB_CUDA(cudaMalloc(&p, std::max<size_t>(n * sizeof(T), 256)));
+  MB_CUDA(dev_malloc(&p, std::max<size_t>(n * sizeof(T), 256)));
   return static_cast<T*>(p);
 }
 
@@ -295,6 +304,10 @@ void check_err(macis_b200_mlp* m) {
   MB_CUDA(cudaMemcpyAsync(&e, m->err, sizeof(int), cudaMemcpyDeviceToHost,
                           m->stream));
   MB_CUDA(cudaStreamSynchronize(m->stream));
+  if(e) {  // cleared, so that the next call starts clean
+    MB_CUDA(cudaMemsetAsync(m->err, 0, sizeof(int), m->stream));
+    MB_CUDA(cudaStreamSynchronize(m->stream));
+  }
   MB_REQUIRE(e == 0, MACIS_B200_ETIMEOUT,
              "screening network kernel timed out waiting on a barrier");
 }
@@ -313,7 +326,7 @@ void ensure_batch(macis_b200_mlp* m, int64_t B) {
   m->scratch.clear();
   auto get = [&](size_t bytes) {
     void* p = nullptr;
-    MB_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+    MB_CUDA(dev_malloc(&p, std::max<size_t>(bytes, 256)));
     MB_CUDA(cudaMemset(p, 0, std::max<size_t>(bytes, 256)));
     m->scratch.push_back(p);
     return p;
@@ -357,7 +370,8 @@ void launch_fwd(const macis_b200_mlp* m, const Src& src, int64_t nrows,
                                int(smem)));
   const int64_t tiles = (nrows + MLP_TM - 1) / MLP_TM;
   const unsigned grid = unsigned(std::min<int64_t>(tiles, num_sms()));
-  kern<<<grid, MLP_TM, smem, s>>>(weights_of(m), src, nrows, y, taps, m->err),
+  kern<<<grid, MLP_TM, smem, s>>>(weights_of(m), src, nrows, y, taps, m->err,
+                                  wait_limit_ns()),
       note_launch();
   MB_CUDA(cudaGetLastError());
 }
@@ -375,7 +389,7 @@ void gemm(const macis_b200_mlp* m, const uint16_t* A, int64_t lda,
   dim3 grid(unsigned(N / GT_N), unsigned(M / GT_M));
   kern<<<grid, 128, smem, s>>>(reinterpret_cast<const __nv_bfloat16*>(A), lda,
                                reinterpret_cast<const __nv_bfloat16*>(B), ldb,
-                               K, o, m->err), note_launch();
+                               K, o, m->err, wait_limit_ns()), note_launch();
   MB_CUDA(cudaGetLastError());
 }
 
@@ -521,7 +535,7 @@ double mlp_gradients_device(macis_b200_mlp* m, const uint16_t* X,
   for(int64_t i = 0; i < n; ++i) id[i] = i;
   MB_CUDA(cudaMemcpyAsync(m->idx, id.data(), n * 8, cudaMemcpyHostToDevice, s));
   double* dl = nullptr;
-  MB_CUDA(cudaMallocAsync(&dl, 8, s));
+  MB_CUDA(dev_malloc_async(&dl, 8, s));
   MB_CUDA(cudaMemsetAsync(dl, 0, 8, s));
   fwd_bwd(m, X, t, m->idx, n, B, dl, s);
   double l = 0;
@@ -543,8 +557,8 @@ double mlp_train_device(macis_b200_mlp* m, const uint16_t* X, const float* t,
   ensure_batch(m, B);
   int64_t* perm = nullptr;
   double* dl = nullptr;
-  MB_CUDA(cudaMallocAsync(&perm, size_t(S) * 8, s));
-  MB_CUDA(cudaMallocAsync(&dl, 8, s));
+  MB_CUDA(dev_malloc_async(&perm, size_t(S) * 8, s));
+  MB_CUDA(dev_malloc_async(&dl, 8, s));
   std::vector<int64_t> p(S);
   for(int64_t i = 0; i < S; ++i) p[i] = i;
   uint64_t st = seed ^ 0x5DEECE66Dull;

@@ -63,7 +63,7 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
 inline size_t mlp_fwd_smem_bytes(int din) {
   const int kx = din > MLP_H ? din : MLP_H;
   return size_t(kx) * MLP_TM * 2 + size_t(MLP_STAGES) * MLP_WCHUNK +
-         (2 * MLP_STAGES + 1) * 8 + 3 * MLP_H * 4 + 16;
+         (2 * MLP_STAGES + 2) * 8 + 3 * MLP_H * 4 + 16;
 }
 
 // Dense row source: X row-major [nrows][din] BF16.
@@ -82,11 +82,13 @@ struct DenseRows {
 };
 
 // Forward over nrows rows; y[row] = network output. TRAIN also writes the
-// taps. err (device) is set to a non-zero code if a wait timed out.
+// taps. Every barrier wait gives up after limit_ns nanoseconds; then err
+// (device) is set, the CTA waits (at most 100 ms each) for its bulk copies
+// and MMAs still in flight, frees its TMEM and returns.
 template <class Src, bool TRAIN>
 __global__ void __launch_bounds__(MLP_TM, 1)
     mlp_fwd_k(MlpWeights W, Src src, int64_t nrows, float* y, MlpTaps tap,
-              int* err) {
+              int* err, uint64_t limit_ns) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -99,7 +101,8 @@ __global__ void __launch_bounds__(MLP_TM, 1)
   uint64_t* full = reinterpret_cast<uint64_t*>(ws + MLP_STAGES * MLP_WCHUNK);
   uint64_t* empty = full + MLP_STAGES;
   uint64_t* accb = empty + MLP_STAGES;
-  float* sb1 = reinterpret_cast<float*>(accb + 1);
+  uint64_t* drain = accb + 1;  // used once, by the timeout path only
+  float* sb1 = reinterpret_cast<float*>(drain + 1);
   float* sb2 = sb1 + MLP_H;
   float* sw3 = sb2 + MLP_H;
 
@@ -119,6 +122,7 @@ __global__ void __launch_bounds__(MLP_TM, 1)
       tc::mbar_init(empty + s, 1);
     }
     tc::mbar_init(accb, 1);
+    tc::mbar_init(drain, 1);
     tc::mbar_init_fence();
   }
   if(warp == 0) tc::tmem_alloc(&tslot, MLP_H);
@@ -168,7 +172,8 @@ __global__ void __launch_bounds__(MLP_TM, 1)
         const uint32_t xaddr = tc::smem_addr(xs);
         for(int c = 0; c < nch && !fail; ++c, ++g_mma) {
           const int s = int(g_mma % MLP_STAGES);
-          if(!tc::mbar_wait(full + s, uint32_t((g_mma / MLP_STAGES) & 1))) {
+          if(!tc::mbar_wait(full + s, uint32_t((g_mma / MLP_STAGES) & 1),
+                            limit_ns)) {
             fail = true;
             break;
           }
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(MLP_TM, 1)
           if(g_mma >= 1 && g_load < total) {
             const int64_t gp = g_mma - 1;
             if(!tc::mbar_wait(empty + gp % MLP_STAGES,
-                              uint32_t((gp / MLP_STAGES) & 1))) {
+                              uint32_t((gp / MLP_STAGES) & 1), limit_ns)) {
               fail = true;
               break;
             }
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(MLP_TM, 1)
         tc::mma_commit(accb);
       }
       // every thread: the accumulator of this layer
-      if(!fail && !tc::mbar_wait(accb, acc_n & 1)) fail = true;
+      if(!fail && !tc::mbar_wait(accb, acc_n & 1, limit_ns)) fail = true;
       ++acc_n;
       if(__syncthreads_or(fail)) {
         abort = true;
@@ -259,13 +264,17 @@ __global__ void __launch_bounds__(MLP_TM, 1)
   if(abort) {
     if(tid == 0) {
       atomicExch(err, 1);
-      // bounded wait for the bulk copies still in flight
+      // bounded wait for the bulk copies still in flight: at most one per
+      // stage is outstanding, and its phase is the stage's current one
       for(int64_t g = g_mma; g < g_load; ++g)
         tc::mbar_wait(full + g % MLP_STAGES, uint32_t((g / MLP_STAGES) & 1),
                       100000000ull);
-      // and for the MMAs issued so far
-      tc::mma_commit(accb);
-      tc::mbar_wait(accb, acc_n & 1, 100000000ull);
+      // and for every MMA this thread issued: a commit on the unused drain
+      // barrier completes its phase 0 only after all of them (a commit on
+      // accb could not be waited for unambiguously: its previous phase may
+      // still be open)
+      tc::mma_commit(drain);
+      tc::mbar_wait(drain, 0u, 100000000ull);
     }
   }
   tc::fence_before_sync();

@@ -32,7 +32,7 @@ struct Arena {
     void* p = nullptr;
     size_t bytes = n * sizeof(T);
     if(bytes == 0) bytes = 256;
-    MB_CUDA(cudaMallocAsync(&p, (bytes + 255) & ~size_t(255), s));
+    MB_CUDA(dev_malloc_async(&p, (bytes + 255) & ~size_t(255), s));
     ptrs.push_back(p);
     return static_cast<T*>(p);
   }
