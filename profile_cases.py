@@ -21,8 +21,8 @@
         # the same on n = 64, 16a/16b, bitset<128>; learned_mixed also runs
         # one exact search from its last core set and reports the top-k
         # recall of the screened one
-    python profile_cases.py c5 --ntdets 51200 --refine 1
-        # n = 100, 20a/20b, bitset<256>, exact search, FP64 Davidson
+    python profile_cases.py c5 --ntdets 51200 --refine 1 --mode ...
+        # n = 100, 20a/20b, bitset<256>, modes as c3
 
 Each case runs its hot call a few times (--reps) and prints one timing line.
 """
@@ -265,9 +265,8 @@ def main():
     elif a.case == "c4":
         c3(a.ntdets, a.mode, n=64, k=16)
     elif a.case == "c5":
-        # n = 100, 20a/20b, bitset<256>: exact search only (the network
-        # input of 256-bit dets is wider than the network takes)
-        c3(a.ntdets, "fp64", refine=a.refine, n=100, k=20, nbits=256)
+        # n = 100, 20a/20b, bitset<256> (network input 320 columns)
+        c3(a.ntdets, a.mode, refine=a.refine, n=100, k=20, nbits=256)
     else:
         raise SystemExit(f"unknown case {a.case}")
 
