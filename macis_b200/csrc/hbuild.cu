@@ -1686,8 +1686,12 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       int hb[2];
       MB_CUDA(cudaMemcpyAsync(hb, bad, 8, cudaMemcpyDeviceToHost, s));
       MB_CUDA(cudaStreamSynchronize(s));
+      // the fill keeps a singles table of 2 norb^2 doubles per warp in
+      // shared memory: spaces whose orbitals make it too large (norb above
+      // ~33) take the general path even when they have the product layout
       direct = hb[0] == 0 && hb[1] == 0 && UA < (size_t(1) << 31) &&
-               UB < (size_t(1) << 31);
+               UB < (size_t(1) << 31) && h->norb <= 127 &&
+               dp_shared_layout(int(h->norb), 512, 1024).bytes <= 220 * 1024;
     }
   }
 

@@ -224,3 +224,23 @@ def test_general_path_large_groups(ref, nbits):
     assert_csr_equal(A.to_host(), ref.build_csr(ref.ham(nbits, n, T, V), dets,
                                                 dets, np.finfo(float).eps,
                                                 nthreads=8))
+
+
+def test_product_layout_with_many_orbitals_takes_general_path(ref):
+    """A selected space in the product layout (one alpha string, distinct
+    betas) at 48 orbitals: the direct-product fill's per-warp singles table
+    would not fit in shared memory, so the general path builds it,
+    bit-exact with the reference."""
+    from macis_b200.integrals import synthetic_integrals
+    n, k = 48, 12
+    T, V = synthetic_integrals(n, 1)
+    hf = (1 << k) - 1
+    betas = sorted({hf} | {hf ^ (1 << i) ^ (1 << a) for i in range(k)
+                           for a in range(k, n)})
+    dets = mb.sd.make_dets([hf] * len(betas), betas, 128)
+    H = mb.HamiltonianGenerator(T, V, 128)
+    A = mb.make_csr_hamiltonian(dets, H, np.finfo(float).eps)
+    assert A.build_stats()["direct_product"] == 0
+    assert_csr_equal(A.to_host(), ref.build_csr(ref.ham(128, n, T, V), dets,
+                                                dets, np.finfo(float).eps,
+                                                nthreads=8))
