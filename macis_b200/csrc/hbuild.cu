@@ -544,6 +544,15 @@ __global__ void __launch_bounds__(DP_THREADS, DP_CTAS)
       el = s2 ? sl2[lane]
               : make_uint2(uint32_t(__ldg(d.l2col + l2b + lane)),
                            __ldg(d.l2info + l2b + lane));
+    // beta L2 entries 32..63 (n2l <= 64): each lane also holds entry lane + 32
+    // and emits it in the same segment iteration as entry lane
+    const bool fold = n2l > 32 && n2l <= 64;
+    uint2 el2 = make_uint2(0u, 0u);
+    const bool has2 = fold && lane + 32 < n2l;
+    if(has2)
+      el2 = s2 ? sl2[lane + 32]
+               : make_uint2(uint32_t(__ldg(d.l2col + l2b + lane + 32)),
+                            __ldg(d.l2info + l2b + lane + 32));
     using CS = typename std::conditional<sizeof(CI) == 4, int, long long>::type;
     CS* __restrict__ rcs = reinterpret_cast<CS*>(rc);
     // entries whose column differs from the row (every phase but the
@@ -643,7 +652,37 @@ __global__ void __launch_bounds__(DP_THREADS, DP_CTAS)
       }
       __syncwarp();
       const int k2 = __popc(m2);
-      if(lane < n2l) {
+      if(fold) {
+        const bool bsame = ((el.y >> 29) & 3u) == 0;
+        const uint32_t boff = el.y & 0x0FFFFFFFu, bsg = el.y & 0x80000000u;
+        const bool bsame2 = ((el2.y >> 29) & 3u) == 0;
+        const uint32_t boff2 = el2.y & 0x0FFFFFFFu, bsg2 = el2.y & 0x80000000u;
+        CS* __restrict__ rcl = rcs + lane;
+        VT* __restrict__ rvl = rv + lane;
+        for(int q = 0; q < k2; ++q) {
+          const int4 sd = seg_d[wid][q];
+          const double sgl = seg_single[wid][q];
+          const double v = __ldg(gVT + uint32_t(sd.z + int(boff)));
+          const double v2 = has2 ? __ldg(gVT + uint32_t(sd.z + int(boff2))) : 0.0;
+          const double hv = __hiloint2double(
+              __double2hiint(v) ^ (sd.w ^ int(bsg)), __double2loint(v));
+          const double h = bsame ? sgl : hv;
+          const bool keep = fabs(h) > thresh;
+          dropped += keep ? 0 : 1;
+          const uint32_t p = uint32_t(sd.x);
+          __stcs(rcl + p, CS(keep ? sd.y + int32_t(el.x) : -1));
+          __stcs(rvl + p, store_val<VT>(h, false));
+          if(has2) {
+            const double hv2 = __hiloint2double(
+                __double2hiint(v2) ^ (sd.w ^ int(bsg2)), __double2loint(v2));
+            const double h2 = bsame2 ? sgl : hv2;
+            const bool keep2 = fabs(h2) > thresh;
+            dropped += keep2 ? 0 : 1;
+            __stcs(rcl + p + 32, CS(keep2 ? sd.y + int32_t(el2.x) : -1));
+            __stcs(rvl + p + 32, store_val<VT>(h2, false));
+          }
+        }
+      } else if(lane < n2l) {
         // branch-free body: the same-beta entry (offset 0) also loads from
         // its VT row and then selects the alpha-single value
         const bool bsame = ((el.y >> 29) & 3u) == 0;
@@ -667,7 +706,7 @@ __global__ void __launch_bounds__(DP_THREADS, DP_CTAS)
           __stcs(rvl + p, store_val<VT>(h, false));
         }
       }
-      if(n2l > 32) {  // list entries 32.. of every segment, flattened
+      if(n2l > 64) {  // list entries 32.. of every segment, flattened
         const int32_t w2 = n2l - 32;
         const int32_t tot2 = k2 * w2;
         const float invw = 1.0f / float(w2);

@@ -137,7 +137,8 @@ def test_injected_out_of_memory(faults):
 def test_injected_int32_capacity(faults):
     T, V, d = fci(9, 4, 4, 64, seed=5)
     H = mb.HamiltonianGenerator(T, V, 64)
-    E0, _ = mb.selected_ci_diag(d, H, EPS, 80, 1e-8)
+    dav = dict(restart_keep=8, max_iter=3000)
+    E0, _ = mb.selected_ci_diag(d, H, EPS, 40, 1e-8, **dav)
     A = mb.make_csr_hamiltonian(d, H, EPS)
     faults(_lib.FAULT_INT32_LIMIT, A.nnz - 1)
     with pytest.raises(mb.MacisError) as e:
@@ -148,6 +149,7 @@ def test_injected_int32_capacity(faults):
     # index_t=None: int32 first, int64 after the capacity error, remembered
     # for later spaces of this generator
     t = {}
-    E1, _ = mb.selected_ci_diag(d, H, EPS, 80, 1e-8, index_t=None, timings=t)
+    E1, _ = mb.selected_ci_diag(d, H, EPS, 40, 1e-8, index_t=None, timings=t,
+                                **dav)
     assert abs(E1 - E0) < 1e-9 and t["nnz"] == A.nnz
     assert H._int64_from_ndets == len(d)
