@@ -14,6 +14,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -271,19 +272,23 @@ constexpr size_t rs_stage_bytes() {
   return size_t(RS_TILE) * (8 * NW + sizeof(P));
 }
 
-// One digit pass. Every warp ranks its 256 items (__match_any_sync, input
-// order), the block turns the per-warp counts into each item's position in
-// a bucket-ordered copy of the tile in shared memory, and then consecutive
-// threads write consecutive items of a bucket to consecutive addresses, so
-// the stores of a bucket run (8 items per bucket on average) coalesce.
-// Stable: within a bucket items keep warp, round and lane order, which is
-// the input order. Keys are read twice (the second time from L2) so that no
-// per-thread key array is needed.
-template <int NW, typename P>
-__global__ void __launch_bounds__(RS_THREADS, 4)
-    radix_scatter_k(const uint64_t* keys, const P* vals, size_t n, int shift,
-                    const uint64_t* offsets, unsigned nblocks,
-                    uint64_t* keys_out, P* vals_out) {
+// One digit pass over one tile of RS_TILE items starting at tile0. Every
+// warp ranks its 256 items (__match_any_sync, input order), the block turns
+// the per-warp counts into each item's position in a bucket-ordered copy of
+// the tile in shared memory, and then consecutive threads write consecutive
+// items of a bucket to consecutive addresses, so the stores of a bucket run
+// (8 items per bucket on average) coalesce. Stable: within a bucket items
+// keep warp, round and lane order, which is the input order. Keys are read
+// twice (the second time from L2) so that no per-thread key array is needed.
+// `resolve(d, count)` is called by thread d (one per digit) with the tile's
+// count of digit d, between two block barriers, and returns the output
+// position of the tile's first item with that digit.
+template <int NW, typename P, class Resolve>
+__device__ __forceinline__ void rs_tile_pass(const uint64_t* keys,
+                                             const P* vals, size_t n,
+                                             int shift, size_t tile0,
+                                             uint64_t* keys_out, P* vals_out,
+                                             Resolve resolve) {
   extern __shared__ __align__(16) uint8_t rs_smem[];
   uint64_t* skeys = reinterpret_cast<uint64_t*>(rs_smem);
   P* svals = reinterpret_cast<P*>(skeys + size_t(RS_TILE) * NW);
@@ -294,9 +299,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for(int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS)
     (&wcount[0][0])[d] = 0;
-  boff[threadIdx.x] = offsets[size_t(threadIdx.x) * nblocks + blockIdx.x];
   __syncthreads();
-  const size_t tile0 = size_t(blockIdx.x) * RS_TILE;
   const size_t wbase = tile0 + size_t(wid) * RS_WARP_ITEMS;
   uint32_t rank[RS_IPT];
   unsigned dig[RS_IPT];
@@ -322,7 +325,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
   __syncthreads();
   {
     // per digit: exclusive prefix over warps, then over digits (bucket
-    // starts inside the tile)
+    // starts inside the tile), and the digit's output position
     const int d = threadIdx.x;
     uint32_t acc = 0;
 #pragma unroll
@@ -332,6 +335,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
       acc += c;
     }
     bstart[d] = block_excl_scan<uint32_t>(acc, scan_sh, nullptr);
+    boff[d] = resolve(d, acc);
   }
   __syncthreads();
 #pragma unroll
@@ -354,6 +358,109 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
   }
 }
 
+// One digit pass with per-block bucket offsets from radix_hist_k + scan.
+template <int NW, typename P>
+__global__ void __launch_bounds__(RS_THREADS, 4)
+    radix_scatter_k(const uint64_t* keys, const P* vals, size_t n, int shift,
+                    const uint64_t* offsets, unsigned nblocks,
+                    uint64_t* keys_out, P* vals_out) {
+  // issued before the ranking: its latency hides behind the tile loads
+  const uint64_t my_off =
+      offsets[size_t(threadIdx.x) * nblocks + blockIdx.x];
+  rs_tile_pass<NW, P>(keys, vals, n, shift, size_t(blockIdx.x) * RS_TILE,
+                      keys_out, vals_out,
+                      [&](int, uint32_t) { return my_off; });
+}
+
+// ------------------------------------------------------ one-sweep passes
+// All digit histograms of the sort in one read of the keys: hist[p][d] =
+// number of keys whose digit at shifts[p] is d (shared-memory counts per
+// block, then one global add per (p, d)).
+constexpr int RS_MAX_PASSES = 32;
+// sorts of at least this many keys use the one-sweep passes
+constexpr size_t RS_ONESWEEP_MIN = size_t(1) << 16;
+// polls of one look-back wait (each an L2 round trip) before it gives up
+constexpr long long RS_SPIN_LIMIT = 1ll << 22;
+template <int NW>
+__global__ void __launch_bounds__(RS_THREADS)
+    rs_hist_all_k(const uint64_t* keys, size_t n, const int* shifts, int np,
+                  unsigned long long* hist) {
+  __shared__ uint32_t h[RS_MAX_PASSES][256];
+  __shared__ int sh_shift[RS_MAX_PASSES];
+  for(int i = threadIdx.x; i < np * 256; i += RS_THREADS) (&h[0][0])[i] = 0;
+  if(threadIdx.x < np) sh_shift[threadIdx.x] = shifts[threadIdx.x];
+  __syncthreads();
+  for(size_t i = size_t(blockIdx.x) * RS_THREADS + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * RS_THREADS) {
+    const Key<NW> k = load_key<NW>(keys, i);
+    for(int p = 0; p < np; ++p) atomicAdd(&h[p][digit_of<NW>(k, sh_shift[p])], 1u);
+  }
+  __syncthreads();
+  for(int i = threadIdx.x; i < np * 256; i += RS_THREADS)
+    if((&h[0][0])[i]) atomicAdd(hist + i, (unsigned long long)(&h[0][0])[i]);
+}
+
+// Status word of (tile, digit) in a one-sweep pass: the tile's count of the
+// digit once ranked (AGG) or the inclusive count over tiles 0..tile (PRE).
+constexpr uint64_t RS_AGG = 1ull << 62, RS_PRE = 2ull << 62;
+constexpr uint64_t RS_VAL = (1ull << 62) - 1;
+
+__device__ __forceinline__ uint64_t rs_ld_status(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void rs_st_status(uint64_t* p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// One digit pass in one kernel: blocks take tiles in order from a counter,
+// publish their per-digit counts, and find the counts of all earlier tiles
+// by looking back over the status words (decoupled look-back), so no
+// separate histogram or scan of the pass is needed. Every look-back wait is
+// bounded by `spin_limit` polls; a block that gives up sets *err and the
+// host reruns the pass with radix_hist_k / radix_scatter_k.
+template <int NW, typename P>
+__global__ void __launch_bounds__(RS_THREADS, 4)
+    rs_onesweep_k(const uint64_t* keys, const P* vals, size_t n, int shift,
+                  const unsigned long long* bucket, uint64_t* status,
+                  unsigned* tile_counter, int* err, uint64_t* keys_out,
+                  P* vals_out, long long spin_limit) {
+  __shared__ uint32_t tile_sh;
+  if(threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = tile_sh;
+  const uint64_t base_d = bucket[threadIdx.x];
+  rs_tile_pass<NW, P>(
+      keys, vals, n, shift, size_t(tile) * RS_TILE, keys_out, vals_out,
+      [&](int d, uint32_t count) -> uint64_t {
+        uint64_t* mine = status + size_t(tile) * 256 + d;
+        if(tile == 0) {
+          rs_st_status(mine, RS_PRE | count);
+          return base_d;
+        }
+        rs_st_status(mine, RS_AGG | count);
+        uint64_t excl = 0;
+        long long polls = 0;
+        for(int64_t t = int64_t(tile) - 1; t >= 0;) {
+          const uint64_t w = rs_ld_status(status + size_t(t) * 256 + d);
+          const uint64_t flag = w & ~RS_VAL;
+          if(flag == 0) {
+            if(++polls > spin_limit) {
+              atomicExch(err, 1);
+              break;
+            }
+            continue;
+          }
+          excl += w & RS_VAL;
+          if(flag == RS_PRE) break;
+          --t;
+        }
+        rs_st_status(mine, RS_PRE | (excl + count));
+        return base_d + excl;
+      });
+}
+
 // Stable sort of n keys (NW words each) with optional payload. The sorted
 // result ends in (keys, vals); keys_alt/vals_alt are scratch of the same
 // size. Returns the number of digit passes run.
@@ -373,25 +480,90 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
   MB_CUDA(cudaFuncSetAttribute(radix_scatter_k<NW, P>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(stage)));
-  uint32_t* counts = A.get<uint32_t>(size_t(256) * nblocks);
-  uint64_t* offs = A.get<uint64_t>(size_t(256) * nblocks);
   int passes = 0;
+  std::vector<int> shifts;
+  for(int w = 0; w < NW; ++w)
+    for(int sft = 0; sft < 64; sft += 8)
+      if((vary[w] >> sft) & 255ull) shifts.push_back(64 * w + sft);
+  const int np = int(shifts.size());
   uint64_t *kin = keys, *kout = keys_alt;
   P *vin = vals, *vout = vals_alt;
-  for(int w = 0; w < NW; ++w)
-    for(int s = 0; s < 64; s += 8) {
-      if(((vary[w] >> s) & 255ull) == 0) continue;
-      const int shift = 64 * w + s;
-      radix_hist_k<NW><<<nblocks, RS_THREADS, 0, A.s>>>(kin, n, shift, counts,
-                                                        nblocks), note_launch();
-      exclusive_scan<uint32_t, uint64_t>(counts, offs, size_t(256) * nblocks,
-                                         nullptr, A);
-      radix_scatter_k<NW, P><<<nblocks, RS_THREADS, stage, A.s>>>(
-          kin, vin, n, shift, offs, nblocks, kout, vout), note_launch();
+  uint32_t* counts = nullptr;
+  uint64_t* offs = nullptr;
+  // classic pass: per-block histogram, scan, scatter
+  auto classic_pass = [&](int shift) {
+    if(!counts) {
+      counts = A.get<uint32_t>(size_t(256) * nblocks);
+      offs = A.get<uint64_t>(size_t(256) * nblocks);
+    }
+    radix_hist_k<NW><<<nblocks, RS_THREADS, 0, A.s>>>(kin, n, shift, counts,
+                                                      nblocks), note_launch();
+    exclusive_scan<uint32_t, uint64_t>(counts, offs, size_t(256) * nblocks,
+                                       nullptr, A);
+    radix_scatter_k<NW, P><<<nblocks, RS_THREADS, stage, A.s>>>(
+        kin, vin, n, shift, offs, nblocks, kout, vout), note_launch();
+  };
+  const char* force = getenv("MACIS_B200_SORT_CLASSIC");
+  const bool onesweep = n >= RS_ONESWEEP_MIN && np <= RS_MAX_PASSES &&
+                        !(force && force[0] == '1');
+  if(onesweep) {
+    // all digit histograms in one read, bucket starts per pass on the host
+    MB_CUDA(cudaFuncSetAttribute(rs_onesweep_k<NW, P>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(stage)));
+    int* d_shifts = A.get<int>(size_t(np));
+    MB_CUDA(cudaMemcpyAsync(d_shifts, shifts.data(), size_t(np) * sizeof(int),
+                            cudaMemcpyHostToDevice, A.s));
+    auto* hist = A.get<unsigned long long>(size_t(np) * 256);
+    MB_CUDA(cudaMemsetAsync(hist, 0, size_t(np) * 256 * 8, A.s));
+    rs_hist_all_k<NW><<<grid_for(n, RS_THREADS, 4 * size_t(num_sms())),
+                        RS_THREADS, 0, A.s>>>(keys, n, d_shifts, np, hist),
+        note_launch();
+    std::vector<unsigned long long> h(size_t(np) * 256);
+    MB_CUDA(cudaMemcpyAsync(h.data(), hist, h.size() * 8,
+                            cudaMemcpyDeviceToHost, A.s));
+    MB_CUDA(cudaStreamSynchronize(A.s));
+    for(int p = 0; p < np; ++p) {
+      unsigned long long acc = 0;
+      for(int d = 0; d < 256; ++d) {
+        const unsigned long long c = h[size_t(p) * 256 + d];
+        h[size_t(p) * 256 + d] = acc;
+        acc += c;
+      }
+    }
+    auto* bucket = A.get<unsigned long long>(h.size());
+    MB_CUDA(cudaMemcpyAsync(bucket, h.data(), h.size() * 8,
+                            cudaMemcpyHostToDevice, A.s));
+    uint64_t* status = A.get<uint64_t>(size_t(nblocks) * 256);
+    unsigned* counter = A.get<unsigned>(1);
+    int* err = A.get<int>(1);
+    MB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), A.s));
+    for(int p = 0; p < np; ++p) {
+      MB_CUDA(cudaMemsetAsync(status, 0, size_t(nblocks) * 256 * 8, A.s));
+      MB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), A.s));
+      rs_onesweep_k<NW, P><<<nblocks, RS_THREADS, stage, A.s>>>(
+          kin, vin, n, shifts[p], bucket + size_t(p) * 256, status, counter,
+          err, kout, vout, RS_SPIN_LIMIT), note_launch();
+      int e = 0;
+      MB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost,
+                              A.s));
+      MB_CUDA(cudaStreamSynchronize(A.s));
+      if(e) {  // a look-back gave up: this pass again, the classic way
+        MB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), A.s));
+        classic_pass(shifts[p]);
+      }
       std::swap(kin, kout);
       std::swap(vin, vout);
       ++passes;
     }
+  } else {
+    for(int p = 0; p < np; ++p) {
+      classic_pass(shifts[p]);
+      std::swap(kin, kout);
+      std::swap(vin, vout);
+      ++passes;
+    }
+  }
   if(kin != keys) {
     MB_CUDA(cudaMemcpyAsync(keys, kin, n * NW * 8, cudaMemcpyDeviceToDevice, A.s));
     if(vals)

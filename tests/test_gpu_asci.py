@@ -241,3 +241,25 @@ def test_screened_split_search_matches_whole(wcase):
     assert np.array_equal(split(True), whole2)
     with pytest.raises(mb.MacisError, match="recorded sample count"):
         nets[1].set_sample_targets(tmax[:-1])
+
+
+def test_onesweep_sort_matches_classic_passes(monkeypatch):
+    """The candidate sort with one-sweep digit passes (decoupled look-back)
+    against the classic histogram / scan / scatter passes
+    (MACIS_B200_SORT_CLASSIC=1): identical accumulated candidates and
+    scores, and identical selections, on an n = 48 bitset<128> core set of
+    300 determinants (about 8e7 contributions)."""
+    from cases import core_set
+    n, k = 48, 12
+    T, V = mb.synthetic_integrals(n, 0)
+    cd, C = core_set(n, k, 300, 128, nalpha=80, top=40)
+    H = mb.HamiltonianGenerator(T, V, 128)
+    E0 = float(H.matrix_element(cd[:1], cd[:1])[0]) - 0.5
+    s1, r1 = mb.asci_pairs(_settings(), cd, E0, C, H)
+    sel1 = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
+    assert mb.last_search_stats(H)["raw_pairs"] > 5e7
+    monkeypatch.setenv("MACIS_B200_SORT_CLASSIC", "1")
+    s0, r0 = mb.asci_pairs(_settings(), cd, E0, C, H)
+    sel0 = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
+    assert np.array_equal(s1, s0) and np.array_equal(r1, r0)
+    assert np.array_equal(sel1, sel0)
