@@ -254,7 +254,7 @@ def test_onesweep_sort_matches_classic_passes(monkeypatch):
     T, V = mb.synthetic_integrals(n, 0)
     cd, C = core_set(n, k, 300, 128, nalpha=80, top=40)
     H = mb.HamiltonianGenerator(T, V, 128)
-    E0 = float(H.matrix_element(cd[:1], cd[:1])[0]) - 0.5
+    E0 = float(H.matrix_element(cd[:1], cd[:1])) - 0.5
     s1, r1 = mb.asci_pairs(_settings(), cd, E0, C, H)
     sel1 = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
     assert mb.last_search_stats(H)["raw_pairs"] > 5e7

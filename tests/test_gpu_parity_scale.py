@@ -50,7 +50,7 @@ def shape(request, port, ref):
     hr = ref.ham(128, n, T, V)
     hp = port.ham(128, n, T, V)
     H = mb.HamiltonianGenerator(T, V, 128)
-    E0 = float(H.matrix_element(cd[:1], cd[:1])[0]) - 0.5
+    E0 = float(H.matrix_element(cd[:1], cd[:1])) - 0.5
     return dict(n=n, T=T, V=V, cd=cd, C=C, hr=hr, hp=hp, H=H, E0=E0)
 
 
@@ -178,7 +178,7 @@ def n100(port):
     cd, C = core_set(n, k, 3, 256)
     H = mb.HamiltonianGenerator(T, V, 256)
     hp = port.ham(256, n, T, V)
-    E0 = float(H.matrix_element(cd[:1], cd[:1])[0]) - 0.5
+    E0 = float(H.matrix_element(cd[:1], cd[:1])) - 0.5
     return dict(n=n, T=T, V=V, cd=cd, C=C, H=H, hp=hp, E0=E0)
 
 
