@@ -190,6 +190,19 @@ __device__ __forceinline__ uint32_t alpha_bin(const Spin<NSW>& a) {
   return uint32_t(h >> 52);  // 12 bits: ASCI_BINS
 }
 
+// Sort group of a candidate record of a range: groups are runs of the
+// range's alpha-string bins (gtab: bin -> group), so that equal
+// determinants share a group.
+template <int NBITS>
+struct BinGroup {
+  const uint8_t* gtab;  // ASCI_BINS entries
+  __device__ __forceinline__ unsigned operator()(
+      const Key<DetTraits<NBITS>::NW>& k) const {
+    using D = DetTraits<NBITS>;
+    return gtab[alpha_bin<D::NSW>(D::alpha(k.w))];
+  }
+};
+
 #define G2R(p, q) __ldg(I.G2_red + (p) + size_t(q) * n)
 #define V2R(p, q) __ldg(I.V2_red + (p) + size_t(q) * n)
 
@@ -1009,6 +1022,10 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     cap = std::min<int64_t>(std::max<int64_t>(cap, int64_t(1) << 20),
                             int64_t(1) << 31);
   }
+  // records per sort group of a range (MACIS_B200_ASCI_SORT_GROUP)
+  uint64_t sort_group_cap = uint64_t(4) << 28;
+  if(const char* e = getenv("MACIS_B200_ASCI_SORT_GROUP"))
+    sort_group_cap = std::max<uint64_t>(1, uint64_t(atoll(e)));
   // ranges: consecutive alpha-string bins packed up to the cap from the
   // measured bin loads (a single bin above the cap is a range of its own)
   // (a bin above the cap is split into beta-hash classes)
@@ -1175,9 +1192,44 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     if(P) {
       k2 = B.get<uint64_t>(size_t(P) * NW + NW);
       r2 = B.get<double>(size_t(P) + 1);
-      stats.sort_pass_items +=
-          uint64_t(radix_sort<NW, double>(keys, rv, k2, r2, size_t(P), B)) *
-          uint64_t(P);
+      // a large range is first split by bin into groups that are sorted
+      // one at a time: the digit passes of a sort over fewer records run
+      // faster (measured: 12 passes over 6e8 records at 1.7x the rate of
+      // 1.3e9), and equal determinants share a bin, so each group's sums
+      // are complete and in generation order
+      std::vector<size_t> goff{0, size_t(P)};
+      if(!pairs_only && rns[rr] == 0 && rhi[rr] - rlo[rr] > 1 &&
+         P > sort_group_cap) {
+        load_hist();
+        std::vector<uint8_t> gt(ASCI_BINS, 0);
+        int g = 0;
+        unsigned long long acc = 0;
+        for(uint32_t b = rlo[rr]; b < rhi[rr]; ++b) {
+          if(acc && acc + hh[b] > sort_group_cap && g < 255) {
+            ++g;
+            acc = 0;
+          }
+          gt[b] = uint8_t(g);
+          acc += hh[b];
+        }
+        if(g > 0) {
+          uint8_t* dg = B.get<uint8_t>(ASCI_BINS);
+          MB_CUDA(cudaMemcpyAsync(dg, gt.data(), ASCI_BINS,
+                                  cudaMemcpyHostToDevice, s));
+          goff = stable_partition<NW, double>(keys, rv, k2, r2, size_t(P),
+                                              g + 1, BinGroup<NBITS>{dg}, B);
+          std::swap(keys, k2);
+          std::swap(rv, r2);
+          stats.sort_pass_items += uint64_t(P);
+        }
+      }
+      for(size_t gi = 0; gi + 1 < goff.size(); ++gi) {
+        const size_t a = goff[gi], m = goff[gi + 1] - a;
+        stats.sort_pass_items +=
+            uint64_t(radix_sort<NW, double>(keys + a * NW, rv + a,
+                                            k2 + a * NW, r2 + a, m, B)) *
+            uint64_t(m);
+      }
       uint32_t* f = B.get<uint32_t>(size_t(P) + 1);
       uint32_t* fx = B.get<uint32_t>(size_t(P) + 1);
       seg_flags_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(

@@ -283,10 +283,18 @@ constexpr size_t rs_stage_bytes() {
 // `resolve(d, count)` is called by thread d (one per digit) with the tile's
 // count of digit d, between two block barriers, and returns the output
 // position of the tile's first item with that digit.
-template <int NW, typename P, class Resolve>
+template <int NW>
+struct ShiftDigit {  // the byte of the key at bit `shift`
+  int shift;
+  __device__ __forceinline__ unsigned operator()(const Key<NW>& k) const {
+    return digit_of<NW>(k, shift);
+  }
+};
+
+template <int NW, typename P, class Digit, class Resolve>
 __device__ __forceinline__ void rs_tile_pass(const uint64_t* keys,
                                              const P* vals, size_t n,
-                                             int shift, size_t tile0,
+                                             Digit digit, size_t tile0,
                                              uint64_t* keys_out, P* vals_out,
                                              Resolve resolve) {
   extern __shared__ __align__(16) uint8_t rs_smem[];
@@ -307,7 +315,7 @@ __device__ __forceinline__ void rs_tile_pass(const uint64_t* keys,
 #pragma unroll
   for(int r = 0; r < RS_IPT; ++r) {
     const size_t i = wbase + size_t(r) * 32 + lane;
-    dig[r] = i < n ? digit_of<NW>(load_key<NW>(keys, i), shift) : 256u;
+    dig[r] = i < n ? digit(load_key<NW>(keys, i)) : 256u;
   }
 #pragma unroll
   for(int r = 0; r < RS_IPT; ++r) {
@@ -351,7 +359,7 @@ __device__ __forceinline__ void rs_tile_pass(const uint64_t* keys,
   const int cnt = int(n - tile0 < size_t(RS_TILE) ? n - tile0 : size_t(RS_TILE));
   for(int j = threadIdx.x; j < cnt; j += RS_THREADS) {
     const Key<NW> kk = load_key<NW>(skeys, j);
-    const unsigned d = digit_of<NW>(kk, shift);
+    const unsigned d = digit(kk);
     const size_t dst = boff[d] + uint32_t(j - bstart[d]);
     store_key<NW>(keys_out, dst, kk);
     if(vals) vals_out[dst] = svals[j];
@@ -367,8 +375,8 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
   // issued before the ranking: its latency hides behind the tile loads
   const uint64_t my_off =
       offsets[size_t(threadIdx.x) * nblocks + blockIdx.x];
-  rs_tile_pass<NW, P>(keys, vals, n, shift, size_t(blockIdx.x) * RS_TILE,
-                      keys_out, vals_out,
+  rs_tile_pass<NW, P>(keys, vals, n, ShiftDigit<NW>{shift},
+                      size_t(blockIdx.x) * RS_TILE, keys_out, vals_out,
                       [&](int, uint32_t) { return my_off; });
 }
 
@@ -420,9 +428,9 @@ __device__ __forceinline__ void rs_st_status(uint64_t* p, uint64_t v) {
 // separate histogram or scan of the pass is needed. Every look-back wait is
 // bounded by `spin_limit` polls; a block that gives up sets *err and the
 // host reruns the pass with radix_hist_k / radix_scatter_k.
-template <int NW, typename P>
+template <int NW, typename P, class Digit>
 __global__ void __launch_bounds__(RS_THREADS, 4)
-    rs_onesweep_k(const uint64_t* keys, const P* vals, size_t n, int shift,
+    rs_onesweep_k(const uint64_t* keys, const P* vals, size_t n, Digit digit,
                   const unsigned long long* bucket, uint64_t* status,
                   unsigned* tile_counter, int* err, uint64_t* keys_out,
                   P* vals_out, long long spin_limit) {
@@ -432,7 +440,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
   const uint32_t tile = tile_sh;
   const uint64_t base_d = bucket[threadIdx.x];
   rs_tile_pass<NW, P>(
-      keys, vals, n, shift, size_t(tile) * RS_TILE, keys_out, vals_out,
+      keys, vals, n, digit, size_t(tile) * RS_TILE, keys_out, vals_out,
       [&](int d, uint32_t count) -> uint64_t {
         uint64_t* mine = status + size_t(tile) * 256 + d;
         if(tile == 0) {
@@ -508,7 +516,7 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
                         !(force && force[0] == '1');
   if(onesweep) {
     // all digit histograms in one read, bucket starts per pass on the host
-    MB_CUDA(cudaFuncSetAttribute(rs_onesweep_k<NW, P>,
+    MB_CUDA(cudaFuncSetAttribute(rs_onesweep_k<NW, P, ShiftDigit<NW>>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(stage)));
     int* d_shifts = A.get<int>(size_t(np));
@@ -542,8 +550,8 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
       MB_CUDA(cudaMemsetAsync(status, 0, size_t(nblocks) * 256 * 8, A.s));
       MB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), A.s));
       rs_onesweep_k<NW, P><<<nblocks, RS_THREADS, stage, A.s>>>(
-          kin, vin, n, shifts[p], bucket + size_t(p) * 256, status, counter,
-          err, kout, vout, RS_SPIN_LIMIT), note_launch();
+          kin, vin, n, ShiftDigit<NW>{shifts[p]}, bucket + size_t(p) * 256,
+          status, counter, err, kout, vout, RS_SPIN_LIMIT), note_launch();
       int e = 0;
       MB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost,
                               A.s));
@@ -570,6 +578,75 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
       MB_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(P), cudaMemcpyDeviceToDevice, A.s));
   }
   return passes;
+}
+
+// Counts of each digit value (< nbuckets <= 256) of a functor over the keys.
+template <int NW, class Digit>
+__global__ void __launch_bounds__(RS_THREADS)
+    rs_hist_fn_k(const uint64_t* keys, size_t n, Digit digit,
+                 unsigned long long* hist) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  for(size_t i = size_t(blockIdx.x) * RS_THREADS + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * RS_THREADS)
+    atomicAdd(&h[digit(load_key<NW>(keys, i))], 1u);
+  __syncthreads();
+  if(h[threadIdx.x])
+    atomicAdd(hist + threadIdx.x, (unsigned long long)h[threadIdx.x]);
+}
+
+// Stable partition of (keys, vals) into (keys_out, vals_out) by the bucket
+// digit(key) < nbuckets <= 256 (one histogram read, one one-sweep pass;
+// the classic passes if a look-back gives up). Returns the nbuckets + 1
+// bucket offsets.
+template <int NW, typename P, class Digit>
+std::vector<size_t> stable_partition(const uint64_t* keys, const P* vals,
+                                     uint64_t* keys_out, P* vals_out,
+                                     size_t n, int nbuckets, Digit digit,
+                                     Arena& A) {
+  std::vector<size_t> off(size_t(nbuckets) + 1, 0);
+  if(n == 0) return off;
+  auto* hist = A.get<unsigned long long>(256);
+  MB_CUDA(cudaMemsetAsync(hist, 0, 256 * 8, A.s));
+  rs_hist_fn_k<NW><<<grid_for(n, RS_THREADS, 4 * size_t(num_sms())),
+                     RS_THREADS, 0, A.s>>>(keys, n, digit, hist), note_launch();
+  std::vector<unsigned long long> h(256);
+  MB_CUDA(cudaMemcpyAsync(h.data(), hist, 256 * 8, cudaMemcpyDeviceToHost,
+                          A.s));
+  MB_CUDA(cudaStreamSynchronize(A.s));
+  unsigned long long acc = 0;
+  for(int d = 0; d < 256; ++d) {
+    const unsigned long long c = h[d];
+    h[d] = acc;
+    acc += c;
+    if(d < nbuckets) off[size_t(d) + 1] = size_t(acc);
+  }
+  MB_REQUIRE(acc == n, MACIS_B200_EINVAL, "partition digit out of range");
+  auto* bucket = A.get<unsigned long long>(256);
+  MB_CUDA(cudaMemcpyAsync(bucket, h.data(), 256 * 8, cudaMemcpyHostToDevice,
+                          A.s));
+  const unsigned nblocks = unsigned((n + RS_TILE - 1) / RS_TILE);
+  constexpr size_t stage = rs_stage_bytes<NW, P>();
+  MB_CUDA(cudaFuncSetAttribute(rs_onesweep_k<NW, P, Digit>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(stage)));
+  uint64_t* status = A.get<uint64_t>(size_t(nblocks) * 256);
+  unsigned* counter = A.get<unsigned>(1);
+  int* err = A.get<int>(1);
+  MB_CUDA(cudaMemsetAsync(status, 0, size_t(nblocks) * 256 * 8, A.s));
+  MB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), A.s));
+  MB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), A.s));
+  rs_onesweep_k<NW, P, Digit><<<nblocks, RS_THREADS, stage, A.s>>>(
+      keys, vals, n, digit, bucket, status, counter, err, keys_out, vals_out,
+      RS_SPIN_LIMIT), note_launch();
+  int e = 0;
+  MB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, A.s));
+  MB_CUDA(cudaStreamSynchronize(A.s));
+  MB_REQUIRE(e == 0, MACIS_B200_ETIMEOUT,
+             "partition pass: a look-back wait gave up");
+  A.release(status);
+  return off;
 }
 
 // Device bytes that allocations can still obtain: free memory plus what the

@@ -246,7 +246,8 @@ def test_screened_split_search_matches_whole(wcase):
 def test_onesweep_sort_matches_classic_passes(monkeypatch):
     """The candidate sort with one-sweep digit passes (decoupled look-back)
     against the classic histogram / scan / scatter passes
-    (MACIS_B200_SORT_CLASSIC=1): identical accumulated candidates and
+    (MACIS_B200_SORT_CLASSIC=1), and with candidate ranges split by bin
+    into separately sorted groups: identical accumulated candidates and
     scores, and identical selections, on an n = 48 bitset<128> core set of
     300 determinants (about 8e7 contributions)."""
     from cases import core_set
@@ -258,6 +259,15 @@ def test_onesweep_sort_matches_classic_passes(monkeypatch):
     s1, r1 = mb.asci_pairs(_settings(), cd, E0, C, H)
     sel1 = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
     assert mb.last_search_stats(H)["raw_pairs"] > 5e7
+    # a range split by alpha-string bin into sort groups (forced small
+    # here; large searches do it above 1e9 records per range)
+    monkeypatch.setenv("MACIS_B200_ASCI_SORT_GROUP", "3000000")
+    monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", "40000000")
+    selg = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
+    assert mb.last_search_stats(H)["batches"] >= 2
+    assert np.array_equal(selg, sel1)
+    monkeypatch.delenv("MACIS_B200_ASCI_SORT_GROUP")
+    monkeypatch.delenv("MACIS_B200_ASCI_BATCH_PAIRS")
     monkeypatch.setenv("MACIS_B200_SORT_CLASSIC", "1")
     s0, r0 = mb.asci_pairs(_settings(), cd, E0, C, H)
     sel0 = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
