@@ -632,7 +632,8 @@ def asci_rooflines(st, nbits, peak):
 
 
 def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
-                   cpu_ncore=50, cpu_ndets=20000):
+                   cpu_ncore=50, cpu_ndets=20000, problem=None, nbits=128,
+                   net=None, warm=True):
     """One C3-shaped ASCI iteration (asci_iter, iteration.hpp:17-68) both
     ways on n = 48, 12 alpha / 12 beta, bitset<128>: `ncore` core
     determinants -> `ndets` determinants -> rediagonalisation.
@@ -647,19 +648,28 @@ def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
     learned run's wavefunction is also evaluated with the FP64 H.
     cpu_baseline: the compiled reference asci_search (serial,
     determinant_search.hpp:395-663) and the GPU search on a matched small
-    core set."""
+    core set.
+
+    problem = (n, H, core, C, E0) runs the iteration on a given core set
+    (of nbits-bit determinants) instead; net = a network already trained
+    online (then the learned time holds no training); warm = False skips
+    the warm-up search (the caller's run has grown the memory pool)."""
     from macis_b200.solvers import FP64, MIXED
-    n, H, core, C, E0 = _n48_core(mb, ncore, seed)
+    if problem is None:
+        n, H, core, C, E0 = _n48_core(mb, ncore, seed)
+    else:
+        n, H, core, C, E0 = problem
     s = mb.ASCISettings()
     dav = dict(restart_keep=8, max_iter=4000)
-    # warm-up: a search of the same size grows the memory pool, as the
-    # previous iteration of a refine loop would; a small solve loads the
-    # solver kernels
-    warm = mb.asci_search(s, ndets, core, E0, C, n, H)
-    mb.selected_ci_diag(warm[:20000], H, THRESH, 40, 1e-8, **dav)
-    mb.selected_ci_diag(warm[:20000], H, THRESH, 40, 1e-8, precision=MIXED,
-                        **dav)
-    del warm
+    if warm:
+        # warm-up: a search of the same size grows the memory pool, as the
+        # previous iteration of a refine loop would; a small solve loads
+        # the solver kernels
+        w = mb.asci_search(s, ndets, core, E0, C, n, H)
+        mb.selected_ci_diag(w[:20000], H, THRESH, 40, 1e-8, **dav)
+        mb.selected_ci_diag(w[:20000], H, THRESH, 40, 1e-8, precision=MIXED,
+                            **dav)
+        del w
     # exact search + FP64
     t0 = time.perf_counter()
     dets_e = mb.asci_search(s, ndets, core, E0, C, n, H)
@@ -670,19 +680,23 @@ def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
                                    precision=FP64, timings=te, **dav)
     t_exact = time.perf_counter() - t0
     del X_e
-    # learned: the previous iteration's recording search (untimed)
-    nprev = max(1, ncore // 4)
-    net = mb.ScreeningNetwork(nbits=128, seed=seed)
-    rec = mb.ScreenSettings(network=net, max_samples=1000000)
-    mb.asci_search(s, ndets // 4, core[:nprev], E0, C[:nprev], n, H,
-                   screen=rec)
+    rec = mb.ScreenSettings()
+    if net is None:
+        # learned: the previous iteration's recording search (untimed)
+        nprev = max(1, len(core) // 4)
+        net = mb.ScreeningNetwork(nbits=nbits, seed=seed)
+        rec = mb.ScreenSettings(network=net, max_samples=1000000)
+        mb.asci_search(s, ndets // 4, core[:nprev], E0, C[:nprev], n, H,
+                       screen=rec)
     sc = mb.ScreenSettings(network=net, keep_frac=0.2, explore_frac=0.02,
                            train=False, seed=seed)
     mb.asci_search(s, 1000, core[:200], E0, C[:200], n, H, screen=sc,
                    use_net=True)                  # loads the network kernels
     t0 = time.perf_counter()
-    net.clamp_samples(rec.clamp_quantile)
-    loss = net.train(None, None, rec.epochs, rec.batch, rec.lr, seed)
+    loss = None
+    if rec.network is not None:
+        net.clamp_samples(rec.clamp_quantile)
+        loss = net.train(None, None, rec.epochs, rec.batch, rec.lr, seed)
     t_train = time.perf_counter() - t0
     t1 = time.perf_counter()
     dets_l = mb.asci_search(s, ndets, core, E0, C, n, H, screen=sc,
@@ -700,7 +714,7 @@ def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
     recall = sum(1 for d in dets_l[:len(dets_l) - len(core)]
                  if bytes(d) in ea) / max(len(ea), 1)
     out = {
-        "workload": f"ASCI iteration: n = 48, 12a/12b, bitset<128>, "
+        "workload": f"ASCI iteration: n = {n}, bitset<{nbits}>, "
                     f"{len(core)} core dets -> {len(dets_e)} dets, synthetic "
                     f"integrals seed {seed}; Davidson to 1e-8 (max_m 40, "
                     f"thick restart 8)",
@@ -727,11 +741,12 @@ def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
         "dE_Eh": E_l - E_e,
         "dE_target_Eh": 1e-4,
         "within_target": abs(E_l - E_e) <= 1e-4,
-        "roofline": asci_rooflines(st_e, 128, peak),
+        "roofline": asci_rooflines(st_e, nbits, peak),
     }
     del dets_e, dets_l, X_l
-    out["cpu_baseline"] = asci_cpu_baseline(mb, n, H, core[:cpu_ncore],
-                                            C[:cpu_ncore], E0, cpu_ndets, seed)
+    if nbits == 128 and problem is None:
+        out["cpu_baseline"] = asci_cpu_baseline(
+            mb, n, H, core[:cpu_ncore], C[:cpu_ncore], E0, cpu_ndets, seed)
     return out
 
 

@@ -157,7 +157,8 @@ def asci_iter_n48(ncore=100000, ndets=1000000):
                                           ndets=ndets), default=float))
 
 
-def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128):
+def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128,
+       compare=False):
     """One C3-shaped ASCI run (C4 with n = 64, k = 16); prints one JSON line
     with the per-iteration log, the final energy and the wall time."""
     import json
@@ -185,7 +186,19 @@ def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128):
         E, dets, X = mb.asci_iter(s, m, len(dets), E, dets, X, H, n, scr)
     dt = time.perf_counter() - t0
     recall = None
-    if scr is not None:
+    cmp = None
+    if scr is not None and compare:
+        # one more iteration from the final wavefunction both ways: exact
+        # search + FP64 solve against the trained network's screened search
+        # + mixed solve, at equal determinant count
+        core, C = mb.reorder_ci_on_coeff(dets, np.asarray(X))
+        nc = min(int(ncore), len(core))
+        bench = _bench()
+        cmp = bench.asci_iteration(mb, bench.peaks()[0],
+                                   problem=(n, H, core[:nc], C[:nc], E),
+                                   ndets=len(dets), nbits=nbits,
+                                   net=scr.network, warm=False)
+    elif scr is not None:
         # top-k recall of the screened search against the exact one, from
         # the same core set (the last iteration's wavefunction)
         core, C = mb.reorder_ci_on_coeff(dets, np.asarray(X))
@@ -219,7 +232,7 @@ def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128):
     out = {"mode": mode, "ntdets": int(ntdets), "ndets": len(dets),
            "n": n, "electrons": [k, k], "E_grow": Eg, "E_final": E,
            "E_final_fp64_H": E_fp64, "topk_recall_last": recall,
-           "seconds": dt, "grow_seconds": t_grow,
+           "seconds": dt, "grow_seconds": t_grow, "compare": cmp,
            "final_product_ms": {"csr": csr_ms, "matrix_free": hop_ms,
                                 "matrix_free_setup": hop_setup_ms,
                                 "max_rel_diff": hop_diff},
@@ -236,6 +249,7 @@ def main():
     ap.add_argument("--mode", default="fp64")
     ap.add_argument("--ncore", type=int, default=10000)
     ap.add_argument("--refine", type=int, default=3)
+    ap.add_argument("--compare", action="store_true")
     a = ap.parse_args()
     if a.case == "hbuild_c1":
         hbuild(10, 5, a.reps)
@@ -266,7 +280,8 @@ def main():
         c3(a.ntdets, a.mode, n=64, k=16)
     elif a.case == "c5":
         # n = 100, 20a/20b, bitset<256> (network input 320 columns)
-        c3(a.ntdets, a.mode, refine=a.refine, n=100, k=20, nbits=256)
+        c3(a.ntdets, a.mode, refine=a.refine, n=100, k=20, nbits=256,
+           compare=a.compare)
     else:
         raise SystemExit(f"unknown case {a.case}")
 
