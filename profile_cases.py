@@ -274,14 +274,18 @@ def main():
     elif a.case == "asci_iter_n48":
         asci_iter_n48(a.ncore if a.ncore != 10000 else 100000,
                       int(a.ntdets))
-    elif a.case == "c3":
-        c3(a.ntdets, a.mode)
-    elif a.case == "c4":
-        c3(a.ntdets, a.mode, n=64, k=16)
-    elif a.case == "c5":
-        # n = 100, 20a/20b, bitset<256> (network input 320 columns)
-        c3(a.ntdets, a.mode, refine=a.refine, n=100, k=20, nbits=256,
-           compare=a.compare)
+    elif a.case in ("c3", "c4", "c5"):
+        # --ncore: core determinants per search (default 1e5 for these)
+        nc = a.ncore if a.ncore != 10000 else 100000
+        if a.case == "c3":
+            c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, compare=a.compare)
+        elif a.case == "c4":
+            c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, n=64, k=16,
+               compare=a.compare)
+        else:
+            # n = 100, 20a/20b, bitset<256> (network input 320 columns)
+            c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, n=100, k=20,
+               nbits=256, compare=a.compare)
     else:
         raise SystemExit(f"unknown case {a.case}")
 
