@@ -398,21 +398,10 @@ __global__ void __launch_bounds__(RS_THREADS)
   for(int i = threadIdx.x; i < np * 256; i += RS_THREADS) (&h[0][0])[i] = 0;
   if(threadIdx.x < np) sh_shift[threadIdx.x] = shifts[threadIdx.x];
   __syncthreads();
-  // whole warps step together so that equal digits of a warp (most of them,
-  // for keys near one determinant) are added once, not 32 times in a row
-  const int lane = threadIdx.x & 31;
-  const size_t stride = size_t(gridDim.x) * RS_THREADS;
-  for(size_t b = size_t(blockIdx.x) * RS_THREADS + (threadIdx.x & ~31u); b < n;
-      b += stride) {
-    const size_t i = b + lane;
-    const bool ok = i < n;
-    Key<NW> k;
-    if(ok) k = load_key<NW>(keys, i);
-    for(int p = 0; p < np; ++p) {
-      const unsigned d = ok ? digit_of<NW>(k, sh_shift[p]) : 256u;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
-      if(ok && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], __popc(peers));
-    }
+  for(size_t i = size_t(blockIdx.x) * RS_THREADS + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * RS_THREADS) {
+    const Key<NW> k = load_key<NW>(keys, i);
+    for(int p = 0; p < np; ++p) atomicAdd(&h[p][digit_of<NW>(k, sh_shift[p])], 1u);
   }
   __syncthreads();
   for(int i = threadIdx.x; i < np * 256; i += RS_THREADS)
