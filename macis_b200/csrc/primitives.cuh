@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
 // number of keys whose digit at shifts[p] is d (shared-memory counts per
 // block, then one global add per (p, d)).
 constexpr int RS_MAX_PASSES = 32;
-// sorts of at least this many keys use the one-sweep passes
+// sorts of at least this many keys may use the one-sweep passes
 constexpr size_t RS_ONESWEEP_MIN = size_t(1) << 16;
 // polls of one look-back wait (each an L2 round trip) before it gives up
 constexpr long long RS_SPIN_LIMIT = 1ll << 22;
@@ -511,9 +511,13 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
     radix_scatter_k<NW, P><<<nblocks, RS_THREADS, stage, A.s>>>(
         kin, vin, n, shift, offs, nblocks, kout, vout), note_launch();
   };
-  const char* force = getenv("MACIS_B200_SORT_CLASSIC");
+  // The one-sweep passes are opt-in (MACIS_B200_SORT_ONESWEEP=1): measured
+  // on the n = 48 ASCI searches with bin-grouped ranges, the classic passes
+  // were faster (1e5 core dets: 6.9 s against 8.1-11.3 s; 1e4: 0.64 s
+  // against 0.67-0.69 s) and steadier
+  const char* opt = getenv("MACIS_B200_SORT_ONESWEEP");
   const bool onesweep = n >= RS_ONESWEEP_MIN && np <= RS_MAX_PASSES &&
-                        !(force && force[0] == '1');
+                        opt && opt[0] == '1';
   if(onesweep) {
     // all digit histograms in one read, bucket starts per pass on the host
     MB_CUDA(cudaFuncSetAttribute(rs_onesweep_k<NW, P, ShiftDigit<NW>>,
