@@ -217,20 +217,6 @@ struct DPData {
   // gathering G
   const double* aval;
   const double* l4val;
-  // the alpha list of every A split for the fill (dp_split_k): the entries
-  // that open a segment (A' = A, alpha singles) and the alpha doubles, each
-  // with its position in the row (the same for every B: all beta lists of
-  // a product space have the same lengths)
-  const int64_t* ndoff;    // UA+1
-  const int32_t* ndcol;
-  const uint32_t* ndinfo;
-  const int32_t* ndpos;
-  const int32_t* nddb;     // doubles of A's list before the entry
-  const int64_t* doff;     // UA+1
-  const int32_t* dcol;
-  const int32_t* dpos;
-  const double* dval;
-  const int32_t* rowlen;   // UA: entries of each row of A
 };
 
 // Occupied and empty orbitals of a spin string, in ascending order, into
@@ -311,66 +297,6 @@ __global__ void dp_dval_k(const uint32_t* info, int64_t m, const double* G,
       v = (e >> 31) ? -g : g;
     }
     val[i] = v;
-  }
-}
-
-// Splits each alpha list (encoded) into its segment entries (class 0 and 1)
-// and its doubles (class 2), with the row position of every entry: the
-// positions are the exclusive prefix sums of n4 (class 0), n2 (class 1) and
-// 1 (class 2) over the list in column order. One warp per alpha string.
-__global__ void dp_split_k(const int64_t* aoff, const int32_t* acol,
-                           const uint32_t* ainfo, const double* aval,
-                           int64_t UA, int32_t n2, int32_t n4,
-                           const int64_t* ndoff, const int64_t* doff,
-                           int32_t* ndcol, uint32_t* ndinfo, int32_t* ndpos,
-                           int32_t* nddb, int32_t* dcol, int32_t* dpos,
-                           double* dval, int32_t* rowlen) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
-  for(int64_t A = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      A < UA; A += nw) {
-    const int64_t c0 = aoff[A], c1 = aoff[A + 1];
-    int32_t pos = 0, nnd = 0, nd = 0;
-    for(int64_t c = c0; c < c1; c += 32) {
-      const int64_t j = c + lane;
-      const bool ok = j < c1;
-      const uint32_t e = ok ? ainfo[j] : 0u;
-      const uint32_t cls = (e >> 29) & 3u;
-      const int32_t cnt = ok ? (cls == 0 ? n4 : cls == 1 ? n2 : 1) : 0;
-      const int32_t incl = warp_incl_scan(cnt);
-      const int32_t p = pos + incl - cnt;
-      const bool isd = ok && cls == 2, isn = ok && cls != 2;
-      const unsigned md = __ballot_sync(0xffffffffu, isd);
-      const unsigned mn = __ballot_sync(0xffffffffu, isn);
-      const int32_t dbefore = nd + __popc(md & lanemask_lt());
-      if(isn) {
-        const int64_t k = ndoff[A] + nnd + __popc(mn & lanemask_lt());
-        ndcol[k] = acol[j];
-        ndinfo[k] = e;
-        ndpos[k] = p;
-        nddb[k] = dbefore;
-      }
-      if(isd) {
-        const int64_t k = doff[A] + dbefore;
-        dcol[k] = acol[j];
-        dpos[k] = p;
-        dval[k] = aval[j];
-      }
-      pos += __shfl_sync(0xffffffffu, incl, 31);
-      nnd += __popc(mn);
-      nd += __popc(md);
-    }
-    if(lane == 0) rowlen[A] = pos;
-  }
-}
-
-// counts of segment entries (class 0 and 1) and doubles per alpha string
-__global__ void dp_splitcount_k(const int32_t* na, int64_t UA, int64_t* ndc,
-                                int64_t* dc) {
-  for(int64_t A = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; A < UA;
-      A += int64_t(gridDim.x) * blockDim.x) {
-    ndc[A] = int64_t(na[3 * A]) + na[3 * A + 1];
-    dc[A] = na[3 * A + 2];
   }
 }
 
@@ -612,7 +538,7 @@ __global__ void __launch_bounds__(DP_THREADS, DP_CTAS)
     const int64_t out0 = rowptr[row];
     CI* __restrict__ rc = colind + out0;
     VT* __restrict__ rv = nzval + out0;
-    int32_t dropped = 0;  // this lane's count
+    int32_t pos = 0, dropped = 0;  // dropped: this lane's count
     uint2 el = make_uint2(0u, 0u);  // this lane's entry of the beta L2 list
     if(lane < n2l)
       el = s2 ? sl2[lane]
@@ -649,49 +575,44 @@ __global__ void __launch_bounds__(DP_THREADS, DP_CTAS)
         if(isd) diag[row] = h;
       }
     };
-    // The segment entries of the alpha list (A' = A and the alpha singles)
-    // go in chunks of 32; the alpha doubles (one entry each) are written
-    // 32 at a time before the segments they precede. Row positions come from
-    // dp_split_k, so the row is still written front to back, chunk by chunk.
-    const int64_t c0n = d.ndoff[A], c1 = d.ndoff[A + 1];
-    const int64_t d0 = d.doff[A];
-    const int32_t dcnt = int32_t(d.doff[A + 1] - d0);
-    int32_t dn = 0;  // doubles of the row written so far
-    // the next chunk of entries is loaded while this one is emitted
-    int32_t nx_col = 0, nx_pos = 0;
+    const int64_t c1 = d.aoff[A + 1];
+    // the next chunk of the alpha list is loaded while this one is emitted
+    int32_t nx_col = 0;
     uint32_t nx_ai = 0;
+    double nx_val = 0.0;
     {
-      const int64_t j = c0n + lane;
+      const int64_t j = d.aoff[A] + lane;
       if(j < c1) {
-        nx_col = __ldg(d.ndcol + j);
-        nx_ai = __ldg(d.ndinfo + j);
-        nx_pos = __ldg(d.ndpos + j);
+        nx_col = __ldg(d.acol + j);
+        nx_ai = __ldg(d.ainfo + j);
+        nx_val = __ldg(d.aval + j);
       }
     }
-    auto put_doubles = [&](int32_t dend) {
-      for(int32_t k = dn + lane; k < dend; k += 32)
-        put(true, __ldg(d.dpos + d0 + k), __ldg(d.dcol + d0 + k) * UB + B,
-            __ldg(d.dval + d0 + k));
-      dn = dend;
-    };
-    for(int64_t c = c0n; c < c1; c += 32) {
+    for(int64_t c = d.aoff[A]; c < c1; c += 32) {
       const int64_t j = c + lane;
-      int32_t colA = 0, spos = 0;
+      int32_t colA = 0;
       uint32_t ai = 0;
-      int cls = 3;
+      double aval = 0.0;
+      int cls = 3, cnt = 0;
       if(j < c1) {
         colA = nx_col * UB;
         ai = nx_ai;
-        spos = nx_pos;
+        aval = nx_val;
         cls = int((ai >> 29) & 3u);
+        cnt = cls == 0 ? n4l : cls == 1 ? n2l : 1;
       }
       if(j + 32 < c1) {
-        nx_col = __ldg(d.ndcol + j + 32);
-        nx_ai = __ldg(d.ndinfo + j + 32);
-        nx_pos = __ldg(d.ndpos + j + 32);
+        nx_col = __ldg(d.acol + j + 32);
+        nx_ai = __ldg(d.ainfo + j + 32);
+        nx_val = __ldg(d.aval + j + 32);
       }
-      // (1) alpha doubles before this chunk's last segment
-      put_doubles(__ldg(d.nddb + (c + 31 < c1 ? c + 31 : c1 - 1)));
+      const int incl = warp_incl_scan(cnt);
+      const int32_t spos = pos + incl - cnt;
+      pos += __shfl_sync(0xffffffffu, incl, 31);
+      // (1) alpha doubles: beta unchanged, one entry each
+      {
+        put(cls == 2, spos, colA + B, aval);
+      }
       // (2) the same-alpha segment: every beta string within two excitations
       unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
       while(m0) {
@@ -813,11 +734,10 @@ __global__ void __launch_bounds__(DP_THREADS, DP_CTAS)
       }
       __syncwarp();
     }
-    put_doubles(dcnt);  // doubles after the last segment
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1)
       dropped += __shfl_xor_sync(0xffffffffu, dropped, o);
-    if(lane == 0) rowcnt[row] = int64_t(__ldg(d.rowlen + A)) - dropped;
+    if(lane == 0) rowcnt[row] = int64_t(pos) - dropped;
   }
 }
 
@@ -1901,51 +1821,10 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       MB_CUDA(cudaMemcpyAsync(h2.data(), l2off, (UB + 1) * 8, cudaMemcpyDeviceToHost, s));
       MB_CUDA(cudaMemcpyAsync(h4.data(), l4off, (UB + 1) * 8, cudaMemcpyDeviceToHost, s));
       MB_CUDA(cudaStreamSynchronize(s));
-      int64_t l2min = l2max = h2[1] - h2[0], l4min = l4max = h4[1] - h4[0];
       for(size_t b = 0; b < UB; ++b) {
         l2max = std::max(l2max, h2[b + 1] - h2[b]);
         l4max = std::max(l4max, h4[b + 1] - h4[b]);
-        l2min = std::min(l2min, h2[b + 1] - h2[b]);
-        l4min = std::min(l4min, h4[b + 1] - h4[b]);
       }
-      // beta strings of one electron count have lists of one length
-      MB_REQUIRE(l2min == l2max && l4min == l4max, MACIS_B200_EINVAL,
-                 "direct-product fill: beta lists of unequal lengths");
-    }
-    // the alpha lists split into segment entries and doubles, with the row
-    // position of every entry
-    {
-      int64_t* ndc = A.get<int64_t>(UA + 1);
-      int64_t* dc = A.get<int64_t>(UA + 1);
-      dp_splitcount_k<<<grid_for(UA, 256, 4 * sms), 256, 0, s>>>(
-          na, int64_t(UA), ndc, dc), note_launch();
-      int64_t* ndoff = A.get<int64_t>(UA + 1);
-      int64_t* doff = A.get<int64_t>(UA + 1);
-      exclusive_scan<int64_t, int64_t>(ndc, ndoff, UA, ndoff + UA, A);
-      exclusive_scan<int64_t, int64_t>(dc, doff, UA, doff + UA, A);
-      const int64_t nnd = to_host(ndoff + UA, s), ndb = to_host(doff + UA, s);
-      int32_t* ndcol = A.get<int32_t>(size_t(std::max<int64_t>(nnd, 1)));
-      uint32_t* ndinfo = A.get<uint32_t>(size_t(std::max<int64_t>(nnd, 1)));
-      int32_t* ndpos = A.get<int32_t>(size_t(std::max<int64_t>(nnd, 1)));
-      int32_t* nddb = A.get<int32_t>(size_t(std::max<int64_t>(nnd, 1)));
-      int32_t* dcol = A.get<int32_t>(size_t(std::max<int64_t>(ndb, 1)));
-      int32_t* dpos = A.get<int32_t>(size_t(std::max<int64_t>(ndb, 1)));
-      double* dval = A.get<double>(size_t(std::max<int64_t>(ndb, 1)));
-      int32_t* rowlen = A.get<int32_t>(UA);
-      dp_split_k<<<grid_for(UA * 32, 256, 8 * sms), 256, 0, s>>>(
-          aoff, acol, ainfo, aval, int64_t(UA), int32_t(l2max),
-          int32_t(l4max), ndoff, doff, ndcol, ndinfo, ndpos, nddb, dcol, dpos,
-          dval, rowlen), note_launch();
-      d.ndoff = ndoff;
-      d.ndcol = ndcol;
-      d.ndinfo = ndinfo;
-      d.ndpos = ndpos;
-      d.nddb = nddb;
-      d.doff = doff;
-      d.dcol = dcol;
-      d.dpos = dpos;
-      d.dval = dval;
-      d.rowlen = rowlen;
     }
     const int nn = h->norb;
     // The integrals of the singles are read through L1 rather than staged in
