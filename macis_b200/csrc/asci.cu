@@ -899,6 +899,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   const int sms = num_sms();
   auto t_all = std::chrono::steady_clock::now();
   macis_b200_asci_stats stats{};
+  NvtxRange nv("macis_b200: ASCI search");
 
   // ------------------------------------------------ core precompute
   CoreData cd{};
@@ -1158,6 +1159,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   double sort_ms = 0, pair_ms = 0, keep_ms = 0;
   for(uint32_t rr = 0; rr < nr; ++rr) {
     auto tb = std::chrono::steady_clock::now();
+    NvtxRange nv_range("macis_b200: ASCI candidate range");
     Arena B(s);
     int64_t* rc = ucnt;
     int64_t* off = uout;

@@ -8,6 +8,7 @@
 // beta in words 2-3. Spin strings are handled as Spin<NSW> (1 or 2 words).
 #pragma once
 #include <atomic>
+#include <nvtx3/nvToolsExt.h>
 #include <climits>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -320,6 +321,15 @@ inline unsigned long long& launch_counter() {
   return n;
 }
 inline void note_launch() { ++launch_counter(); }
+
+// Named range on a profiler's timeline (NVTX v3, header-only: a no-op unless
+// a tool is attached), around the library's phases.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ------------------------------------------------------- fault injection
 // Host-side failures for the tests of the error paths

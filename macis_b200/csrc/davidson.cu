@@ -371,6 +371,7 @@ int davidson_op(const DavOperator& op, int64_t max_m, double tol,
              "Davidson: max_m must be in [1, 1000]");
   MB_REQUIRE(restart_keep >= 0 && restart_keep < max_m, MACIS_B200_EINVAL,
              "Davidson: restart_keep must be in [0, max_m)");
+  NvtxRange nv("macis_b200: Davidson");
   cudaStream_t s = op.s;
   Arena Ar(s);
   const auto t_wall = std::chrono::steady_clock::now();

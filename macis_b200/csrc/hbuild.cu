@@ -1869,6 +1869,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       MB_CUDA(dev_malloc(&h->VT, n4 * 8));
       v_pair_transpose_k<<<grid_for(n4, 256, 8 * sms), 256, 0, s>>>(h->V, h->VT, nn), note_launch();
     }
+    NvtxRange nv_fill("macis_b200: direct-product fill");
     cudaEventRecord(ev[0], s);
     dp_fill_k<NBITS, CI, VT><<<g, DP_THREADS, Ls.bytes, s>>>(
         I, h->VT, d, Ls, hdiag, rowptr64, colind, nzval, out->diag, rowcnt, thresh,
@@ -2001,6 +2002,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
 macis_b200_csr* build_csr_device(macis_b200_ham* h, const uint64_t* bra,
                                  size_t nbra, const uint64_t* ket, size_t nket,
                                  double thresh, int idx_bytes, int val_bytes) {
+  NvtxRange nv("macis_b200: CSR build");
   MB_REQUIRE(idx_bytes == 4 || idx_bytes == 8, MACIS_B200_EINVAL,
              "Unsupported index_t");
   MB_REQUIRE(val_bytes == 4 || val_bytes == 8, MACIS_B200_EINVAL,
