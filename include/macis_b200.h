@@ -78,6 +78,9 @@ typedef struct {
   uint64_t sort_pass_items; /* sum over the sorted candidate ranges of
                                (radix digit passes x records): each pass
                                reads and writes every record once */
+  uint64_t alpha_strings;   /* distinct alpha strings of the core dets when
+                               the candidate ranges used per-alpha-string
+                               lists of the alpha doubles, else 0 */
 } macis_b200_asci_stats;
 
 /* Learned screening (no MACIS counterpart). A "unit" of the ASCI search is

@@ -39,7 +39,8 @@ class AsciStatsC(C.Structure):
                 ("total_ms", C.c_double), ("units_total", C.c_uint64),
                 ("units_kept", C.c_uint64), ("samples", C.c_uint64),
                 ("screen_ms", C.c_double), ("predict_ms", C.c_double),
-                ("sort_pass_items", C.c_uint64)]
+                ("sort_pass_items", C.c_uint64),
+                ("alpha_strings", C.c_uint64)]
 
 
 class AsciScreenC(C.Structure):

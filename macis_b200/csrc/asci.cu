@@ -203,6 +203,30 @@ struct BinGroup {
   }
 };
 
+// Alpha lists of a partitioned search. The bins of the contributions of an
+// alpha same-spin double unit (kind 2) depend only on the core det's alpha
+// string, and so does their threshold test (|G| against the tolerance):
+// for every distinct alpha string u and outer pair k = ii * nvA + aa, the
+// inner indices q of the kept contributions are listed once per search,
+// grouped by the candidate range their bin falls into (ascending q inside a
+// group). A range's count pass then reads each unit's count from the lists
+// instead of evaluating the bins of all its contributions, and its fill
+// pass generates the listed contributions only. The bins of the units with
+// a fixed alpha string (kinds 1, 3, 4) are tabulated per alpha string too.
+// Used for the ranges that are not split by beta string (group g >= 0).
+struct AlphaLists {
+  const int32_t* aidx = nullptr;  // per core det: its alpha string
+  int NK = 0;                     // nA * nvA outer pairs per alpha string
+  int G = 0;                      // groups: the unsplit ranges
+  const uint16_t* abin = nullptr;  // per alpha string: its bin
+  const uint16_t* kbin = nullptr;  // per (u, k): bin after the outer alpha
+                                   // excitation (opposite-spin units)
+  const int64_t* base = nullptr;   // per (u, k): first list entry
+  const uint16_t* rel = nullptr;   // per (u, k): G + 1 group starts
+  const uint16_t* q = nullptr;     // inner indices, by group
+  int g = -1;                      // group of the range, -1: not used
+};
+
 #define G2R(p, q) __ldg(I.G2_red + (p) + size_t(q) * n)
 #define V2R(p, q) __ldg(I.V2_red + (p) + size_t(q) * n)
 
@@ -258,7 +282,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                          int64_t out0, uint64_t* keys, double* rv,
                          float* umax, uint32_t blo, uint32_t bhi,
                          uint32_t nsub, uint32_t sub,
-                         unsigned long long* hist) {
+                         unsigned long long* hist, const AlphaLists& al) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
   const int lane = threadIdx.x & 31;
@@ -291,7 +315,11 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
   bool chkb = false;
   const bool fixed_alpha = kind == 1 || kind == 3 || kind == 4;
   uint32_t ubin = 0;
-  if(fixed_alpha && (part || hist)) {
+  // with alpha lists the caller runs a unit only when it has contributions
+  // in the range: no bin test
+  const bool listed = al.g >= 0 && kind != 0;
+  if(listed) chk = false;
+  if(fixed_alpha && !listed && (part || hist)) {
     Spin<NSW> ua = sA;
     if(kind == 4) ua = sp_flip(sp_flip(sA, int(occA[ii])), int(virA[aa]));
     ubin = alpha_bin<NSW>(ua);
@@ -306,12 +334,22 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
     if(MODE == 0 && lane == 0) *count_out = 0;
     return;
   }
-  for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
-    const int64_t q = q0 + lane;
+  int64_t nloop = ninner;
+  const uint16_t* qlist = nullptr;
+  if(listed && kind == 2) {
+    const size_t row = size_t(al.aidx[c]) * al.NK + size_t(ii) * nvA + aa;
+    const uint16_t* rr = al.rel + row * (al.G + 1);
+    const int e0 = rr[al.g];
+    qlist = al.q + al.base[row] + e0;
+    nloop = int64_t(rr[al.g + 1]) - e0;
+  }
+  for(int64_t q0 = 0; q0 < nloop; q0 += 32) {
+    const int64_t qi = q0 + lane;
     bool keep = false;
     double r = 0;
     uint64_t ex[D::NW];
-    if(q < ninner) {
+    if(qi < nloop) {
+      const int64_t q = qlist ? int64_t(qlist[qi]) : qi;
       if(kind <= 1) {
         // append_singles_asci_contributions (determinant_contributions.hpp:25-66)
         const int S = kind;
@@ -452,7 +490,7 @@ __global__ void __launch_bounds__(256)
             double E0, double tol, int64_t* counts, const int64_t* outoff,
             uint64_t* keys, double* rv, const uint8_t* umask, float* umax,
             uint32_t blo, uint32_t bhi, uint32_t nsub, uint32_t sub,
-            unsigned long long* hist) {
+            unsigned long long* hist, AlphaLists al) {
   // hist (count pass only): per-block bin counts in shared memory
   // (dynamic, ASCI_BINS x 8 B), added to the global histogram at the end
   extern __shared__ unsigned long long shist[];
@@ -467,18 +505,192 @@ __global__ void __launch_bounds__(256)
       if(MODE == 0 && (threadIdx.x & 31) == 0) counts[u - u0] = 0;
       continue;
     }
+    if(MODE == 1 && al.g >= 0 && counts[u - u0] == 0) continue;
     // core det owning unit u (in [c0, c1))
     const size_t lo = size_t(cd.udet[u]);
     const int64_t t = u - cd.uoff[lo];
     unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
                           MODE ? outoff[u - u0] : 0, keys, rv,
                           umax ? umax + u : nullptr, blo, bhi, nsub, sub,
-                          hist ? shist : nullptr);
+                          hist ? shist : nullptr, al);
   }
   if(hist) {
     __syncthreads();
     for(uint32_t i = threadIdx.x; i < ASCI_BINS; i += blockDim.x)
       if(shist[i]) atomicAdd(hist + i, shist[i]);
+  }
+}
+
+// Alpha lists, count pass: one warp per (alpha string u, outer pair k) row.
+// Writes the row's group starts (prefix of the per-group counts, G + 1
+// entries) and the opposite-spin outer bin of the row; grp maps a bin to
+// its group (255: a split range or outside this search's bins). The lists
+// keep the inner indices whose integral passes the threshold test of
+// unit_run (kind 2) and whose bin has a group.
+template <int NBITS>
+__global__ void __launch_bounds__(256)
+    alpha_count_k(Ints I, CoreData cd, const int32_t* rep, size_t nua, int nA,
+                  int nvA, double tol, const uint8_t* grp, AlphaLists al,
+                  uint16_t* rel, uint16_t* kbin, uint16_t* abin,
+                  int64_t* tot) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  extern __shared__ int gcnt[];  // per warp: G counters
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int* cnt = gcnt + wib * (al.G + 1);
+  const int n = cd.n;
+  const size_t rows = nua * size_t(al.NK);
+  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
+  for(size_t row = size_t(blockIdx.x) * (blockDim.x >> 5) + wib; row < rows;
+      row += nwarp) {
+    const size_t u = row / al.NK;
+    const int k = int(row - u * al.NK);
+    const int ii = k / nvA, aa = k - ii * nvA;
+    const size_t c = size_t(rep[u]);
+    const uint8_t* occA = cd.occ + (c * 2) * MAXORB;
+    const uint8_t* virA = cd.vir + (c * 2) * MAXORB;
+    const Spin<NSW> sA = D::alpha(cd.dets + c * D::NW);
+    for(int g = lane; g < al.G; g += 32) cnt[g] = 0;
+    __syncwarp();
+    const int i = occA[ii], a = virA[aa];
+    if(lane == 0) {
+      kbin[row] = uint16_t(alpha_bin<NSW>(sp_flip(sp_flip(sA, i), a)));
+      if(k == 0) abin[u] = uint16_t(alpha_bin<NSW>(sA));
+    }
+    const int span = nvA - 1 - aa;
+    const int64_t ninner = int64_t(nA - 1 - ii) * span;
+    for(int64_t q = lane; q < ninner; q += 32) {
+      const int qd = small_div(q, 1.0f / float(span));
+      const int j = occA[ii + 1 + qd], b = virA[aa + 1 + (int(q) - qd * span)];
+      const double Gv =
+          __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
+      if(!(fabs(Gv) < tol)) {
+        const uint8_t g = grp[alpha_bin<NSW>(
+            sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b))];
+        if(g != 255) atomicAdd(cnt + g, 1);
+      }
+    }
+    __syncwarp();
+    if(lane == 0) {
+      int acc = 0;
+      uint16_t* rr = rel + row * (al.G + 1);
+      for(int g = 0; g < al.G; ++g) {
+        rr[g] = uint16_t(acc);
+        acc += cnt[g];
+      }
+      rr[al.G] = uint16_t(acc);
+      tot[row] = acc;
+    }
+    __syncwarp();
+  }
+}
+
+// Alpha lists, fill pass: the same rows, inner indices written at their
+// group's position in ascending q (lanes with equal groups ranked by
+// __match_any_sync).
+template <int NBITS>
+__global__ void __launch_bounds__(256)
+    alpha_fill_k(Ints I, CoreData cd, const int32_t* rep, size_t nua, int nA,
+                 int nvA, double tol, const uint8_t* grp, AlphaLists al,
+                 uint16_t* qout) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  extern __shared__ int gcnt[];  // per warp: running position per group
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int* run = gcnt + wib * (al.G + 1);
+  const int n = cd.n;
+  const size_t rows = nua * size_t(al.NK);
+  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
+  for(size_t row = size_t(blockIdx.x) * (blockDim.x >> 5) + wib; row < rows;
+      row += nwarp) {
+    const size_t u = row / al.NK;
+    const int k = int(row - u * al.NK);
+    const int ii = k / nvA, aa = k - ii * nvA;
+    const size_t c = size_t(rep[u]);
+    const uint8_t* occA = cd.occ + (c * 2) * MAXORB;
+    const uint8_t* virA = cd.vir + (c * 2) * MAXORB;
+    const Spin<NSW> sA = D::alpha(cd.dets + c * D::NW);
+    const uint16_t* rr = al.rel + row * (al.G + 1);
+    for(int g = lane; g < al.G; g += 32) run[g] = rr[g];
+    __syncwarp();
+    uint16_t* out = qout + al.base[row];
+    const int i = occA[ii], a = virA[aa];
+    const int span = nvA - 1 - aa;
+    const int64_t ninner = int64_t(nA - 1 - ii) * span;
+    for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
+      const int64_t q = q0 + lane;
+      unsigned g = 255;
+      if(q < ninner) {
+        const int qd = small_div(q, 1.0f / float(span));
+        const int j = occA[ii + 1 + qd],
+                  b = virA[aa + 1 + (int(q) - qd * span)];
+        const double Gv =
+            __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
+        if(!(fabs(Gv) < tol))
+          g = grp[alpha_bin<NSW>(
+              sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b))];
+      }
+      const unsigned peers = __match_any_sync(0xffffffffu, g);
+      if(g != 255) {
+        out[run[g] + __popc(peers & lanemask_lt())] = uint16_t(q);
+      }
+      __syncwarp();
+      if(g != 255 && (peers & lanemask_lt()) == 0) run[g] += __popc(peers);
+      __syncwarp();
+    }
+  }
+}
+
+// Count pass of an unsplit range with alpha lists: one thread per unit.
+// Fixed-alpha units (kinds 1, 3, 4) are in the range as a whole, with the
+// count of the whole-search pass (ucnt); alpha doubles (kind 2) read their
+// group's list length. Alpha singles (kind 0, whose threshold test depends
+// on the beta string) are counted by units0_count_k.
+__global__ void range_count_k(CoreData cd, AlphaLists al, int64_t U,
+                              const int64_t* ucnt, const uint8_t* umask,
+                              uint32_t blo, uint32_t bhi, int64_t* rc) {
+  for(int64_t u = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < U;
+      u += int64_t(gridDim.x) * blockDim.x) {
+    const size_t c = size_t(cd.udet[u]);
+    const int64_t t = u - cd.uoff[c];
+    if(t == 0) continue;
+    int64_t r = 0;
+    if(!umask || umask[u]) {
+      const int64_t KA = int64_t(cd.cnt[c * 4]) * cd.cnt[c * 4 + 2];
+      const int64_t KB = int64_t(cd.cnt[c * 4 + 1]) * cd.cnt[c * 4 + 3];
+      const size_t ua = size_t(al.aidx[c]);
+      uint32_t bin = ASCI_BINS;
+      if(t < 2 + KA && t >= 2) {
+        const uint16_t* rr = al.rel + (ua * al.NK + size_t(t - 2)) * (al.G + 1);
+        r = int64_t(rr[al.g + 1]) - rr[al.g];
+      } else if(t == 1 || t < 2 + KA + KB) {
+        bin = al.abin[ua];
+      } else {
+        bin = al.kbin[ua * al.NK + size_t(t - 2 - KA - KB)];
+      }
+      if(bin < ASCI_BINS && bin >= blo && bin < bhi) r = ucnt[u];
+    }
+    rc[u] = r;
+  }
+}
+
+// Alpha-single units (t = 0) of a range with alpha lists: one warp per core
+// det, the per-contribution path of unit_run.
+template <int NBITS>
+__global__ void __launch_bounds__(256)
+    units0_count_k(Ints I, CoreData cd, double E0, double tol,
+                   const uint8_t* umask, uint32_t blo, uint32_t bhi,
+                   int64_t* rc) {
+  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
+  for(size_t c = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      c < cd.ncdets; c += nwarp) {
+    const int64_t u = cd.uoff[c];
+    if(umask && !umask[u]) {
+      if((threadIdx.x & 31) == 0) rc[u] = 0;
+      continue;
+    }
+    unit_run<NBITS, 0>(I, cd, c, 0, E0, tol, rc + u, 0, nullptr, nullptr,
+                       nullptr, blo, bhi, 0u, 0u, nullptr, AlphaLists{});
   }
 }
 
@@ -873,6 +1085,52 @@ static int64_t core_setup(macis_b200_ham* h, Arena& A, const uint64_t* cdets,
   return U;
 }
 
+// Distinct alpha strings of the core dets (host): per det the index of its
+// alpha string, per alpha string a representative det. Off (nua = 0) when
+// the alpha electron counts differ.
+struct AlphaPlan {
+  std::vector<int32_t> aidx, rep;
+  size_t nua = 0;
+  int nA = 0, nvA = 0;
+};
+template <int NBITS>
+static AlphaPlan plan_alpha(const uint64_t* cdets, size_t ncdets, int n,
+                            cudaStream_t s) {
+  constexpr int NW = DetTraits<NBITS>::NW;
+  AlphaPlan ap;
+  if(!ncdets) return ap;
+  std::vector<uint64_t> hd(ncdets * NW);
+  MB_CUDA(cudaMemcpyAsync(hd.data(), cdets, hd.size() * 8,
+                          cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  auto key = [&](size_t c) {
+    if constexpr(NBITS == 64)
+      return std::pair<uint64_t, uint64_t>(hd[c] & 0xffffffffull, 0);
+    else if constexpr(NBITS == 128)
+      return std::pair<uint64_t, uint64_t>(hd[c * 2], 0);
+    else
+      return std::pair<uint64_t, uint64_t>(hd[c * 4 + 1], hd[c * 4]);
+  };
+  std::vector<uint32_t> ord(ncdets);
+  for(size_t c = 0; c < ncdets; ++c) ord[c] = uint32_t(c);
+  std::sort(ord.begin(), ord.end(),
+            [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+  ap.aidx.resize(ncdets);
+  for(size_t p = 0; p < ncdets; ++p) {
+    if(p == 0 || key(ord[p]) != key(ord[p - 1])) {
+      ap.rep.push_back(int32_t(ord[p]));
+      const auto k = key(ord[p]);
+      const int na = __builtin_popcountll(k.first) + __builtin_popcountll(k.second);
+      if(p == 0) ap.nA = na;
+      if(na != ap.nA) return AlphaPlan{};
+    }
+    ap.aidx[ord[p]] = int32_t(ap.rep.size() - 1);
+  }
+  ap.nua = ap.rep.size();
+  ap.nvA = n - ap.nA;
+  return ap;
+}
+
 static void check_net(const macis_b200_mlp* net, cudaStream_t s) {
   int e = 0;
   MB_CUDA(cudaMemcpyAsync(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -991,7 +1249,8 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, hbytes,
                         s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt,
                              nullptr, nullptr, nullptr, umask, nullptr, 0u,
-                             ASCI_BINS, 0u, 0u, dhist), note_launch();
+                             ASCI_BINS, 0u, 0u, dhist, AlphaLists{}),
+        note_launch();
   }
   int64_t* uout = A.get<int64_t>(U + 1);
   exclusive_scan<int64_t, int64_t>(ucnt, uout, size_t(U), uout + U, A);
@@ -1015,7 +1274,8 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   // MACIS_B200_ASCI_BATCH_PAIRS caps the raw pairs per range (exercises the
   // partitioned path on small problems).
   int64_t cap = 0;
-  if(const char* e = getenv("MACIS_B200_ASCI_BATCH_PAIRS")) {
+  const char* cap_env = getenv("MACIS_B200_ASCI_BATCH_PAIRS");
+  if(const char* e = cap_env) {
     cap = std::max<int64_t>(1, atoll(e));
   } else {
     cap = int64_t((0.8 * double(device_bytes_available()) - keep_reserve) /
@@ -1070,6 +1330,31 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     Ppart = 0;
     for(uint32_t b = bin_lo; b < bin_hi; ++b) Ppart += hh[b];
   }
+  // alpha lists (AlphaLists) when the ranges need count passes of their own:
+  // memory for them, at most 15 % of what is free, comes off the range size
+  AlphaPlan ap;
+  int g_est = 0;
+  const char* al_env = getenv("MACIS_B200_ASCI_ALPHA_LISTS");
+  const bool al_allowed = !(al_env && al_env[0] == '0');
+  if(al_allowed && !pairs_only && !st.just_singles && bin_lo < bin_hi &&
+     ((part && part->count > 1) || Ppart > uint64_t(cap))) {
+    ap = plan_alpha<NBITS>(cdets, ncdets, h->norb, s);
+    if(ap.nua) {
+      g_est = int(std::min<uint64_t>(254, 2 * ((Ppart + cap - 1) / cap) + 2));
+      const double nk = double(ap.nA) * ap.nvA;
+      const double pairs2 = double(ap.nA) * (ap.nA - 1) / 2 * double(ap.nvA) *
+                            (ap.nvA - 1) / 2;
+      const double bytes =
+          double(ap.nua) * (nk * (18.0 + 2.0 * (g_est + 1)) + 2.0 * pairs2 + 2.0) +
+          4.0 * double(ncdets + ap.nua) + 8192.0;
+      if(bytes <= 0.15 * double(device_bytes_available())) {
+        if(!cap_env)
+          cap = std::max<int64_t>(cap - int64_t(bytes / per_pair), int64_t(1) << 20);
+      } else {
+        ap = AlphaPlan{};
+      }
+    }
+  }
   if(bin_lo == bin_hi) {
     // this part owns no bins: nothing to search
   } else if((Ppart <= uint64_t(cap) || pairs_only) && bin_lo == 0 &&
@@ -1101,6 +1386,62 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   }
   const uint32_t nr = uint32_t(rlo.size());
   stats.batches = nr;
+  // groups of the alpha lists: the unsplit ranges
+  std::vector<int> rgrp(nr, -1);
+  AlphaLists al;
+  if(ap.nua) {
+    int G = 0;
+    for(uint32_t r = 0; r < nr; ++r)
+      if(rns[r] == 0) rgrp[r] = G++;
+    if(G > g_est || G == 0 || (G < 2 && 2 * ap.nua > ncdets)) {
+      std::fill(rgrp.begin(), rgrp.end(), -1);
+    } else {
+      std::vector<uint8_t> gt(ASCI_BINS, 255);
+      for(uint32_t r = 0; r < nr; ++r)
+        if(rgrp[r] >= 0)
+          for(uint32_t b = rlo[r]; b < rhi[r]; ++b) gt[b] = uint8_t(rgrp[r]);
+      uint8_t* grp = A.get<uint8_t>(ASCI_BINS);
+      MB_CUDA(cudaMemcpyAsync(grp, gt.data(), ASCI_BINS, cudaMemcpyHostToDevice, s));
+      int32_t* aidx = A.get<int32_t>(ncdets);
+      int32_t* rep = A.get<int32_t>(ap.nua);
+      MB_CUDA(cudaMemcpyAsync(aidx, ap.aidx.data(), ncdets * 4,
+                              cudaMemcpyHostToDevice, s));
+      MB_CUDA(cudaMemcpyAsync(rep, ap.rep.data(), ap.nua * 4,
+                              cudaMemcpyHostToDevice, s));
+      al.aidx = aidx;
+      al.NK = ap.nA * ap.nvA;
+      al.G = G;
+      const size_t rows = ap.nua * size_t(al.NK);
+      uint16_t* abin = A.get<uint16_t>(ap.nua);
+      uint16_t* kbin = A.get<uint16_t>(rows + 1);
+      uint16_t* rel = A.get<uint16_t>(rows * (G + 1) + 1);
+      int64_t* base = A.get<int64_t>(rows + 1);
+      al.abin = abin;
+      al.kbin = kbin;
+      al.rel = rel;
+      al.base = base;
+      const size_t smem = 8 * size_t(G + 1) * sizeof(int);
+      if(rows) {
+        int64_t* tot = A.get<int64_t>(rows + 1);
+        alpha_count_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
+                               s>>>(I, cd, rep, ap.nua, ap.nA, ap.nvA,
+                                    st.h_el_tol, grp, al, rel, kbin, abin, tot),
+            note_launch();
+        MB_CUDA(cudaGetLastError());
+        exclusive_scan<int64_t, int64_t>(tot, base, rows, base + rows, A);
+        A.release(tot);
+      }
+      const int64_t E = rows ? to_host(base + rows, s) : 0;
+      uint16_t* ql = A.get<uint16_t>(size_t(E) + 1);
+      al.q = ql;
+      if(E)
+        alpha_fill_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
+                              s>>>(I, cd, rep, ap.nua, ap.nA, ap.nvA,
+                                   st.h_el_tol, grp, al, ql), note_launch();
+      MB_CUDA(cudaGetLastError());
+      stats.alpha_strings = ap.nua;
+    }
+  }
   stats.pairs_ms = ms_since(t_all);
 
   // sorted core dets (dropped from the candidates)
@@ -1169,10 +1510,21 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     if(nr > 1 || rlo[rr] != 0 || rhi[rr] != ASCI_BINS) {
       rc = B.get<int64_t>(U + 1);
       off = B.get<int64_t>(U + 1);
-      units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
-          I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, nullptr, nullptr,
-          nullptr, umask, nullptr, rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr),
-          note_launch();
+      if(rgrp[rr] >= 0) {
+        AlphaLists alr = al;
+        alr.g = rgrp[rr];
+        range_count_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
+            cd, alr, U, ucnt, umask, rlo[rr], rhi[rr], rc), note_launch();
+        units0_count_k<NBITS><<<grid_for(ncdets * 32, 256, 16 * sms), 256, 0,
+                                s>>>(I, cd, E0, st.h_el_tol, umask, rlo[rr],
+                                     rhi[rr], rc), note_launch();
+      } else {
+        units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0,
+                            s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,
+                                 nullptr, nullptr, nullptr, umask, nullptr,
+                                 rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr,
+                                 AlphaLists{}), note_launch();
+      }
       exclusive_scan<int64_t, int64_t>(rc, off, size_t(U), off + U, B);
       P = to_host(off + U, s);
     }
@@ -1181,7 +1533,12 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     if(P) {
       units_k<NBITS, 1><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
           I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, off, keys, rv, umask,
-          umax, rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr), note_launch();
+          umax, rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr,
+          rgrp[rr] >= 0 && rc != ucnt ? [&] {
+            AlphaLists alr = al;
+            alr.g = rgrp[rr];
+            return alr;
+          }() : AlphaLists{}), note_launch();
       MB_CUDA(cudaGetLastError());
     }
     MB_CUDA(cudaStreamSynchronize(s));

@@ -274,3 +274,52 @@ def test_onesweep_sort_matches_classic_passes(monkeypatch):
     sel0 = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
     assert np.array_equal(s1, s0) and np.array_equal(r1, r0)
     assert np.array_equal(sel1, sel0)
+
+
+@pytest.mark.parametrize("nbits,n,k,ncore,nalpha,top",
+                         [(128, 48, 12, 300, 80, 40), (256, 100, 20, 8, 6, 4)])
+def test_alpha_lists_match_per_contribution_bins(monkeypatch, nbits, n, k,
+                                                 ncore, nalpha, top):
+    """Candidate ranges that take their alpha-double counts and contributions
+    from per-alpha-string lists (the default once a search needs several
+    ranges) against ranges that test every contribution's bin
+    (MACIS_B200_ASCI_ALPHA_LISTS=0) and against the single-range search:
+    identical selections and recorded unit targets, with a range cap that
+    leaves every range whole and one small enough to split the heaviest
+    alpha-string bin by beta string; exact and screened."""
+    from cases import core_set
+    T, V = mb.synthetic_integrals(n, 0)
+    cd, C = core_set(n, k, ncore, nbits, nalpha=nalpha, top=top)
+    H = mb.HamiltonianGenerator(T, V, nbits)
+    E0 = float(H.matrix_element(cd[:1], cd[:1])) - 0.5
+    net = mb.ScreeningNetwork(nbits=nbits, seed=0)
+    keep = mb.ScreenSettings(network=net, keep_frac=0.4, explore_frac=0.0,
+                             train=False)
+    rec = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=nbits, seed=1),
+                            max_samples=200000)
+
+    def run():
+        exact = mb.asci_search(_settings(), 40000, cd, E0, C, n, H)
+        st = mb.last_search_stats(H)
+        scr = mb.asci_search(_settings(), 40000, cd, E0, C, n, H, screen=keep,
+                             use_net=True)
+        mb.asci_search(_settings(), 40000, cd, E0, C, n, H, screen=rec)
+        return exact, scr, rec.network.samples(), st
+
+    one = run()
+    assert one[3]["batches"] == 1 and one[3]["alpha_strings"] == 0
+    raw = one[3]["raw_pairs"]
+    for cap in (raw // 12, raw // 150):
+        monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", str(cap))
+        lists = run()
+        assert lists[3]["batches"] > 3
+        assert lists[3]["alpha_strings"] > 0
+        monkeypatch.setenv("MACIS_B200_ASCI_ALPHA_LISTS", "0")
+        bins = run()
+        assert bins[3]["alpha_strings"] == 0
+        monkeypatch.delenv("MACIS_B200_ASCI_ALPHA_LISTS")
+        for got in (lists, bins):
+            assert np.array_equal(got[0], one[0])
+            assert np.array_equal(got[1], one[1])
+            assert np.array_equal(got[2][0], one[2][0])
+            assert np.array_equal(got[2][1], one[2][1])
