@@ -607,8 +607,11 @@ def asci_rooflines(st, nbits, peak):
     """HBM rooflines of the exact search's two dominant phases from its
     statistics: contribution generation (units_k count and fill passes:
     every raw record written once) and the candidate sort (lower bound: one
-    read and one write of every record; per pass: the digit passes run)."""
-    rec = 8 * (nbits // 64) + 8
+    read and one write of every record; per pass: the digit passes run).
+    A record is a determinant and its score, or a ranked key (alpha and beta
+    string ranks, 8 B) and its score when the search sorted by ranked keys
+    (key_bits > 0)."""
+    rec = 16 if st.get("key_bits") else 8 * (nbits // 64) + 8
     gen_b = st["raw_pairs"] * rec
     gen = gen_b / (st["pairs_ms"] * 1e-3) / 1e9
     lb_b = 2 * st["raw_pairs"] * rec
@@ -620,7 +623,8 @@ def asci_rooflines(st, nbits, peak):
                     "unit": "GB/s", "frac": gen / peak,
                     "alg_bytes": gen_b, "ms": st["pairs_ms"],
                     "basis": f"raw contributions x {rec} B written, over the "
-                             "count + generation passes"},
+                             "count + generation passes",
+                    "key_bits": st.get("key_bits", 0)},
         "sort": {"bound": "hbm", "achieved": sort_lb, "peak": peak,
                  "unit": "GB/s", "frac": sort_lb / peak, "alg_bytes": lb_b,
                  "ms": st["sort_ms"],

@@ -81,6 +81,10 @@ typedef struct {
   uint64_t alpha_strings;   /* distinct alpha strings of the core dets when
                                the candidate ranges used per-alpha-string
                                lists of the alpha doubles, else 0 */
+  uint64_t key_bits;        /* bits of the ranked candidate keys (alpha and
+                               beta string ranks) the candidates were sorted
+                               by, 0 when sorted by the determinant bitset */
+  double rank_ms;           /* building the string rank tables */
 } macis_b200_asci_stats;
 
 /* Learned screening (no MACIS counterpart). A "unit" of the ASCI search is

@@ -40,7 +40,8 @@ class AsciStatsC(C.Structure):
                 ("units_kept", C.c_uint64), ("samples", C.c_uint64),
                 ("screen_ms", C.c_double), ("predict_ms", C.c_double),
                 ("sort_pass_items", C.c_uint64),
-                ("alpha_strings", C.c_uint64)]
+                ("alpha_strings", C.c_uint64), ("key_bits", C.c_uint64),
+                ("rank_ms", C.c_double)]
 
 
 class AsciScreenC(C.Structure):

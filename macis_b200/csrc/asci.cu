@@ -227,6 +227,135 @@ struct AlphaLists {
   int g = -1;                      // group of the range, -1: not used
 };
 
+// String ranks. The candidate determinants of a search are the core dets'
+// alpha strings, their singles and doubles, combined with beta strings of
+// the same kinds. With every distinct candidate string of a spin replaced
+// by its rank in the sorted list of those strings, a candidate determinant
+// is one 64-bit key, (beta rank << bits_a) | alpha rank, that sorts in the
+// same order as the determinant's bitset: the digit passes of the candidate
+// sort cover bits_a + bits_b bits instead of the 2 x norb varying bits of
+// the determinant, over 16-byte instead of 24- or 40-byte records. Per
+// distinct core string u of a spin the table R holds the ranks of its
+// M = 1 + N1 + N2 candidates: u itself, its N1 singles (index ii * nv + aa,
+// occupied ii -> virtual aa) and its N2 doubles (row ii * nv + aa, then the
+// inner index q of the double loops of unit_run).
+struct SpinRanks {
+  const uint32_t* R = nullptr;
+  const int32_t* idx = nullptr;  // per core det: its string
+  int64_t M = 0, N1 = 0;
+};
+struct RankTables {
+  SpinRanks a, b;
+  int bits_a = 0;
+  const uint64_t* La = nullptr;  // distinct candidate alpha strings (NSW words)
+  const uint64_t* Lb = nullptr;
+  const uint16_t* bin_a = nullptr;  // per alpha rank: its bin
+};
+// First double of row ii * nv + aa among the doubles of a string with ne
+// electrons and nv virtuals (rows before it hold (ne-1-ii')(nv-1-aa') each).
+__device__ __forceinline__ int64_t double_row_base(int ii, int aa, int ne,
+                                                   int nv) {
+  const int64_t A = int64_t(ii) * (ne - 1) - int64_t(ii) * (ii - 1) / 2;
+  const int64_t T = int64_t(nv) * (nv - 1) / 2;
+  const int64_t B = int64_t(aa) * (nv - 1) - int64_t(aa) * (aa - 1) / 2;
+  return A * T + int64_t(ne - 1 - ii) * B;
+}
+
+// The candidate strings of the distinct core strings, one thread per
+// (string, candidate): written with their index, for the rank sort.
+template <int NSW>
+__global__ void cand_strings_k(const uint64_t* words, const uint8_t* occ,
+                               const uint8_t* vir, size_t nu, int ne, int nv,
+                               int64_t M, int64_t N1, const int64_t* dbase,
+                               int nrows, uint64_t* cand, uint32_t* idx) {
+  const size_t tot = nu * size_t(M);
+  for(size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < tot;
+      e += size_t(gridDim.x) * blockDim.x) {
+    const size_t u = e / size_t(M);
+    const int64_t r = int64_t(e - u * size_t(M));
+    Spin<NSW> st;
+#pragma unroll
+    for(int j = 0; j < NSW; ++j) st.w[j] = words[u * NSW + j];
+    const uint8_t* o = occ + u * MAXORB;
+    const uint8_t* v = vir + u * MAXORB;
+    if(r >= 1 && r <= N1) {
+      const int t = int(r - 1), ii = t / nv, aa = t - ii * nv;
+      st = sp_flip(sp_flip(st, int(o[ii])), int(v[aa]));
+    } else if(r > N1) {
+      const int64_t d = r - 1 - N1;
+      int lo = 0, hi = nrows;  // last row whose first double is <= d
+      while(hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if(dbase[mid] <= d) lo = mid; else hi = mid;
+      }
+      const int ii = lo / nv, aa = lo - ii * nv;
+      const int span = nv - 1 - aa;
+      const int q = int(d - dbase[lo]);
+      const int jj = ii + 1 + q / span, bb = aa + 1 + q % span;
+      st = sp_flip(sp_flip(sp_flip(sp_flip(st, int(o[ii])), int(o[jj])),
+                           int(v[aa])), int(v[bb]));
+    }
+#pragma unroll
+    for(int j = 0; j < NSW; ++j) cand[e * NSW + j] = st.w[j];
+    idx[e] = uint32_t(e);
+  }
+}
+// Rank of every candidate (sorted position p holds candidate idx[p]) and
+// the distinct strings in rank order.
+template <int NSW>
+__global__ void rank_scatter_k(const uint64_t* cand, const uint32_t* idx,
+                               const uint32_t* f, const uint32_t* fx, size_t n,
+                               uint32_t* R, uint64_t* L) {
+  for(size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n;
+      p += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t r = fx[p] + f[p] - 1;
+    R[idx[p]] = r;
+    if(f[p]) {
+#pragma unroll
+      for(int j = 0; j < NSW; ++j) L[size_t(r) * NSW + j] = cand[p * NSW + j];
+    }
+  }
+}
+template <int NSW>
+__global__ void string_bins_k(const uint64_t* L, size_t n, uint16_t* bin) {
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    Spin<NSW> st;
+#pragma unroll
+    for(int j = 0; j < NSW; ++j) st.w[j] = L[i * NSW + j];
+    bin[i] = uint16_t(alpha_bin<NSW>(st));
+  }
+}
+// Ranked keys back to determinants.
+template <int NBITS>
+__global__ void unrank_k(const uint64_t* rk, size_t n, RankTables rt,
+                         uint64_t* dets) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  const uint64_t ma = (uint64_t(1) << rt.bits_a) - 1;
+  for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+      i += size_t(gridDim.x) * blockDim.x) {
+    const uint64_t k = rk[i];
+    const size_t ra = size_t(k & ma), rb = size_t(k >> rt.bits_a);
+    Spin<NSW> a, b;
+#pragma unroll
+    for(int j = 0; j < NSW; ++j) {
+      a.w[j] = rt.La[ra * NSW + j];
+      b.w[j] = rt.Lb[rb * NSW + j];
+    }
+    D::make(dets + i * D::NW, a, b);
+  }
+}
+// Sort group of a ranked key: the group of its alpha string's bin.
+struct RankBinGroup {
+  const uint8_t* gtab;
+  const uint16_t* bin_a;
+  uint64_t mask_a;
+  __device__ __forceinline__ unsigned operator()(const Key<1>& k) const {
+    return gtab[bin_a[k.w[0] & mask_a]];
+  }
+};
+
 #define G2R(p, q) __ldg(I.G2_red + (p) + size_t(q) * n)
 #define V2R(p, q) __ldg(I.V2_red + (p) + size_t(q) * n)
 
@@ -267,7 +396,8 @@ __device__ __forceinline__ UnitDesc decode_unit(int nA, int nB, int nvA,
   return d;
 }
 
-// One unit of contributions; MODE 0 counts, MODE 1 writes. Warp-synchronous.
+// One unit of contributions; MODE 0 counts, MODE 1 writes determinants,
+// MODE 2 writes ranked keys (RankTables). Warp-synchronous.
 // q / d for 0 <= q < 2^14 and 1 <= d <= 128 from a float product with rd =
 // 1 / d: (q + 0.5) / d is at least 0.5 / d away from an integer, far above
 // the float rounding error (< 2^-22 q / d), so truncation gives the quotient
@@ -282,7 +412,8 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                          int64_t out0, uint64_t* keys, double* rv,
                          float* umax, uint32_t blo, uint32_t bhi,
                          uint32_t nsub, uint32_t sub,
-                         unsigned long long* hist, const AlphaLists& al) {
+                         unsigned long long* hist, const AlphaLists& al,
+                         const RankTables& rt) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
   const int lane = threadIdx.x & 31;
@@ -334,6 +465,35 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
     if(MODE == 0 && lane == 0) *count_out = 0;
     return;
   }
+  // ranked keys: the rank of the spin string that is fixed for the unit, and
+  // the table of the other spin's ranks indexed by the inner index q
+  uint64_t rfix = 0;
+  const uint32_t* rvar = nullptr;
+  int rshift = 0;
+  if constexpr(MODE == 2) {
+    const uint32_t* Ra = rt.a.R + size_t(rt.a.idx[c]) * size_t(rt.a.M);
+    const uint32_t* Rb = rt.b.R + size_t(rt.b.idx[c]) * size_t(rt.b.M);
+    const int ba = rt.bits_a;
+    if(kind == 0) {
+      rfix = uint64_t(Rb[0]) << ba;
+      rvar = Ra + 1;
+    } else if(kind == 1) {
+      rfix = Ra[0];
+      rvar = Rb + 1;
+      rshift = ba;
+    } else if(kind == 2) {
+      rfix = uint64_t(Rb[0]) << ba;
+      rvar = Ra + 1 + rt.a.N1 + double_row_base(ii, aa, nA, nvA);
+    } else if(kind == 3) {
+      rfix = Ra[0];
+      rvar = Rb + 1 + rt.b.N1 + double_row_base(ii, aa, nB, nvB);
+      rshift = ba;
+    } else {
+      rfix = Ra[1 + ii * nvA + aa];
+      rvar = Rb + 1;
+      rshift = ba;
+    }
+  }
   int64_t nloop = ninner;
   const uint16_t* qlist = nullptr;
   if(listed && kind == 2) {
@@ -348,6 +508,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
     bool keep = false;
     double r = 0;
     uint64_t ex[D::NW];
+    uint64_t rkey = 0;
     if(qi < nloop) {
       const int64_t q = qlist ? int64_t(qlist[qi]) : qi;
       if(kind <= 1) {
@@ -376,16 +537,18 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         }
         keep = inr && !(fabs(h) < tol);
         if(MODE == 0 && hist && S == 0 && keep) atomicAdd(hist + cbin, 1ull);
-        if(MODE == 1 && keep) {
+        if(MODE >= 1 && keep) {
           const double* eps = S ? epsB : epsA;
           h *= ex_sign(S ? sB : sA, a, i);
           const double hd = hii + eps[a] - eps[i] - G2R(a, i) - G2R(i, a);
           h /= (E0 - hd);
           r = coeff * h;
+          if constexpr(MODE == 1) {
 #pragma unroll
-          for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
-          det_flip<NBITS>(ex, S, i);
-          det_flip<NBITS>(ex, S, a);
+            for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
+            det_flip<NBITS>(ex, S, i);
+            det_flip<NBITS>(ex, S, a);
+          }
         }
         (void)nS;
       } else if(kind <= 3) {
@@ -412,7 +575,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                 : 0.0;
         keep = inr && !(fabs(Gv) < tol);
         if(MODE == 0 && hist && S == 0 && keep) atomicAdd(hist + cbin, 1ull);
-        if(MODE == 1 && keep) {
+        if(MODE >= 1 && keep) {
           const Spin<NSW> st = S ? sB : sA;
           Spin<NSW> fx = sp_flip(sp_flip(sp_flip(sp_flip(sp_zero<NSW>(), i), j), a), b);
           const uint32_t e = double_ex(st, st ^ fx);
@@ -424,12 +587,14 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                             G2R(j, a) - G2R(b, j) - G2R(j, b);
           h /= (E0 - hd);
           r = coeff * h;
+          if constexpr(MODE == 1) {
 #pragma unroll
-          for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
-          det_flip<NBITS>(ex, S, i);
-          det_flip<NBITS>(ex, S, j);
-          det_flip<NBITS>(ex, S, a);
-          det_flip<NBITS>(ex, S, b);
+            for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
+            det_flip<NBITS>(ex, S, i);
+            det_flip<NBITS>(ex, S, j);
+            det_flip<NBITS>(ex, S, a);
+            det_flip<NBITS>(ex, S, b);
+          }
         }
       } else {
         // append_os_doubles_asci_contributions (determinant_contributions.hpp:122-160)
@@ -442,7 +607,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
             inr ? __ldg(I.V + a + size_t(i) * n + size_t(b + size_t(j) * n) * n * n)
                 : 0.0;
         keep = inr && !(fabs(Vv) < tol);
-        if(MODE == 1 && keep) {
+        if(MODE >= 1 && keep) {
           const double sign = ex_sign(sA, a, i) * ex_sign(sB, b, j);
           double h = sign * Vv;
           const double hd = hii + epsA[a] + epsB[b] - epsA[i] - epsB[j] +
@@ -450,20 +615,28 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
                             G2R(b, j) - G2R(j, b) - V2R(a, j) - V2R(i, b);
           h /= (E0 - hd);
           r = coeff * h;
+          if constexpr(MODE == 1) {
 #pragma unroll
-          for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
-          det_flip<NBITS>(ex, 0, a);
-          det_flip<NBITS>(ex, 0, i);
-          det_flip<NBITS>(ex, 1, j);
-          det_flip<NBITS>(ex, 1, b);
+            for(int w = 0; w < D::NW; ++w) ex[w] = det[w];
+            det_flip<NBITS>(ex, 0, a);
+            det_flip<NBITS>(ex, 0, i);
+            det_flip<NBITS>(ex, 1, j);
+            det_flip<NBITS>(ex, 1, b);
+          }
         }
       }
+      if constexpr(MODE == 2)
+        if(keep) rkey = rfix | (uint64_t(__ldg(rvar + q)) << rshift);
     }
     const unsigned m = __ballot_sync(0xffffffffu, keep);
-    if(MODE == 1 && keep) {
+    if(MODE >= 1 && keep) {
       const int64_t pos = out0 + done + __popc(m & lanemask_lt());
+      if constexpr(MODE == 1) {
 #pragma unroll
-      for(int w = 0; w < D::NW; ++w) keys[pos * D::NW + w] = ex[w];
+        for(int w = 0; w < D::NW; ++w) keys[pos * D::NW + w] = ex[w];
+      } else {
+        keys[pos] = rkey;
+      }
       rv[pos] = r;
       mx = fmaxf(mx, float(fabs(r)));
     }
@@ -473,7 +646,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
     *count_out = done;
     if(hist && fixed_alpha && done) atomicAdd(hist + ubin, (unsigned long long)done);
   }
-  if(MODE == 1 && umax) {
+  if(MODE >= 1 && umax) {
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1)
       mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -490,7 +663,7 @@ __global__ void __launch_bounds__(256)
             double E0, double tol, int64_t* counts, const int64_t* outoff,
             uint64_t* keys, double* rv, const uint8_t* umask, float* umax,
             uint32_t blo, uint32_t bhi, uint32_t nsub, uint32_t sub,
-            unsigned long long* hist, AlphaLists al) {
+            unsigned long long* hist, AlphaLists al, RankTables rt) {
   // hist (count pass only): per-block bin counts in shared memory
   // (dynamic, ASCI_BINS x 8 B), added to the global histogram at the end
   extern __shared__ unsigned long long shist[];
@@ -505,14 +678,14 @@ __global__ void __launch_bounds__(256)
       if(MODE == 0 && (threadIdx.x & 31) == 0) counts[u - u0] = 0;
       continue;
     }
-    if(MODE == 1 && al.g >= 0 && counts[u - u0] == 0) continue;
+    if(MODE >= 1 && al.g >= 0 && counts[u - u0] == 0) continue;
     // core det owning unit u (in [c0, c1))
     const size_t lo = size_t(cd.udet[u]);
     const int64_t t = u - cd.uoff[lo];
     unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
                           MODE ? outoff[u - u0] : 0, keys, rv,
                           umax ? umax + u : nullptr, blo, bhi, nsub, sub,
-                          hist ? shist : nullptr, al);
+                          hist ? shist : nullptr, al, rt);
   }
   if(hist) {
     __syncthreads();
@@ -690,7 +863,8 @@ __global__ void __launch_bounds__(256)
       continue;
     }
     unit_run<NBITS, 0>(I, cd, c, 0, E0, tol, rc + u, 0, nullptr, nullptr,
-                       nullptr, blo, bhi, 0u, 0u, nullptr, AlphaLists{});
+                       nullptr, blo, bhi, 0u, 0u, nullptr, AlphaLists{},
+                       RankTables{});
   }
 }
 
@@ -1085,50 +1259,196 @@ static int64_t core_setup(macis_b200_ham* h, Arena& A, const uint64_t* cdets,
   return U;
 }
 
-// Distinct alpha strings of the core dets (host): per det the index of its
-// alpha string, per alpha string a representative det. Off (nua = 0) when
-// the alpha electron counts differ.
-struct AlphaPlan {
-  std::vector<int32_t> aidx, rep;
-  size_t nua = 0;
-  int nA = 0, nvA = 0;
+// Distinct spin strings of the core dets (host, from a copy of the dets):
+// per det the index of its string of the spin, per string a representative
+// det, its words and its occupied / virtual orbital lists. Empty (nu = 0)
+// when the electron counts of the spin differ between dets.
+struct SpinPlan {
+  std::vector<int32_t> idx, rep;
+  std::vector<uint64_t> words;  // nu x NSW
+  std::vector<uint8_t> occ, vir;  // nu x MAXORB
+  size_t nu = 0;
+  int ne = 0, nv = 0;
 };
 template <int NBITS>
-static AlphaPlan plan_alpha(const uint64_t* cdets, size_t ncdets, int n,
-                            cudaStream_t s) {
+static SpinPlan plan_spin(const std::vector<uint64_t>& hd, size_t ncdets,
+                          int n, int spin) {
   constexpr int NW = DetTraits<NBITS>::NW;
-  AlphaPlan ap;
-  if(!ncdets) return ap;
-  std::vector<uint64_t> hd(ncdets * NW);
-  MB_CUDA(cudaMemcpyAsync(hd.data(), cdets, hd.size() * 8,
-                          cudaMemcpyDeviceToHost, s));
-  MB_CUDA(cudaStreamSynchronize(s));
+  constexpr int NSW = DetTraits<NBITS>::NSW;
+  SpinPlan sp;
+  if(!ncdets) return sp;
   auto key = [&](size_t c) {
+    const uint64_t* d = hd.data() + c * NW;
     if constexpr(NBITS == 64)
-      return std::pair<uint64_t, uint64_t>(hd[c] & 0xffffffffull, 0);
+      return std::pair<uint64_t, uint64_t>(
+          spin ? d[0] >> 32 : d[0] & 0xffffffffull, 0);
     else if constexpr(NBITS == 128)
-      return std::pair<uint64_t, uint64_t>(hd[c * 2], 0);
+      return std::pair<uint64_t, uint64_t>(d[spin], 0);
     else
-      return std::pair<uint64_t, uint64_t>(hd[c * 4 + 1], hd[c * 4]);
+      return std::pair<uint64_t, uint64_t>(d[2 * spin + 1], d[2 * spin]);
   };
   std::vector<uint32_t> ord(ncdets);
   for(size_t c = 0; c < ncdets; ++c) ord[c] = uint32_t(c);
   std::sort(ord.begin(), ord.end(),
             [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
-  ap.aidx.resize(ncdets);
+  sp.idx.resize(ncdets);
   for(size_t p = 0; p < ncdets; ++p) {
     if(p == 0 || key(ord[p]) != key(ord[p - 1])) {
-      ap.rep.push_back(int32_t(ord[p]));
       const auto k = key(ord[p]);
-      const int na = __builtin_popcountll(k.first) + __builtin_popcountll(k.second);
-      if(p == 0) ap.nA = na;
-      if(na != ap.nA) return AlphaPlan{};
+      const int ne = __builtin_popcountll(k.first) + __builtin_popcountll(k.second);
+      if(p == 0) sp.ne = ne;
+      if(ne != sp.ne) return SpinPlan{};
+      sp.rep.push_back(int32_t(ord[p]));
+      // words in the determinant's order (low word first)
+      if constexpr(NSW == 1) {
+        sp.words.push_back(k.first);
+      } else {
+        sp.words.push_back(k.second);
+        sp.words.push_back(k.first);
+      }
+      std::vector<uint8_t> o(MAXORB, 0), v(MAXORB, 0);
+      int no = 0, nv = 0;
+      for(int i = 0; i < n; ++i) {
+        const uint64_t w = i < 64 ? (NSW == 1 ? k.first : k.second) : k.first;
+        if((w >> (i & 63)) & 1)
+          o[no++] = uint8_t(i);
+        else
+          v[nv++] = uint8_t(i);
+      }
+      sp.occ.insert(sp.occ.end(), o.begin(), o.end());
+      sp.vir.insert(sp.vir.end(), v.begin(), v.end());
     }
-    ap.aidx[ord[p]] = int32_t(ap.rep.size() - 1);
+    sp.idx[ord[p]] = int32_t(sp.rep.size() - 1);
   }
-  ap.nua = ap.rep.size();
-  ap.nvA = n - ap.nA;
-  return ap;
+  sp.nu = sp.rep.size();
+  sp.nv = n - sp.ne;
+  return sp;
+}
+
+// Candidates per distinct core string of a spin with ne electrons and nv
+// virtuals: itself, ne nv singles, C(ne,2) C(nv,2) doubles.
+static int64_t spin_candidates(int ne, int nv) {
+  return 1 + int64_t(ne) * nv +
+         int64_t(ne) * (ne - 1) / 2 * (int64_t(nv) * (nv - 1) / 2);
+}
+
+// Rank table of one spin (SpinRanks) and its distinct candidate strings in
+// rank order (*L, NSW words each); returns their number. The candidates are
+// generated with their index, radix-sorted, and equal neighbours share a
+// rank.
+template <int NBITS>
+static size_t build_spin_ranks(const SpinPlan& sp, Arena& A, cudaStream_t s,
+                               SpinRanks& out, uint64_t** L) {
+  constexpr int NSW = DetTraits<NBITS>::NSW;
+  const int ne = sp.ne, nv = sp.nv, nrows = ne * nv;
+  const int64_t M = spin_candidates(ne, nv);
+  const size_t tot = sp.nu * size_t(M);
+  const int sms = num_sms();
+  std::vector<int64_t> db(size_t(nrows) + 1, 0);
+  for(int k = 0; k < nrows; ++k) {
+    const int ii = k / nv, aa = k - ii * nv;
+    db[size_t(k) + 1] = db[k] + int64_t(ne - 1 - ii) * (nv - 1 - aa);
+  }
+  uint32_t* R = A.get<uint32_t>(tot + 1);
+  uint64_t* words = A.get<uint64_t>(sp.nu * NSW);
+  uint8_t* occ = A.get<uint8_t>(sp.nu * MAXORB);
+  uint8_t* vir = A.get<uint8_t>(sp.nu * MAXORB);
+  int64_t* dbase = A.get<int64_t>(db.size());
+  MB_CUDA(cudaMemcpyAsync(words, sp.words.data(), sp.nu * NSW * 8,
+                          cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaMemcpyAsync(occ, sp.occ.data(), sp.nu * MAXORB,
+                          cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaMemcpyAsync(vir, sp.vir.data(), sp.nu * MAXORB,
+                          cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaMemcpyAsync(dbase, db.data(), db.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  uint64_t* cand = A.get<uint64_t>(tot * NSW + NSW);
+  uint32_t* idx = A.get<uint32_t>(tot + 1);
+  cand_strings_k<NSW><<<grid_for(tot, 256, 16 * sms), 256, 0, s>>>(
+      words, occ, vir, sp.nu, ne, nv, M, int64_t(nrows), dbase, nrows, cand,
+      idx), note_launch();
+  MB_CUDA(cudaGetLastError());
+  {
+    uint64_t* cand2 = A.get<uint64_t>(tot * NSW + NSW);
+    uint32_t* idx2 = A.get<uint32_t>(tot + 1);
+    radix_sort<NSW, uint32_t>(cand, idx, cand2, idx2, tot, A);
+    A.release(cand2);
+    A.release(idx2);
+  }
+  uint32_t* f = A.get<uint32_t>(tot + 1);
+  uint32_t* fx = A.get<uint32_t>(tot + 1);
+  seg_flags_k<NSW><<<grid_for(tot, 256, 16 * sms), 256, 0, s>>>(cand, tot, f),
+      note_launch();
+  exclusive_scan<uint32_t, uint32_t>(f, fx, tot, fx + tot, A);
+  const size_t NL = to_host(fx + tot, s);
+  uint64_t* Ls = A.get<uint64_t>(NL * NSW + NSW);
+  rank_scatter_k<NSW><<<grid_for(tot, 256, 16 * sms), 256, 0, s>>>(
+      cand, idx, f, fx, tot, R, Ls), note_launch();
+  MB_CUDA(cudaGetLastError());
+  for(void* q : {static_cast<void*>(cand), static_cast<void*>(idx),
+                 static_cast<void*>(f), static_cast<void*>(fx),
+                 static_cast<void*>(words), static_cast<void*>(occ),
+                 static_cast<void*>(vir), static_cast<void*>(dbase)})
+    A.release(q);
+  out.R = R;
+  out.M = M;
+  out.N1 = int64_t(nrows);
+  *L = Ls;
+  return NL;
+}
+
+static int bits_for(size_t n) {
+  return n <= 1 ? 1 : 64 - __builtin_clzll(uint64_t(n - 1));
+}
+
+// Rank tables of both spins (RankTables), when they fit: the tables and
+// the distinct candidate strings within 10 % of the free device memory,
+// the candidate sort within half of it, 32-bit candidate indices and
+// bits_a + bits_b <= 64. Returns the key width in bits, 0 when not built.
+template <int NBITS>
+static int build_ranks(const SpinPlan& pa, const SpinPlan& pb, size_t ncdets,
+                       Arena& A, cudaStream_t s, RankTables& rt) {
+  constexpr int NSW = DetTraits<NBITS>::NSW;
+  const size_t ta = pa.nu * size_t(spin_candidates(pa.ne, pa.nv));
+  const size_t tb = pb.nu * size_t(spin_candidates(pb.ne, pb.nv));
+  if(ta >= (size_t(1) << 32) - 1 || tb >= (size_t(1) << 32) - 1) return 0;
+  const double avail = double(device_bytes_available());
+  const double persist = (4.0 + 8.0 * NSW + 2.0) * double(ta + tb) +
+                         8.0 * double(ncdets);
+  const double trans = double(std::max(ta, tb)) * (16.0 * NSW + 20.0);
+  if(persist > 0.1 * avail || persist + trans > 0.5 * avail) return 0;
+  uint64_t *La = nullptr, *Lb = nullptr;
+  SpinRanks ra, rb;
+  const size_t na = build_spin_ranks<NBITS>(pa, A, s, ra, &La);
+  const size_t nb = build_spin_ranks<NBITS>(pb, A, s, rb, &Lb);
+  const int ba = bits_for(na), bb = bits_for(nb);
+  if(ba + bb > 64) {
+    for(const void* q : {static_cast<const void*>(ra.R),
+                         static_cast<const void*>(rb.R),
+                         static_cast<const void*>(La),
+                         static_cast<const void*>(Lb)})
+      A.release(const_cast<void*>(q));
+    return 0;
+  }
+  uint16_t* bin = A.get<uint16_t>(na + 1);
+  string_bins_k<NSW><<<grid_for(na, 256, 4 * num_sms()), 256, 0, s>>>(
+      La, na, bin), note_launch();
+  int32_t* ai = A.get<int32_t>(ncdets);
+  int32_t* bi = A.get<int32_t>(ncdets);
+  MB_CUDA(cudaMemcpyAsync(ai, pa.idx.data(), ncdets * 4,
+                          cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaMemcpyAsync(bi, pb.idx.data(), ncdets * 4,
+                          cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaGetLastError());
+  ra.idx = ai;
+  rb.idx = bi;
+  rt.a = ra;
+  rt.b = rb;
+  rt.bits_a = ba;
+  rt.La = La;
+  rt.Lb = Lb;
+  rt.bin_a = bin;
+  return ba + bb;
 }
 
 static void check_net(const macis_b200_mlp* net, cudaStream_t s) {
@@ -1249,7 +1569,8 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, hbytes,
                         s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt,
                              nullptr, nullptr, nullptr, umask, nullptr, 0u,
-                             ASCI_BINS, 0u, 0u, dhist, AlphaLists{}),
+                             ASCI_BINS, 0u, 0u, dhist, AlphaLists{},
+                             RankTables{}),
         note_launch();
   }
   int64_t* uout = A.get<int64_t>(U + 1);
@@ -1263,7 +1584,43 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   // accumulated scores are complete (summed in generation order, as in the
   // unpartitioned search) and the range can go straight into the running
   // top-k: memory stays bounded by one range plus ~ndets_max candidates.
-  const double rs = double(NW * 8 + 8);
+  // ranked candidate keys (RankTables) for searches above 2^22 raw
+  // contributions (MACIS_B200_ASCI_RANKS: 0 off, 1 always)
+  std::vector<uint64_t> hdets;  // the core dets on the host, for the plans
+  auto host_dets = [&]() -> const std::vector<uint64_t>& {
+    if(hdets.empty() && ncdets) {
+      hdets.resize(ncdets * NW);
+      MB_CUDA(cudaMemcpyAsync(hdets.data(), cdets, ncdets * NW * 8,
+                              cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaStreamSynchronize(s));
+    }
+    return hdets;
+  };
+  SpinPlan pa;
+  bool pa_done = false;
+  auto alpha_plan = [&]() -> const SpinPlan& {
+    if(!pa_done) pa = plan_spin<NBITS>(host_dets(), ncdets, h->norb, 0);
+    pa_done = true;
+    return pa;
+  };
+  RankTables rt;
+  bool ranked = false;
+  if constexpr(NBITS > 64) {
+    const char* e = getenv("MACIS_B200_ASCI_RANKS");
+    const bool force = e && e[0] == '1', off = e && e[0] == '0';
+    if(U && !off && (force || Ptot >= (int64_t(1) << 22))) {
+      auto t_rk = std::chrono::steady_clock::now();
+      const SpinPlan& a = alpha_plan();
+      const SpinPlan b = plan_spin<NBITS>(host_dets(), ncdets, h->norb, 1);
+      if(a.nu && b.nu) {
+        const int bits = build_ranks<NBITS>(a, b, ncdets, A, s, rt);
+        ranked = bits > 0;
+        stats.key_bits = uint64_t(bits);
+      }
+      stats.rank_ms = ms_since(t_rk);
+    }
+  }
+  const double rs = ranked ? 16.0 : double(NW * 8 + 8);
   // per raw contribution while a range is processed: record + sort copy,
   // flags and radix tables (sort), then the unique list + kept copy + the
   // running top-k concatenation (few duplicates: unique ~ raw)
@@ -1332,26 +1689,26 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   }
   // alpha lists (AlphaLists) when the ranges need count passes of their own:
   // memory for them, at most 15 % of what is free, comes off the range size
-  AlphaPlan ap;
+  SpinPlan ap;
   int g_est = 0;
   const char* al_env = getenv("MACIS_B200_ASCI_ALPHA_LISTS");
   const bool al_allowed = !(al_env && al_env[0] == '0');
   if(al_allowed && !pairs_only && !st.just_singles && bin_lo < bin_hi &&
      ((part && part->count > 1) || Ppart > uint64_t(cap))) {
-    ap = plan_alpha<NBITS>(cdets, ncdets, h->norb, s);
-    if(ap.nua) {
+    ap = alpha_plan();
+    if(ap.nu) {
       g_est = int(std::min<uint64_t>(254, 2 * ((Ppart + cap - 1) / cap) + 2));
-      const double nk = double(ap.nA) * ap.nvA;
-      const double pairs2 = double(ap.nA) * (ap.nA - 1) / 2 * double(ap.nvA) *
-                            (ap.nvA - 1) / 2;
+      const double nk = double(ap.ne) * ap.nv;
+      const double pairs2 = double(ap.ne) * (ap.ne - 1) / 2 * double(ap.nv) *
+                            (ap.nv - 1) / 2;
       const double bytes =
-          double(ap.nua) * (nk * (18.0 + 2.0 * (g_est + 1)) + 2.0 * pairs2 + 2.0) +
-          4.0 * double(ncdets + ap.nua) + 8192.0;
+          double(ap.nu) * (nk * (18.0 + 2.0 * (g_est + 1)) + 2.0 * pairs2 + 2.0) +
+          4.0 * double(ncdets + ap.nu) + 8192.0;
       if(bytes <= 0.15 * double(device_bytes_available())) {
         if(!cap_env)
           cap = std::max<int64_t>(cap - int64_t(bytes / per_pair), int64_t(1) << 20);
       } else {
-        ap = AlphaPlan{};
+        ap = SpinPlan{};
       }
     }
   }
@@ -1389,11 +1746,11 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   // groups of the alpha lists: the unsplit ranges
   std::vector<int> rgrp(nr, -1);
   AlphaLists al;
-  if(ap.nua) {
+  if(ap.nu) {
     int G = 0;
     for(uint32_t r = 0; r < nr; ++r)
       if(rns[r] == 0) rgrp[r] = G++;
-    if(G > g_est || G == 0 || (G < 2 && 2 * ap.nua > ncdets)) {
+    if(G > g_est || G == 0 || (G < 2 && 2 * ap.nu > ncdets)) {
       std::fill(rgrp.begin(), rgrp.end(), -1);
     } else {
       std::vector<uint8_t> gt(ASCI_BINS, 255);
@@ -1403,16 +1760,16 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       uint8_t* grp = A.get<uint8_t>(ASCI_BINS);
       MB_CUDA(cudaMemcpyAsync(grp, gt.data(), ASCI_BINS, cudaMemcpyHostToDevice, s));
       int32_t* aidx = A.get<int32_t>(ncdets);
-      int32_t* rep = A.get<int32_t>(ap.nua);
-      MB_CUDA(cudaMemcpyAsync(aidx, ap.aidx.data(), ncdets * 4,
+      int32_t* rep = A.get<int32_t>(ap.nu);
+      MB_CUDA(cudaMemcpyAsync(aidx, ap.idx.data(), ncdets * 4,
                               cudaMemcpyHostToDevice, s));
-      MB_CUDA(cudaMemcpyAsync(rep, ap.rep.data(), ap.nua * 4,
+      MB_CUDA(cudaMemcpyAsync(rep, ap.rep.data(), ap.nu * 4,
                               cudaMemcpyHostToDevice, s));
       al.aidx = aidx;
-      al.NK = ap.nA * ap.nvA;
+      al.NK = ap.ne * ap.nv;
       al.G = G;
-      const size_t rows = ap.nua * size_t(al.NK);
-      uint16_t* abin = A.get<uint16_t>(ap.nua);
+      const size_t rows = ap.nu * size_t(al.NK);
+      uint16_t* abin = A.get<uint16_t>(ap.nu);
       uint16_t* kbin = A.get<uint16_t>(rows + 1);
       uint16_t* rel = A.get<uint16_t>(rows * (G + 1) + 1);
       int64_t* base = A.get<int64_t>(rows + 1);
@@ -1424,7 +1781,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       if(rows) {
         int64_t* tot = A.get<int64_t>(rows + 1);
         alpha_count_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
-                               s>>>(I, cd, rep, ap.nua, ap.nA, ap.nvA,
+                               s>>>(I, cd, rep, ap.nu, ap.ne, ap.nv,
                                     st.h_el_tol, grp, al, rel, kbin, abin, tot),
             note_launch();
         MB_CUDA(cudaGetLastError());
@@ -1436,10 +1793,10 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       al.q = ql;
       if(E)
         alpha_fill_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
-                              s>>>(I, cd, rep, ap.nua, ap.nA, ap.nvA,
+                              s>>>(I, cd, rep, ap.nu, ap.ne, ap.nv,
                                    st.h_el_tol, grp, al, ql), note_launch();
       MB_CUDA(cudaGetLastError());
-      stats.alpha_strings = ap.nua;
+      stats.alpha_strings = ap.nu;
     }
   }
   stats.pairs_ms = ms_since(t_all);
@@ -1523,22 +1880,32 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
                             s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,
                                  nullptr, nullptr, nullptr, umask, nullptr,
                                  rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr,
-                                 AlphaLists{}), note_launch();
+                                 AlphaLists{}, RankTables{}), note_launch();
       }
       exclusive_scan<int64_t, int64_t>(rc, off, size_t(U), off + U, B);
       P = to_host(off + U, s);
     }
-    uint64_t* keys = B.get<uint64_t>(size_t(P) * NW + NW);
+    const size_t KWr = ranked ? 1 : NW;  // words per record key
+    uint64_t* keys = B.get<uint64_t>(size_t(P) * KWr + KWr);
     double* rv = B.get<double>(size_t(P) + 1);
     if(P) {
-      units_k<NBITS, 1><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0, s>>>(
-          I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, off, keys, rv, umask,
-          umax, rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr,
-          rgrp[rr] >= 0 && rc != ucnt ? [&] {
-            AlphaLists alr = al;
-            alr.g = rgrp[rr];
-            return alr;
-          }() : AlphaLists{}), note_launch();
+      AlphaLists alr{};
+      if(rgrp[rr] >= 0 && rc != ucnt) {
+        alr = al;
+        alr.g = rgrp[rr];
+      }
+      if(ranked)
+        units_k<NBITS, 2><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0,
+                            s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,
+                                 off, keys, rv, umask, umax, rlo[rr], rhi[rr],
+                                 rns[rr], rsub[rr], nullptr, alr, rt),
+            note_launch();
+      else
+        units_k<NBITS, 1><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0,
+                            s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,
+                                 off, keys, rv, umask, umax, rlo[rr], rhi[rr],
+                                 rns[rr], rsub[rr], nullptr, alr,
+                                 RankTables{}), note_launch();
       MB_CUDA(cudaGetLastError());
     }
     MB_CUDA(cudaStreamSynchronize(s));
@@ -1548,8 +1915,11 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     Pairs uq;
     uint64_t* k2 = nullptr;
     double* r2 = nullptr;
-    if(P) {
-      k2 = B.get<uint64_t>(size_t(P) * NW + NW);
+    // KW key words per record; group(dg) the sort-group functor of a bin ->
+    // group table
+    auto accumulate = [&](auto kw, auto group) {
+      constexpr int KW = decltype(kw)::value;
+      k2 = B.get<uint64_t>(size_t(P) * KW + KW);
       r2 = B.get<double>(size_t(P) + 1);
       // a large range is first split by bin into groups that are sorted
       // one at a time: the digit passes of a sort over fewer records run
@@ -1558,7 +1928,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       // are complete and in generation order
       std::vector<size_t> goff{0, size_t(P)};
       if(!pairs_only && rns[rr] == 0 && rhi[rr] - rlo[rr] > 1 &&
-         P > sort_group_cap) {
+         uint64_t(P) > sort_group_cap) {
         load_hist();
         std::vector<uint8_t> gt(ASCI_BINS, 0);
         int g = 0;
@@ -1575,8 +1945,8 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
           uint8_t* dg = B.get<uint8_t>(ASCI_BINS);
           MB_CUDA(cudaMemcpyAsync(dg, gt.data(), ASCI_BINS,
                                   cudaMemcpyHostToDevice, s));
-          goff = stable_partition<NW, double>(keys, rv, k2, r2, size_t(P),
-                                              g + 1, BinGroup<NBITS>{dg}, B);
+          goff = stable_partition<KW, double>(keys, rv, k2, r2, size_t(P),
+                                              g + 1, group(dg), B);
           std::swap(keys, k2);
           std::swap(rv, r2);
           stats.sort_pass_items += uint64_t(P);
@@ -1585,19 +1955,19 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       for(size_t gi = 0; gi + 1 < goff.size(); ++gi) {
         const size_t a = goff[gi], m = goff[gi + 1] - a;
         stats.sort_pass_items +=
-            uint64_t(radix_sort<NW, double>(keys + a * NW, rv + a,
-                                            k2 + a * NW, r2 + a, m, B)) *
+            uint64_t(radix_sort<KW, double>(keys + a * KW, rv + a,
+                                            k2 + a * KW, r2 + a, m, B)) *
             uint64_t(m);
       }
       uint32_t* f = B.get<uint32_t>(size_t(P) + 1);
       uint32_t* fx = B.get<uint32_t>(size_t(P) + 1);
-      seg_flags_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
+      seg_flags_k<KW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
           keys, size_t(P), f), note_launch();
       exclusive_scan<uint32_t, uint32_t>(f, fx, size_t(P), fx + P, B);
       const uint32_t nu = to_host(fx + P, s);
       int64_t* start = B.get<int64_t>(nu + 1);
       // unique keys into k2, sums into r2
-      seg_starts_k<NW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
+      seg_starts_k<KW><<<grid_for(size_t(P), 256, 16 * sms), 256, 0, s>>>(
           f, fx, size_t(P), start, keys, k2), note_launch();
       seg_sum_k<<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(
           start, nu, size_t(P), rv, r2), note_launch();
@@ -1606,6 +1976,27 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
                      static_cast<void*>(start), static_cast<void*>(keys),
                      static_cast<void*>(rv)})
         B.release(q);
+      return nu;
+    };
+    if(P) {
+      uint32_t nu = 0;
+      if(ranked) {
+        nu = accumulate(std::integral_constant<int, 1>{},
+                        [&](const uint8_t* dg) {
+                          return RankBinGroup{
+                              dg, rt.bin_a, (uint64_t(1) << rt.bits_a) - 1};
+                        });
+        // ranked keys back to determinants
+        uint64_t* kd = B.get<uint64_t>(size_t(nu) * NW + NW);
+        if(nu)
+          unrank_k<NBITS><<<grid_for(nu, 256, 16 * sms), 256, 0, s>>>(
+              k2, nu, rt, kd), note_launch();
+        B.release(k2);
+        k2 = kd;
+      } else {
+        nu = accumulate(std::integral_constant<int, NW>{},
+                        [&](const uint8_t* dg) { return BinGroup<NBITS>{dg}; });
+      }
       uq.keys = k2;
       uq.rv = r2;
       uq.n = nu;

@@ -278,27 +278,36 @@ def test_onesweep_sort_matches_classic_passes(monkeypatch):
 
 @pytest.mark.parametrize("nbits,n,k,ncore,nalpha,top",
                          [(128, 48, 12, 300, 80, 40), (256, 100, 20, 8, 6, 4)])
-def test_alpha_lists_match_per_contribution_bins(monkeypatch, nbits, n, k,
-                                                 ncore, nalpha, top):
-    """Candidate ranges that take their alpha-double counts and contributions
-    from per-alpha-string lists (the default once a search needs several
-    ranges) against ranges that test every contribution's bin
-    (MACIS_B200_ASCI_ALPHA_LISTS=0) and against the single-range search:
-    identical selections and recorded unit targets, with a range cap that
-    leaves every range whole and one small enough to split the heaviest
-    alpha-string bin by beta string; exact and screened."""
+def test_ranked_keys_and_alpha_lists_match_plain_search(monkeypatch, nbits, n,
+                                                        k, ncore, nalpha, top):
+    """The candidate paths of a large search against the plain one (one
+    range, candidates sorted by their determinant bitsets,
+    MACIS_B200_ASCI_RANKS=0): candidates sorted by ranked keys (alpha and
+    beta string ranks; the default above 2^22 contributions), and candidate
+    ranges that take their alpha-double counts and contributions from
+    per-alpha-string lists (the default once a search needs several ranges)
+    or test every contribution's bin (MACIS_B200_ASCI_ALPHA_LISTS=0), with a
+    range cap that leaves every range whole and one small enough to split
+    the heaviest alpha-string bin by beta string. Identical accumulated
+    candidates and scores, selections (exact and screened) and recorded
+    unit targets."""
     from cases import core_set
     T, V = mb.synthetic_integrals(n, 0)
     cd, C = core_set(n, k, ncore, nbits, nalpha=nalpha, top=top)
     H = mb.HamiltonianGenerator(T, V, nbits)
     E0 = float(H.matrix_element(cd[:1], cd[:1])) - 0.5
-    net = mb.ScreeningNetwork(nbits=nbits, seed=0)
-    keep = mb.ScreenSettings(network=net, keep_frac=0.4, explore_frac=0.0,
-                             train=False)
+    keep = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=nbits, seed=0),
+                             keep_frac=0.4, explore_frac=0.0, train=False)
     rec = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=nbits, seed=1),
                             max_samples=200000)
 
-    def run():
+    def run(ranks, lists="1", cap=None):
+        monkeypatch.setenv("MACIS_B200_ASCI_RANKS", ranks)
+        monkeypatch.setenv("MACIS_B200_ASCI_ALPHA_LISTS", lists)
+        if cap is None:
+            monkeypatch.delenv("MACIS_B200_ASCI_BATCH_PAIRS", raising=False)
+        else:
+            monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", str(cap))
         exact = mb.asci_search(_settings(), 40000, cd, E0, C, n, H)
         st = mb.last_search_stats(H)
         scr = mb.asci_search(_settings(), 40000, cd, E0, C, n, H, screen=keep,
@@ -306,20 +315,28 @@ def test_alpha_lists_match_per_contribution_bins(monkeypatch, nbits, n, k,
         mb.asci_search(_settings(), 40000, cd, E0, C, n, H, screen=rec)
         return exact, scr, rec.network.samples(), st
 
-    one = run()
-    assert one[3]["batches"] == 1 and one[3]["alpha_strings"] == 0
-    raw = one[3]["raw_pairs"]
+    def same(a, b):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        assert np.array_equal(a[2][0], b[2][0])
+        assert np.array_equal(a[2][1], b[2][1])
+
+    plain = run("0")
+    st = plain[3]
+    assert st["batches"] == 1 and st["key_bits"] == 0
+    assert st["alpha_strings"] == 0
+    ranked = run("1")
+    assert 0 < ranked[3]["key_bits"] < 2 * n
+    same(ranked, plain)
+    monkeypatch.setenv("MACIS_B200_ASCI_RANKS", "1")
+    pr = mb.asci_pairs(_settings(), cd, E0, C, H)
+    monkeypatch.setenv("MACIS_B200_ASCI_RANKS", "0")
+    pp = mb.asci_pairs(_settings(), cd, E0, C, H)
+    assert np.array_equal(pr[0], pp[0]) and np.array_equal(pr[1], pp[1])
+    raw = st["raw_pairs"]
     for cap in (raw // 12, raw // 150):
-        monkeypatch.setenv("MACIS_B200_ASCI_BATCH_PAIRS", str(cap))
-        lists = run()
-        assert lists[3]["batches"] > 3
-        assert lists[3]["alpha_strings"] > 0
-        monkeypatch.setenv("MACIS_B200_ASCI_ALPHA_LISTS", "0")
-        bins = run()
-        assert bins[3]["alpha_strings"] == 0
-        monkeypatch.delenv("MACIS_B200_ASCI_ALPHA_LISTS")
-        for got in (lists, bins):
-            assert np.array_equal(got[0], one[0])
-            assert np.array_equal(got[1], one[1])
-            assert np.array_equal(got[2][0], one[2][0])
-            assert np.array_equal(got[2][1], one[2][1])
+        for ranks, lists in (("1", "1"), ("1", "0"), ("0", "1")):
+            got = run(ranks, lists, cap)
+            assert got[3]["batches"] > 3
+            assert (got[3]["alpha_strings"] > 0) == (lists == "1")
+            assert (got[3]["key_bits"] > 0) == (ranks == "1")
+            same(got, plain)
