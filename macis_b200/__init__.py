@@ -17,7 +17,8 @@ Importing the package loads the native library and fails if it is missing.
 from ._lib import MacisError  # noqa: F401  (loads libmacis_b200.so)
 from .asci import (ASCISettings, MCSCFSettings, asci_grow, asci_iter,  # noqa
                    asci_pairs, asci_refine, asci_search, asci_search_part,
-                   last_search_stats, merge_asci_parts, reorder_ci_on_coeff)
+                   last_search_stats, merge_asci_parts, reorder_ci_on_coeff,
+                   topk_recall)
 from .hamiltonian import (DeviceCSR, HamiltonianGenerator,  # noqa: F401
                           MatrixFreeHamiltonian, make_csr_hamiltonian,
                           make_csr_hamiltonian_block, row_bounds)

@@ -26,7 +26,7 @@ from .solvers import FP64, selected_ci_diag
 __all__ = ["ASCISettings", "MCSCFSettings", "asci_search", "asci_pairs",
            "asci_search_part", "merge_asci_parts",
            "asci_iter", "asci_grow", "asci_refine", "reorder_ci_on_coeff",
-           "last_search_stats"]
+           "last_search_stats", "topk_recall"]
 
 
 @dataclass
@@ -208,7 +208,22 @@ def _screened(screen):
     """Whether the next search prunes by prediction."""
     return (screen is not None and screen.network is not None and
             screen.network.trained_steps > 0 and
-            screen.searches >= screen.warmup_searches)
+            screen.searches >= screen.warmup_searches and
+            screen.keep_frac < 1.0)
+
+
+def topk_recall(got, exact, ncore):
+    """Fraction of the exact search's new determinants (all but the trailing
+    ncore core determinants) that another search of the same core set also
+    selected."""
+    ne, ng = len(exact) - ncore, len(got) - ncore
+    if ne <= 0:
+        return 1.0
+    W = exact.shape[1]
+    key = np.dtype((np.void, 8 * W))
+    a = np.ascontiguousarray(exact[:ne]).view(key).ravel()
+    b = np.ascontiguousarray(got[:max(ng, 0)]).view(key).ravel()
+    return float(np.isin(a, b).sum()) / ne
 
 
 def _use_net(screen, ham_gen, cdets, E0, C):
@@ -221,6 +236,23 @@ def _use_net(screen, ham_gen, cdets, E0, C):
         _, nunits = unit_features(ham_gen, cdets, E0, C, 0, 0)
         use_net = nunits >= screen.min_units
     return use_net
+
+
+def _recall_check(screen, use_net, st, got, ncore, ham_gen, exact_search):
+    """The recall check of ScreenSettings after a pruning search `got` with
+    statistics st: when it applies, the exact search of the same core set
+    (exact_search(), recording unbiased samples for the training that
+    follows) replaces the result, its top-k recall is measured and
+    keep_frac doubles below recall_target. Returns (dets, recall or None,
+    statistics for the training)."""
+    if not (use_net and screen.recall_target and
+            st["units_total"] <= screen.check_units_max):
+        return got, None, st
+    exact = exact_search()
+    recall = topk_recall(got, exact, ncore)
+    if recall < screen.recall_target:
+        screen.keep_frac = min(1.0, 2.0 * screen.keep_frac)
+    return exact, recall, dict(st, samples=last_search_stats(ham_gen)["samples"])
 
 
 def _train_after_search(screen, stats):
@@ -249,10 +281,15 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
         wfn, X = reorder_ci_on_coeff(wfn, X)
     nkeep = min(int(asci_settings.ncdets_max), len(wfn))
     t0 = time.perf_counter()
-    use_net = _use_net(screen, ham_gen, wfn[:nkeep], E0, X[:nkeep])
-    wfn = asci_search(asci_settings, ndets_max, wfn[:nkeep], E0, X[:nkeep],
-                      norb, ham_gen, screen=screen, use_net=use_net)
+    core, Cc = wfn[:nkeep], X[:nkeep]
+    use_net = _use_net(screen, ham_gen, core, E0, Cc)
+    wfn = asci_search(asci_settings, ndets_max, core, E0, Cc, norb, ham_gen,
+                      screen=screen, use_net=use_net)
     st = last_search_stats(ham_gen)
+    wfn, recall, st = _recall_check(
+        screen, use_net, st, wfn, nkeep, ham_gen,
+        lambda: asci_search(asci_settings, ndets_max, core, E0, Cc, norb,
+                            ham_gen, screen=screen, use_net=False))
     t1 = time.perf_counter()
     train_ms = _train_after_search(screen, st)
     t1b = time.perf_counter()
@@ -269,7 +306,8 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
         ndets=len(wfn), E=E, search_ms=(t1 - t0) * 1e3, train_ms=train_ms,
         diag_ms=(t2 - t1b) * 1e3, screened=bool(use_net),
         units_total=st["units_total"], units_kept=st["units_kept"],
-        raw_pairs=st["raw_pairs"], **tim))
+        raw_pairs=st["raw_pairs"], recall_check=recall,
+        keep_frac=None if screen is None else screen.keep_frac, **tim))
     return E, wfn, X
 
 

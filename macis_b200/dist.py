@@ -427,7 +427,7 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
     eigenvector all-gathered to every rank. screen as in asci.asci_iter,
     with an equal network on every rank. Only the reference solver is
     distributed: FP64 values, no thick restart."""
-    from .asci import (_dets, _train_after_search, _use_net,
+    from .asci import (_dets, _recall_check, _train_after_search, _use_net,
                        last_search_stats, reorder_ci_on_coeff)
     from .solvers import FP64
     if mcscf_settings.precision != FP64 or mcscf_settings.davidson_restart_keep:
@@ -439,11 +439,18 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
     if len(wfn) > 1:
         wfn, X = reorder_ci_on_coeff(wfn, X)
     nkeep = min(int(asci_settings.ncdets_max), len(wfn))
-    use_net = _use_net(screen, ham_gen, wfn[:nkeep], E0, X[:nkeep])
-    wfn = asci_search(asci_settings, ndets_max, wfn[:nkeep], E0, X[:nkeep],
-                      norb, ham_gen, group, screen=screen, use_net=use_net)
+    core, Cc = wfn[:nkeep], X[:nkeep]
+    use_net = _use_net(screen, ham_gen, core, E0, Cc)
+    wfn = asci_search(asci_settings, ndets_max, core, E0, Cc, norb, ham_gen,
+                      group, screen=screen, use_net=use_net)
     if screen is not None:
-        _train_after_search(screen, last_search_stats(ham_gen))
+        # the recall check of asci.asci_iter; every rank holds the merged
+        # results and the same statistics, so all take the same branch
+        wfn, _, st = _recall_check(
+            screen, use_net, last_search_stats(ham_gen), wfn, nkeep, ham_gen,
+            lambda: asci_search(asci_settings, ndets_max, core, E0, Cc, norb,
+                                ham_gen, group, screen=screen, use_net=False))
+        _train_after_search(screen, st)
     E, X_local = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,
                                   mcscf_settings.ci_max_subspace,
                                   mcscf_settings.ci_res_tol, None, group)

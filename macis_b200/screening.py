@@ -147,6 +147,13 @@ class ScreenSettings:
     train: bool = True            # retrain after every search
     seed: int = 0
     searches: int = 0             # searches run so far (updated)
+    # Recall check: a pruning search of asci_iter / asci_grow / asci_refine
+    # with at most check_units_max units is also run exactly; its top-k
+    # recall against the exact selection is measured, the exact selection is
+    # kept, and below recall_target keep_frac doubles (at 1 pruning stops).
+    # 0 turns the check off.
+    recall_target: float = 0.95
+    check_units_max: int = 20_000_000
 
     def c_struct(self, use_net):
         return _lib.AsciScreenC(

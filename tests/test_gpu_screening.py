@@ -230,3 +230,37 @@ def test_trained_network_gains_over_the_search_without_it():
     assert st_l["raw_pairs"] <= 0.5 * st_exact["raw_pairs"]
     assert r_l >= r_c + 0.05 and r_l >= r_f + 0.15
     assert dl < 0.7 * dc and dl < df
+
+
+def test_recall_check_keeps_exact_selections():
+    """Pruning searches small enough for the recall check
+    (ScreenSettings.check_units_max) also run exactly and keep the exact
+    selection: a screened grow follows the unscreened grow determinant for
+    determinant, the measured recalls are logged, and keep_frac doubles
+    after every check below recall_target (above 1 here, so every check
+    fails) until pruning stops at keep_frac 1."""
+    norb, nbits, na, nb = 16, 64, 5, 5
+    T, V, H = _ham(norb, nbits, seed=2)
+    _, _, (E0, d0, X0) = _grow(H, norb, nbits, na, nb, 6000, 1500)
+    scr = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=nbits, seed=0),
+                            min_units=0, recall_target=1.01,
+                            check_units_max=10 ** 12)
+    _, m, (E1, d1, X1) = _grow(H, norb, nbits, na, nb, 6000, 1500, scr)
+    assert np.array_equal(d1, d0) and abs(E1 - E0) < 1e-9
+    log = m.iteration_log
+    checks = [it["recall_check"] for it in log if it["screened"]]
+    assert len(checks) >= 2 and all(0.0 <= r <= 1.0 for r in checks)
+    assert scr.keep_frac == min(1.0, 0.2 * 2 ** len(checks))
+    assert all(it["recall_check"] is None for it in log if not it["screened"])
+    # a check that passes leaves keep_frac alone
+    sc2 = mb.ScreenSettings(network=scr.network, recall_target=0.0,
+                            min_units=0, check_units_max=10 ** 12)
+    sc2.searches = sc2.warmup_searches
+    s = mb.ASCISettings(ntdets_max=6000, ntdets_min=100, ncdets_max=1500,
+                        h_el_tol=1e-8)
+    m2 = mb.MCSCFSettings(ci_max_subspace=60, davidson_restart_keep=8,
+                          davidson_max_iter=400)
+    mb.asci_iter(s, m2, 6000, E1, d1, X1, H, norb, sc2)
+    assert m2.iteration_log[-1]["screened"]
+    assert m2.iteration_log[-1]["recall_check"] is not None
+    assert sc2.keep_frac == 0.2
