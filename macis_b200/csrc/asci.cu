@@ -45,6 +45,9 @@ struct CoreData {
   int64_t* uoff;  // ncdets+1 unit offsets
   int32_t* udet;  // per unit: the core det it belongs to
   const double* pairmax;  // 2 n^2 outer-pair integral bounds (screening)
+  const double* VT;       // V with its index pairs swapped (ham_vt): the
+                          // opposite-spin elements of one outer pair are a
+                          // contiguous row
 };
 
 // udet[u] = c for the units u of core det c (one warp per det): one load
@@ -603,8 +606,10 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
         const int j = occB[qd], b = virB[int(q) - qd * nvB];
         const bool inr =
             !chkb || beta_sub<NSW>(sp_flip(sp_flip(sB, j), b), nsub) == sub;
+        // V(a,i,b,j) from row (a,i) of the pair-swapped copy: consecutive
+        // inner indices read neighbouring addresses
         const double Vv =
-            inr ? __ldg(I.V + a + size_t(i) * n + size_t(b + size_t(j) * n) * n * n)
+            inr ? __ldg(cd.VT + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n)
                 : 0.0;
         keep = inr && !(fabs(Vv) < tol);
         if(MODE >= 1 && keep) {
@@ -1243,6 +1248,7 @@ static int64_t core_setup(macis_b200_ham* h, Arena& A, const uint64_t* cdets,
     MB_CUDA(cudaGetLastError());
   }
   cd.pairmax = h->pairmax;
+  cd.VT = ham_vt(h);
   if(ncdets) {
     core_prep_k<NBITS><<<grid_for(ncdets * 32, 256, 16 * sms), 256, 0, s>>>(
         h->ints(), cd, just_singles, units), note_launch();

@@ -439,6 +439,18 @@ __global__ void v_pair_transpose_k(const double* V, double* VT, int n) {
     VT[(x % n2) * n2 + x / n2] = V[x];
 }
 
+const double* ham_vt(macis_b200_ham* h) {
+  if(!h->VT) {
+    const int n = h->norb;
+    const size_t n4 = size_t(n) * n * n * n;
+    MB_CUDA(dev_malloc(&h->VT, n4 * 8));
+    v_pair_transpose_k<<<grid_for(n4, 256, 8 * num_sms()), 256, 0, h->stream>>>(
+        h->V, h->VT, n), note_launch();
+    MB_CUDA(cudaGetLastError());
+  }
+  return h->VT;
+}
+
 __device__ __forceinline__ double sgnd(uint32_t w, double v) {
   return (w >> 31) ? -v : v;  // == sign * v for sign in {+1, -1}
 }
@@ -1864,11 +1876,7 @@ static void build_impl(macis_b200_ham* h, const uint64_t* bra, size_t nbra,
       }
     }
     const unsigned g = unsigned(std::max(1, per_sm) * sms);
-    if(!h->VT) {
-      const size_t n4 = size_t(nn) * nn * nn * nn;
-      MB_CUDA(dev_malloc(&h->VT, n4 * 8));
-      v_pair_transpose_k<<<grid_for(n4, 256, 8 * sms), 256, 0, s>>>(h->V, h->VT, nn), note_launch();
-    }
+    ham_vt(h);
     NvtxRange nv_fill("macis_b200: direct-product fill");
     cudaEventRecord(ev[0], s);
     dp_fill_k<NBITS, CI, VT><<<g, DP_THREADS, Ls.bytes, s>>>(

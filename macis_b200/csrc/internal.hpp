@@ -163,6 +163,9 @@ void small_syev_lowest(int k, const double* lower, int nwant, double* W,
 struct AsciPart {
   uint32_t index = 0, count = 1;
 };
+// V with its index pairs swapped (macis_b200_ham::VT), built on first use.
+const double* ham_vt(macis_b200_ham* h);
+
 void asci_search_device(macis_b200_ham* h, const macis_b200_asci_settings& s,
                         const macis_b200_asci_screen* scr, size_t ndets_max,
                         const uint64_t* cdets, size_t ncdets, double E0,

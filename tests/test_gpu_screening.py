@@ -253,7 +253,7 @@ def test_recall_check_keeps_exact_selections():
     assert scr.keep_frac == min(1.0, 0.2 * 2 ** len(checks))
     assert all(it["recall_check"] is None for it in log if not it["screened"])
     # a check that passes leaves keep_frac alone
-    sc2 = mb.ScreenSettings(network=scr.network, recall_target=0.0,
+    sc2 = mb.ScreenSettings(network=scr.network, recall_target=1e-9,
                             min_units=0, check_units_max=10 ** 12)
     sc2.searches = sc2.warmup_searches
     s = mb.ASCISettings(ntdets_max=6000, ntdets_min=100, ncdets_max=1500,
