@@ -572,14 +572,14 @@ def extras(mb, H, dets, torch):
     return out
 
 
-def _n48_core(mb, ncore, seed=0):
+def _n48_core(mb, ncore, seed=0, n=48, k=12, nbits=128):
     """n = 48 orbitals, 12 alpha / 12 beta, bitset<128>: HF plus products of
     its low single / double alpha and beta excitations, ordered by total
     excitation degree, as the core set, with decaying coefficients
-    (C3-shaped)."""
-    n, k = 48, 12
+    (C3-shaped). Other shapes through n, k (electrons per spin) and nbits
+    (C5: 100, 20, 256)."""
     T, V = mb.synthetic_integrals(n, seed)
-    H = mb.HamiltonianGenerator(T, V, 128)
+    H = mb.HamiltonianGenerator(T, V, nbits)
     rng = np.random.default_rng(seed)
     top = max(200, int(np.ceil(np.sqrt(ncore))) + 8)
     hf = (1 << k) - 1
@@ -596,7 +596,7 @@ def _n48_core(mb, ncore, seed=0):
     pairs = [(a, b) for a in alphas[:top] for b in alphas[:top]]
     pairs.sort(key=lambda ab: bin(ab[0] ^ hf).count("1") + bin(ab[1] ^ hf).count("1"))
     pairs = pairs[:ncore]
-    core = mb.sd.make_dets([a for a, _ in pairs], [b for _, b in pairs], 128)
+    core = mb.sd.make_dets([a for a, _ in pairs], [b for _, b in pairs], nbits)
     C = np.exp(-0.5 * np.arange(len(core)) / 100.0)
     C /= np.linalg.norm(C)
     hd = H.matrix_element(core[:1], core[:1])
@@ -711,12 +711,13 @@ def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
     E_l, X_l = mb.selected_ci_diag(dets_l, H, THRESH, 40, 1e-8,
                                    precision=MIXED, timings=tl, **dav)
     t_learned = time.perf_counter() - t0
-    A = mb.make_csr_hamiltonian(dets_l, H, THRESH, np.int64)
+    try:  # the FP64 H: stored when it fits, else applied matrix-free
+        A = mb.make_csr_hamiltonian(dets_l, H, THRESH, np.int64)
+    except mb.MacisError:
+        A = mb.MatrixFreeHamiltonian(dets_l, H, THRESH)
     E_l64 = float(X_l @ A.spmv(X_l)) / float(X_l @ X_l)
     del A
-    ea = set(map(bytes, dets_e[:len(dets_e) - len(core)]))
-    recall = sum(1 for d in dets_l[:len(dets_l) - len(core)]
-                 if bytes(d) in ea) / max(len(ea), 1)
+    recall = mb.topk_recall(dets_l, dets_e, len(core))
     out = {
         "workload": f"ASCI iteration: n = {n}, bitset<{nbits}>, "
                     f"{len(core)} core dets -> {len(dets_e)} dets, synthetic "
