@@ -661,7 +661,11 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
 #undef G2R
 #undef V2R
 
-// Warp per unit over the global unit range [u0, u1) of the batch.
+// Units [u0, u1) of the batch, a warp at a time over runs of 32
+// consecutive units: the lanes read the 32 units' masks, counts, owners and
+// output offsets at once, and the warp runs the units with work one after
+// another (a fill pass skips the units without contributions in its range:
+// output positions come from the offsets, not from the order).
 template <int NBITS, int MODE>
 __global__ void __launch_bounds__(256)
     units_k(Ints I, CoreData cd, int64_t u0, int64_t u1, size_t c0, size_t c1,
@@ -676,21 +680,38 @@ __global__ void __launch_bounds__(256)
     for(uint32_t i = threadIdx.x; i < ASCI_BINS; i += blockDim.x) shist[i] = 0;
     __syncthreads();
   }
-  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
-  for(int64_t u = u0 + int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      u < u1; u += int64_t(nwarp)) {
-    if(umask && !umask[u]) {  // screened out: no contributions
-      if(MODE == 0 && (threadIdx.x & 31) == 0) counts[u - u0] = 0;
-      continue;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarp = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for(int64_t ub = u0 + (int64_t(blockIdx.x) * (blockDim.x >> 5) +
+                         (threadIdx.x >> 5)) * 32;
+      ub < u1; ub += nwarp * 32) {
+    const int64_t ul = ub + lane;
+    bool run = ul < u1;
+    if(run && umask && !umask[ul]) {  // screened out: no contributions
+      if(MODE == 0) counts[ul - u0] = 0;
+      run = false;
     }
-    if(MODE >= 1 && al.g >= 0 && counts[u - u0] == 0) continue;
-    // core det owning unit u (in [c0, c1))
-    const size_t lo = size_t(cd.udet[u]);
-    const int64_t t = u - cd.uoff[lo];
-    unit_run<NBITS, MODE>(I, cd, lo, t, E0, tol, counts + (u - u0),
-                          MODE ? outoff[u - u0] : 0, keys, rv,
-                          umax ? umax + u : nullptr, blo, bhi, nsub, sub,
-                          hist ? shist : nullptr, al, rt);
+    int64_t off = 0;
+    if(MODE >= 1 && run) {
+      run = counts[ul - u0] != 0;
+      off = outoff[ul - u0];
+    }
+    int32_t own = 0;
+    int64_t t = 0;
+    if(run) {  // core det owning unit ul (in [c0, c1)), and its index there
+      own = cd.udet[ul];
+      t = ul - cd.uoff[own];
+    }
+    for(unsigned m = __ballot_sync(0xffffffffu, run); m; m &= m - 1) {
+      const int l = __ffs(m) - 1;
+      const int64_t u = ub + l;
+      const size_t c = size_t(__shfl_sync(0xffffffffu, own, l));
+      const int64_t tu = __shfl_sync(0xffffffffu, t, l);
+      const int64_t ou = __shfl_sync(0xffffffffu, off, l);
+      unit_run<NBITS, MODE>(I, cd, c, tu, E0, tol, counts + (u - u0), ou, keys,
+                            rv, umax ? umax + u : nullptr, blo, bhi, nsub, sub,
+                            hist ? shist : nullptr, al, rt);
+    }
   }
   if(hist) {
     __syncthreads();
@@ -1572,7 +1593,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     MB_CUDA(cudaFuncSetAttribute(units_k<NBITS, 0>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(hbytes)));
-    units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, hbytes,
+    units_k<NBITS, 0><<<grid_for(size_t(U), 256, 32 * sms), 256, hbytes,
                         s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, ucnt,
                              nullptr, nullptr, nullptr, umask, nullptr, 0u,
                              ASCI_BINS, 0u, 0u, dhist, AlphaLists{},
@@ -1646,8 +1667,12 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     cap = std::min<int64_t>(std::max<int64_t>(cap, int64_t(1) << 20),
                             int64_t(1) << 31);
   }
-  // records per sort group of a range (MACIS_B200_ASCI_SORT_GROUP)
-  uint64_t sort_group_cap = uint64_t(4) << 28;
+  // records per sort group of a range (MACIS_B200_ASCI_SORT_GROUP). Only
+  // determinant keys are grouped by default: with ranked keys (16-byte
+  // records) a range sorted whole was measured as fast as or faster than
+  // any grouping (n = 48: 1e4 core dets 246 against 276 ms, 1e5 core dets
+  // 3.48 s against 3.35-5.9 s for groups of 5e8-1.07e9 records)
+  uint64_t sort_group_cap = ranked ? ~uint64_t(0) : uint64_t(4) << 28;
   if(const char* e = getenv("MACIS_B200_ASCI_SORT_GROUP"))
     sort_group_cap = std::max<uint64_t>(1, uint64_t(atoll(e)));
   // ranges: consecutive alpha-string bins packed up to the cap from the
@@ -1882,7 +1907,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
                                 s>>>(I, cd, E0, st.h_el_tol, umask, rlo[rr],
                                      rhi[rr], rc), note_launch();
       } else {
-        units_k<NBITS, 0><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0,
+        units_k<NBITS, 0><<<grid_for(size_t(U), 256, 32 * sms), 256, 0,
                             s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,
                                  nullptr, nullptr, nullptr, umask, nullptr,
                                  rlo[rr], rhi[rr], rns[rr], rsub[rr], nullptr,
@@ -1901,13 +1926,13 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
         alr.g = rgrp[rr];
       }
       if(ranked)
-        units_k<NBITS, 2><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0,
+        units_k<NBITS, 2><<<grid_for(size_t(U), 256, 32 * sms), 256, 0,
                             s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,
                                  off, keys, rv, umask, umax, rlo[rr], rhi[rr],
                                  rns[rr], rsub[rr], nullptr, alr, rt),
             note_launch();
       else
-        units_k<NBITS, 1><<<grid_for(size_t(U) * 32, 256, 32 * sms), 256, 0,
+        units_k<NBITS, 1><<<grid_for(size_t(U), 256, 32 * sms), 256, 0,
                             s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,
                                  off, keys, rv, umask, umax, rlo[rr], rhi[rr],
                                  rns[rr], rsub[rr], nullptr, alr,
