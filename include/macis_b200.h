@@ -67,7 +67,9 @@ typedef struct {
 typedef struct {
   uint64_t raw_pairs;     /* contributions generated (after h_el_tol) */
   uint64_t unique_pairs;  /* after sort + accumulate */
-  uint64_t kept_pairs;    /* after dropping core dets and zero scores */
+  uint64_t kept_pairs;    /* after dropping core dets, zero scores and, in
+                             ranges after the running top-k first filled,
+                             scores below its k-th score */
   uint64_t batches;       /* core-det batches used */
   double pairs_ms, sort_ms, keep_ms, topk_ms, total_ms;
   uint64_t units_total;   /* work units of the search (see asci_screen) */

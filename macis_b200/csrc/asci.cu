@@ -1141,11 +1141,20 @@ __global__ void seg_sum_k(const int64_t* start, size_t nseg, size_t n,
 }
 
 // --------------------------------------------------------- core / top-k
+// Candidates of a range that may enter the top-k: nonzero scores whose
+// |rv| bits are at least tcut (the running k-th score so far: the final
+// threshold is never lower, and ties stay), and not core dets.
 template <int NW>
 __global__ void keep_flags_k(const uint64_t* keys, const double* rv, size_t n,
-                             const uint64_t* core, size_t nc, uint32_t* f) {
+                             const uint64_t* core, size_t nc, uint64_t tcut,
+                             uint32_t* f) {
   for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
       i += size_t(gridDim.x) * blockDim.x) {
+    const double a = fabs(rv[i]);
+    if(!(-a < 0.0) || uint64_t(__double_as_longlong(a)) < tcut) {
+      f[i] = 0u;
+      continue;
+    }
     const Key<NW> k = load_key<NW>(keys, i);
     size_t lo = 0, hi = nc;
     bool found = false;
@@ -1161,7 +1170,7 @@ __global__ void keep_flags_k(const uint64_t* keys, const double* rv, size_t n,
       else
         hi = mid;
     }
-    f[i] = (!found && (-fabs(rv[i]) < 0.0)) ? 1u : 0u;
+    f[i] = found ? 0u : 1u;
   }
 }
 template <int NW>
@@ -1884,6 +1893,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   };
 
   Pairs surv;  // running top-k candidates (ties at the threshold included)
+  uint64_t tcut = 0;  // |rv| bits of its k-th score once it holds k
   uint64_t uniq_total = 0, kept_total = 0;
   double sort_ms = 0, pair_ms = 0, keep_ms = 0;
   for(uint32_t rr = 0; rr < nr; ++rr) {
@@ -2064,7 +2074,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     if(uq.n) {
       uint32_t* f = B.get<uint32_t>(uq.n + 1);
       keep_flags_k<NW><<<grid_for(uq.n, 256, 16 * sms), 256, 0, s>>>(
-          uq.keys, uq.rv, uq.n, core, ncdets, f), note_launch();
+          uq.keys, uq.rv, uq.n, core, ncdets, tcut, f), note_launch();
       kept = compact_to(B, uq.keys, uq.rv, uq.n, f);
     }
     kept_total += kept.n;
@@ -2097,6 +2107,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     if(cat.n > topk) {
       uint64_t need = 0;
       const uint64_t T = kth_bits(cat.rv, cat.n, topk, &need);
+      tcut = T;
       uint32_t* f = B.get<uint32_t>(cat.n + 1);
       ge_flags_k<<<grid_for(cat.n, 256, 16 * sms), 256, 0, s>>>(
           cat.rv, cat.n, T, f), note_launch();
