@@ -637,7 +637,7 @@ def asci_rooflines(st, nbits, peak):
 
 def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
                    cpu_ncore=50, cpu_ndets=20000, problem=None, nbits=128,
-                   net=None, warm=True):
+                   net=None, warm=True, keep_frac=0.2):
     """One C3-shaped ASCI iteration (asci_iter, iteration.hpp:17-68) both
     ways on n = 48, 12 alpha / 12 beta, bitset<128>: `ncore` core
     determinants -> `ndets` determinants -> rediagonalisation.
@@ -692,8 +692,8 @@ def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
         rec = mb.ScreenSettings(network=net, max_samples=1000000)
         mb.asci_search(s, ndets // 4, core[:nprev], E0, C[:nprev], n, H,
                        screen=rec)
-    sc = mb.ScreenSettings(network=net, keep_frac=0.2, explore_frac=0.02,
-                           train=False, seed=seed)
+    sc = mb.ScreenSettings(network=net, keep_frac=keep_frac,
+                           explore_frac=0.02, train=False, seed=seed)
     mb.asci_search(s, 1000, core[:200], E0, C[:200], n, H, screen=sc,
                    use_net=True)                  # loads the network kernels
     t0 = time.perf_counter()
@@ -733,6 +733,7 @@ def asci_iteration(mb, peak, ncore=100000, ndets=1000000, seed=0,
                                     ("pairs_ms", "sort_ms", "keep_ms")}},
         "learned_mixed": {"seconds": t_learned, "train_s": t_train,
                           "train_loss": loss, "search_s": t_sl,
+                          "keep_frac": keep_frac,
                           "h_build_s": tl["h_ms"] / 1e3,
                           "davidson_s": tl["dav_ms"] / 1e3,
                           "davidson_iterations": tl["niter"], "E": E_l,

@@ -307,7 +307,10 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
         diag_ms=(t2 - t1b) * 1e3, screened=bool(use_net),
         units_total=st["units_total"], units_kept=st["units_kept"],
         raw_pairs=st["raw_pairs"], recall_check=recall,
-        keep_frac=None if screen is None else screen.keep_frac, **tim))
+        keep_frac=None if screen is None else screen.keep_frac,
+        ranges=st["batches"], alpha_strings=st["alpha_strings"],
+        key_bits=st["key_bits"], pairs_ms=st["pairs_ms"],
+        sort_ms=st["sort_ms"], **tim))
     return E, wfn, X
 
 

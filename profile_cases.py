@@ -160,7 +160,7 @@ def asci_iter_n48(ncore=100000, ndets=1000000):
 
 
 def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128,
-       compare=False):
+       compare=False, save=None):
     """One C3-shaped ASCI run (C4 with n = 64, k = 16); prints one JSON line
     with the per-iteration log, the final energy and the wall time."""
     import json
@@ -189,6 +189,10 @@ def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128,
     dt = time.perf_counter() - t0
     recall = None
     cmp = None
+    if save:  # the final core set (search input of a next iteration)
+        core, C = mb.reorder_ci_on_coeff(dets, np.asarray(X))
+        nc = min(int(ncore), len(core))
+        np.savez(save, dets=core[:nc], C=C[:nc], E=E, n=n, k=k, nbits=nbits)
     if scr is not None and compare:
         # one more iteration from the final wavefunction both ways: exact
         # search + FP64 solve against the trained network's screened search
@@ -199,7 +203,8 @@ def c3(ntdets, mode, refine=3, ncore=100000, seed=0, n=48, k=12, nbits=128,
         cmp = bench.asci_iteration(mb, bench.peaks()[0],
                                    problem=(n, H, core[:nc], C[:nc], E),
                                    ndets=len(dets), nbits=nbits,
-                                   net=scr.network, warm=False)
+                                   net=scr.network, warm=False,
+                                   keep_frac=scr.keep_frac)
     elif scr is not None:
         # top-k recall of the screened search against the exact one, from
         # the same core set (the last iteration's wavefunction)
@@ -258,6 +263,8 @@ def main():
     ap.add_argument("--ncore", type=int, default=10000)
     ap.add_argument("--refine", type=int, default=3)
     ap.add_argument("--compare", action="store_true")
+    ap.add_argument("--save", default=None,
+                    help="c3/c4/c5: write the final core set to this .npz")
     a = ap.parse_args()
     if a.case == "hbuild_c1":
         hbuild(10, 5, a.reps)
@@ -289,14 +296,15 @@ def main():
         # --ncore: core determinants per search (default 1e5 for these)
         nc = a.ncore if a.ncore != 10000 else 100000
         if a.case == "c3":
-            c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, compare=a.compare)
+            c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, compare=a.compare,
+               save=a.save)
         elif a.case == "c4":
             c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, n=64, k=16,
-               compare=a.compare)
+               compare=a.compare, save=a.save)
         else:
             # n = 100, 20a/20b, bitset<256> (network input 320 columns)
             c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, n=100, k=20,
-               nbits=256, compare=a.compare)
+               nbits=256, compare=a.compare, save=a.save)
     else:
         raise SystemExit(f"unknown case {a.case}")
 
