@@ -7,8 +7,7 @@
 // uint64 words stored item-contiguous; word NW-1 is the most significant
 // (the bitset_less order, bitset_operations.hpp:289-306). Only 8-bit digits
 // in which some key differs from the first key are sorted, so a 24-orbital
-// string costs 3 passes whatever its word width; one-word keys take 9-bit
-// digits from their lowest varying bit when that saves a pass. Within a tile each warp
+// string costs 3 passes whatever its word width. Within a tile each warp
 // ranks its items with __match_any_sync, which keeps the sort stable: equal
 // keys leave in input order, which fixes the accumulation order of duplicate
 // ASCI contributions.
@@ -292,25 +291,21 @@ struct ShiftDigit {  // the byte of the key at bit `shift`
   }
 };
 
-// NB buckets (256, or 512 for 9-bit digits): thread t owns digits
-// t * NB / 256 .. (t + 1) * NB / 256 - 1 in the per-digit steps.
-template <int NW, typename P, class Digit, class Resolve, int NB = 256>
+template <int NW, typename P, class Digit, class Resolve>
 __device__ __forceinline__ void rs_tile_pass(const uint64_t* keys,
                                              const P* vals, size_t n,
                                              Digit digit, size_t tile0,
                                              uint64_t* keys_out, P* vals_out,
                                              Resolve resolve) {
-  static_assert(NB % RS_THREADS == 0, "buckets: a multiple of the threads");
-  constexpr int DPT = NB / RS_THREADS;
   extern __shared__ __align__(16) uint8_t rs_smem[];
   uint64_t* skeys = reinterpret_cast<uint64_t*>(rs_smem);
   P* svals = reinterpret_cast<P*>(skeys + size_t(RS_TILE) * NW);
-  __shared__ uint32_t wcount[RS_WARPS][NB];
-  __shared__ uint32_t bstart[NB];
-  __shared__ uint64_t boff[NB];
+  __shared__ uint32_t wcount[RS_WARPS][256];
+  __shared__ uint32_t bstart[256];
+  __shared__ uint64_t boff[256];
   __shared__ uint32_t scan_sh[RS_WARPS + 1];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for(int d = threadIdx.x; d < RS_WARPS * NB; d += RS_THREADS)
+  for(int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS)
     (&wcount[0][0])[d] = 0;
   __syncthreads();
   const size_t wbase = tile0 + size_t(wid) * RS_WARP_ITEMS;
@@ -320,11 +315,11 @@ __device__ __forceinline__ void rs_tile_pass(const uint64_t* keys,
 #pragma unroll
   for(int r = 0; r < RS_IPT; ++r) {
     const size_t i = wbase + size_t(r) * 32 + lane;
-    dig[r] = i < n ? digit(load_key<NW>(keys, i)) : unsigned(NB);
+    dig[r] = i < n ? digit(load_key<NW>(keys, i)) : 256u;
   }
 #pragma unroll
   for(int r = 0; r < RS_IPT; ++r) {
-    const bool ok = dig[r] < unsigned(NB);
+    const bool ok = dig[r] < 256u;
     const unsigned peers = __match_any_sync(0xffffffffu, dig[r]);
     const unsigned before = __popc(peers & lanemask_lt());
     const int leader = __ffs(peers) - 1;
@@ -339,34 +334,21 @@ __device__ __forceinline__ void rs_tile_pass(const uint64_t* keys,
   {
     // per digit: exclusive prefix over warps, then over digits (bucket
     // starts inside the tile), and the digit's output position
-    uint32_t cnt[DPT];
-    uint32_t tsum = 0;
+    const int d = threadIdx.x;
+    uint32_t acc = 0;
 #pragma unroll
-    for(int j = 0; j < DPT; ++j) {
-      const int d = threadIdx.x * DPT + j;
-      uint32_t acc = 0;
-#pragma unroll
-      for(int w = 0; w < RS_WARPS; ++w) {
-        const uint32_t c = wcount[w][d];
-        wcount[w][d] = acc;
-        acc += c;
-      }
-      cnt[j] = acc;
-      tsum += acc;
+    for(int w = 0; w < RS_WARPS; ++w) {
+      const uint32_t c = wcount[w][d];
+      wcount[w][d] = acc;
+      acc += c;
     }
-    uint32_t run = block_excl_scan<uint32_t>(tsum, scan_sh, nullptr);
-#pragma unroll
-    for(int j = 0; j < DPT; ++j) {
-      const int d = threadIdx.x * DPT + j;
-      bstart[d] = run;
-      run += cnt[j];
-      boff[d] = resolve(d, cnt[j]);
-    }
+    bstart[d] = block_excl_scan<uint32_t>(acc, scan_sh, nullptr);
+    boff[d] = resolve(d, acc);
   }
   __syncthreads();
 #pragma unroll
   for(int r = 0; r < RS_IPT; ++r) {
-    if(dig[r] < unsigned(NB)) {
+    if(dig[r] < 256u) {
       const size_t i = wbase + size_t(r) * 32 + lane;
       const uint32_t pos = bstart[dig[r]] + wcount[wid][dig[r]] + rank[r];
       store_key<NW>(skeys, pos, load_key<NW>(keys, i));
@@ -396,51 +378,6 @@ __global__ void __launch_bounds__(RS_THREADS, 4)
   rs_tile_pass<NW, P>(keys, vals, n, ShiftDigit<NW>{shift},
                       size_t(blockIdx.x) * RS_TILE, keys_out, vals_out,
                       [&](int, uint32_t) { return my_off; });
-}
-
-// 9-bit digits of one-word keys: 512 buckets, so that keys of 41-45
-// varying bits take 5 passes instead of 6 (ranked ASCI keys).
-constexpr int RS_WIDE_BITS = 9;
-constexpr int RS_WIDE_NB = 1 << RS_WIDE_BITS;
-struct WideDigit {
-  int shift;
-  __device__ __forceinline__ unsigned operator()(const Key<1>& k) const {
-    return unsigned(k.w[0] >> shift) & unsigned(RS_WIDE_NB - 1);
-  }
-};
-static __global__ void __launch_bounds__(RS_THREADS)
-    radix_hist_wide_k(const uint64_t* keys, size_t n, int shift,
-                      uint32_t* counts, unsigned nblocks) {
-  __shared__ uint32_t h[RS_WIDE_NB];
-  for(int d = threadIdx.x; d < RS_WIDE_NB; d += RS_THREADS) h[d] = 0;
-  __syncthreads();
-  const size_t base = size_t(blockIdx.x) * RS_TILE;
-  const WideDigit dg{shift};
-#pragma unroll 4
-  for(int r = 0; r < RS_IPT; ++r) {
-    size_t i = base + size_t(r) * RS_THREADS + threadIdx.x;
-    if(i < n) atomicAdd(&h[dg(load_key<1>(keys, i))], 1u);
-  }
-  __syncthreads();
-  for(int d = threadIdx.x; d < RS_WIDE_NB; d += RS_THREADS)
-    counts[size_t(d) * nblocks + blockIdx.x] = h[d];
-}
-template <typename P>
-__global__ void __launch_bounds__(RS_THREADS, 4)
-    radix_scatter_wide_k(const uint64_t* keys, const P* vals, size_t n,
-                         int shift, const uint64_t* offsets, unsigned nblocks,
-                         uint64_t* keys_out, P* vals_out) {
-  constexpr int DPT = RS_WIDE_NB / RS_THREADS;
-  // issued before the ranking: their latency hides behind the tile loads
-  uint64_t my_off[DPT];
-#pragma unroll
-  for(int j = 0; j < DPT; ++j)
-    my_off[j] = offsets[size_t(threadIdx.x * DPT + j) * nblocks + blockIdx.x];
-  static_assert(DPT == 2, "two digits per thread");
-  auto res = [&](int d, uint32_t) { return (d & 1) ? my_off[1] : my_off[0]; };
-  rs_tile_pass<1, P, WideDigit, decltype(res), RS_WIDE_NB>(
-      keys, vals, n, WideDigit{shift}, size_t(blockIdx.x) * RS_TILE, keys_out,
-      vals_out, res);
 }
 
 // ------------------------------------------------------ one-sweep passes
@@ -557,18 +494,6 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
     for(int sft = 0; sft < 64; sft += 8)
       if((vary[w] >> sft) & 255ull) shifts.push_back(64 * w + sft);
   const int np = int(shifts.size());
-  // one-word keys: 9-bit digits from the lowest varying bit when they need
-  // fewer passes than the 8-bit digits (MACIS_B200_SORT_WIDE=0: never)
-  std::vector<int> wide;
-  if constexpr(NW == 1) {
-    const char* we = getenv("MACIS_B200_SORT_WIDE");
-    if(vary[0] && !(we && we[0] == '0')) {
-      const int lo = __builtin_ctzll(vary[0]);
-      const int hi = 64 - __builtin_clzll(vary[0]);
-      for(int sft = lo; sft < hi; sft += RS_WIDE_BITS) wide.push_back(sft);
-      if(wide.size() >= shifts.size()) wide.clear();
-    }
-  }
   uint64_t *kin = keys, *kout = keys_alt;
   P *vin = vals, *vout = vals_alt;
   uint32_t* counts = nullptr;
@@ -592,27 +517,8 @@ int radix_sort(uint64_t* keys, P* vals, uint64_t* keys_alt, P* vals_alt,
   // against 0.67-0.69 s) and steadier
   const char* opt = getenv("MACIS_B200_SORT_ONESWEEP");
   const bool onesweep = n >= RS_ONESWEEP_MIN && np <= RS_MAX_PASSES &&
-                        opt && opt[0] == '1' && wide.empty();
-  if(!wide.empty()) {
-    constexpr size_t wstage = rs_stage_bytes<1, P>();
-    MB_CUDA(cudaFuncSetAttribute(radix_scatter_wide_k<P>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(wstage)));
-    uint32_t* wcounts = A.get<uint32_t>(size_t(RS_WIDE_NB) * nblocks);
-    uint64_t* woffs = A.get<uint64_t>(size_t(RS_WIDE_NB) * nblocks);
-    for(const int sft : wide) {
-      radix_hist_wide_k<<<nblocks, RS_THREADS, 0, A.s>>>(kin, n, sft, wcounts,
-                                                         nblocks), note_launch();
-      exclusive_scan<uint32_t, uint64_t>(wcounts, woffs,
-                                         size_t(RS_WIDE_NB) * nblocks, nullptr,
-                                         A);
-      radix_scatter_wide_k<P><<<nblocks, RS_THREADS, wstage, A.s>>>(
-          kin, vin, n, sft, woffs, nblocks, kout, vout), note_launch();
-      std::swap(kin, kout);
-      std::swap(vin, vout);
-      ++passes;
-    }
-  } else if(onesweep) {
+                        opt && opt[0] == '1';
+  if(onesweep) {
     // all digit histograms in one read, bucket starts per pass on the host
     MB_CUDA(cudaFuncSetAttribute(rs_onesweep_k<NW, P, ShiftDigit<NW>>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,

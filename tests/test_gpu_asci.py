@@ -244,16 +244,14 @@ def test_screened_split_search_matches_whole(wcase):
 
 
 def test_onesweep_sort_matches_classic_passes(monkeypatch):
-    """The candidate sort with one-sweep 8-bit digit passes (decoupled
-    look-back, MACIS_B200_SORT_ONESWEEP=1, MACIS_B200_SORT_WIDE=0) against
-    the classic histogram / scan / scatter passes over 9-bit digits (the
-    default for the ranked keys), and with candidate ranges split by bin
+    """The candidate sort with one-sweep digit passes (decoupled look-back,
+    MACIS_B200_SORT_ONESWEEP=1) against the classic histogram / scan /
+    scatter passes (the default), and with candidate ranges split by bin
     into separately sorted groups: identical accumulated candidates and
     scores, and identical selections, on an n = 48 bitset<128> core set of
     300 determinants (about 8e7 contributions)."""
     from cases import core_set
     monkeypatch.setenv("MACIS_B200_SORT_ONESWEEP", "1")
-    monkeypatch.setenv("MACIS_B200_SORT_WIDE", "0")  # 8-bit one-sweep passes
     n, k = 48, 12
     T, V = mb.synthetic_integrals(n, 0)
     cd, C = core_set(n, k, 300, 128, nalpha=80, top=40)
@@ -272,7 +270,6 @@ def test_onesweep_sort_matches_classic_passes(monkeypatch):
     monkeypatch.delenv("MACIS_B200_ASCI_SORT_GROUP")
     monkeypatch.delenv("MACIS_B200_ASCI_BATCH_PAIRS")
     monkeypatch.delenv("MACIS_B200_SORT_ONESWEEP")
-    monkeypatch.delenv("MACIS_B200_SORT_WIDE")  # 9-bit classic passes
     s0, r0 = mb.asci_pairs(_settings(), cd, E0, C, H)
     sel0 = mb.asci_search(_settings(), 50000, cd, E0, C, n, H)
     assert np.array_equal(s1, s0) and np.array_equal(r1, r0)
