@@ -209,24 +209,24 @@ struct BinGroup {
 // Alpha lists of a partitioned search. The bins of the contributions of an
 // alpha same-spin double unit (kind 2) depend only on the core det's alpha
 // string, and so does their threshold test (|G| against the tolerance):
-// for every distinct alpha string u, one byte per alpha double holds the
-// group (unsplit candidate range) its bin falls into, or 255 when the
-// double fails the threshold or its bin belongs to no unsplit range. The
-// doubles of u are laid out as in unit_run (row k = ii * nvA + aa from
-// double_row_base, then the inner index q), ND = C(nA,2) C(nvA,2) bytes per
-// alpha string. A range's passes then compare one byte per alpha double
-// with the range's group instead of hashing the excited alpha string. The
-// bins of the units with a fixed alpha string (kinds 1, 3, 4) are tabulated
-// per alpha string too. Used for the ranges that are not split by beta
-// string (group g >= 0).
+// for every distinct alpha string u and outer pair k = ii * nvA + aa, the
+// inner indices q of the kept contributions are listed once per search,
+// grouped by the candidate range their bin falls into (ascending q inside a
+// group). A range's count pass then reads each unit's count from the lists
+// instead of evaluating the bins of all its contributions, and its fill
+// pass generates the listed contributions only. The bins of the units with
+// a fixed alpha string (kinds 1, 3, 4) are tabulated per alpha string too.
+// Used for the ranges that are not split by beta string (group g >= 0).
 struct AlphaLists {
   const int32_t* aidx = nullptr;  // per core det: its alpha string
   int NK = 0;                     // nA * nvA outer pairs per alpha string
-  int64_t ND = 0;                 // alpha doubles per alpha string
+  int G = 0;                      // groups: the unsplit ranges
   const uint16_t* abin = nullptr;  // per alpha string: its bin
   const uint16_t* kbin = nullptr;  // per (u, k): bin after the outer alpha
                                    // excitation (opposite-spin units)
-  const uint8_t* grp = nullptr;    // per (u, double): group, 255 none
+  const int64_t* base = nullptr;   // per (u, k): first list entry
+  const uint16_t* rel = nullptr;   // per (u, k): G + 1 group starts
+  const uint16_t* q = nullptr;     // inner indices, by group
   int g = -1;                      // group of the range, -1: not used
 };
 
@@ -497,12 +497,15 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
       rshift = ba;
     }
   }
-  const int64_t nloop = ninner;
-  // alpha lists: the range's group byte of each alpha double of this unit
-  const uint8_t* qgrp = nullptr;
-  if(listed && kind == 2)
-    qgrp = al.grp + size_t(al.aidx[c]) * size_t(al.ND) +
-           size_t(double_row_base(ii, aa, nA, nvA));
+  int64_t nloop = ninner;
+  const uint16_t* qlist = nullptr;
+  if(listed && kind == 2) {
+    const size_t row = size_t(al.aidx[c]) * al.NK + size_t(ii) * nvA + aa;
+    const uint16_t* rr = al.rel + row * (al.G + 1);
+    const int e0 = rr[al.g];
+    qlist = al.q + al.base[row] + e0;
+    nloop = int64_t(rr[al.g + 1]) - e0;
+  }
   for(int64_t q0 = 0; q0 < nloop; q0 += 32) {
     const int64_t qi = q0 + lane;
     bool keep = false;
@@ -510,7 +513,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
     uint64_t ex[D::NW];
     uint64_t rkey = 0;
     if(qi < nloop) {
-      const int64_t q = qi;
+      const int64_t q = qlist ? int64_t(qlist[qi]) : qi;
       if(kind <= 1) {
         // append_singles_asci_contributions (determinant_contributions.hpp:25-66)
         const int S = kind;
@@ -566,7 +569,6 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
           cbin = alpha_bin<NSW>(
               sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b));
         bool inr = !chk || (cbin >= blo && cbin < bhi);
-        if(qgrp) inr = qgrp[q] == unsigned(al.g);
         if(chkb)  // S == 1
           inr = beta_sub<NSW>(
                     sp_flip(sp_flip(sp_flip(sp_flip(sB, i), j), a), b), nsub) ==
@@ -718,25 +720,28 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Alpha lists: one warp per (alpha string u, outer pair k) row writes the
-// group byte of each alpha double of the row (AlphaLists) -- the threshold
-// test of unit_run (kind 2) and grp[] of the double's bin (255: a split
-// range or outside this search's bins) -- and the opposite-spin outer bin
-// of the row.
+// Alpha lists, count pass: one warp per (alpha string u, outer pair k) row.
+// Writes the row's group starts (prefix of the per-group counts, G + 1
+// entries) and the opposite-spin outer bin of the row; grp maps a bin to
+// its group (255: a split range or outside this search's bins). The lists
+// keep the inner indices whose integral passes the threshold test of
+// unit_run (kind 2) and whose bin has a group.
 template <int NBITS>
 __global__ void __launch_bounds__(256)
-    alpha_groups_k(Ints I, CoreData cd, const int32_t* rep, size_t nua,
-                   int nA, int nvA, double tol, const uint8_t* grp,
-                   AlphaLists al, uint8_t* qgrp, uint16_t* kbin,
-                   uint16_t* abin) {
+    alpha_count_k(Ints I, CoreData cd, const int32_t* rep, size_t nua, int nA,
+                  int nvA, double tol, const uint8_t* grp, AlphaLists al,
+                  uint16_t* rel, uint16_t* kbin, uint16_t* abin,
+                  int64_t* tot) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
-  const int lane = threadIdx.x & 31;
+  extern __shared__ int gcnt[];  // per warp: G counters
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int* cnt = gcnt + wib * (al.G + 1);
   const int n = cd.n;
   const size_t rows = nua * size_t(al.NK);
   const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
-  for(size_t row = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      row < rows; row += nwarp) {
+  for(size_t row = size_t(blockIdx.x) * (blockDim.x >> 5) + wib; row < rows;
+      row += nwarp) {
     const size_t u = row / al.NK;
     const int k = int(row - u * al.NK);
     const int ii = k / nvA, aa = k - ii * nvA;
@@ -744,6 +749,8 @@ __global__ void __launch_bounds__(256)
     const uint8_t* occA = cd.occ + (c * 2) * MAXORB;
     const uint8_t* virA = cd.vir + (c * 2) * MAXORB;
     const Spin<NSW> sA = D::alpha(cd.dets + c * D::NW);
+    for(int g = lane; g < al.G; g += 32) cnt[g] = 0;
+    __syncwarp();
     const int i = occA[ii], a = virA[aa];
     if(lane == 0) {
       kbin[row] = uint16_t(alpha_bin<NSW>(sp_flip(sp_flip(sA, i), a)));
@@ -751,56 +758,93 @@ __global__ void __launch_bounds__(256)
     }
     const int span = nvA - 1 - aa;
     const int64_t ninner = int64_t(nA - 1 - ii) * span;
-    uint8_t* out = qgrp + u * size_t(al.ND) + size_t(double_row_base(ii, aa, nA, nvA));
     for(int64_t q = lane; q < ninner; q += 32) {
       const int qd = small_div(q, 1.0f / float(span));
       const int j = occA[ii + 1 + qd], b = virA[aa + 1 + (int(q) - qd * span)];
       const double Gv =
           __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
-      uint8_t gq = 255;
-      if(!(fabs(Gv) < tol))
-        gq = grp[alpha_bin<NSW>(
+      if(!(fabs(Gv) < tol)) {
+        const uint8_t g = grp[alpha_bin<NSW>(
             sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b))];
-      out[q] = gq;
+        if(g != 255) atomicAdd(cnt + g, 1);
+      }
     }
+    __syncwarp();
+    if(lane == 0) {
+      int acc = 0;
+      uint16_t* rr = rel + row * (al.G + 1);
+      for(int g = 0; g < al.G; ++g) {
+        rr[g] = uint16_t(acc);
+        acc += cnt[g];
+      }
+      rr[al.G] = uint16_t(acc);
+      tot[row] = acc;
+    }
+    __syncwarp();
   }
 }
 
-// Alpha-double units (kind 2) of a range with alpha lists: one warp per
-// (core det, outer pair) counts the unit's bytes equal to the range's group.
+// Alpha lists, fill pass: the same rows, inner indices written at their
+// group's position in ascending q (lanes with equal groups ranked by
+// __match_any_sync).
+template <int NBITS>
 __global__ void __launch_bounds__(256)
-    units2_count_k(CoreData cd, AlphaLists al, const uint8_t* umask,
-                   int64_t* rc) {
-  const int lane = threadIdx.x & 31;
-  const size_t pairs = cd.ncdets * size_t(al.NK);
+    alpha_fill_k(Ints I, CoreData cd, const int32_t* rep, size_t nua, int nA,
+                 int nvA, double tol, const uint8_t* grp, AlphaLists al,
+                 uint16_t* qout) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  extern __shared__ int gcnt[];  // per warp: running position per group
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int* run = gcnt + wib * (al.G + 1);
+  const int n = cd.n;
+  const size_t rows = nua * size_t(al.NK);
   const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
-  for(size_t w = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      w < pairs; w += nwarp) {
-    const size_t c = w / size_t(al.NK);
-    const int k = int(w - c * size_t(al.NK));
-    const int nA = cd.cnt[c * 4], nvA = cd.cnt[c * 4 + 2];
+  for(size_t row = size_t(blockIdx.x) * (blockDim.x >> 5) + wib; row < rows;
+      row += nwarp) {
+    const size_t u = row / al.NK;
+    const int k = int(row - u * al.NK);
     const int ii = k / nvA, aa = k - ii * nvA;
-    const int64_t u = cd.uoff[c] + 2 + k;
-    int64_t cnt = 0;
-    if(!umask || umask[u]) {
-      const int64_t ninner = int64_t(nA - 1 - ii) * (nvA - 1 - aa);
-      const uint8_t* row = al.grp + size_t(al.aidx[c]) * size_t(al.ND) +
-                           size_t(double_row_base(ii, aa, nA, nvA));
-      for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
-        const int64_t q = q0 + lane;
-        cnt += __popc(__ballot_sync(
-            0xffffffffu, q < ninner && row[q] == unsigned(al.g)));
+    const size_t c = size_t(rep[u]);
+    const uint8_t* occA = cd.occ + (c * 2) * MAXORB;
+    const uint8_t* virA = cd.vir + (c * 2) * MAXORB;
+    const Spin<NSW> sA = D::alpha(cd.dets + c * D::NW);
+    const uint16_t* rr = al.rel + row * (al.G + 1);
+    for(int g = lane; g < al.G; g += 32) run[g] = rr[g];
+    __syncwarp();
+    uint16_t* out = qout + al.base[row];
+    const int i = occA[ii], a = virA[aa];
+    const int span = nvA - 1 - aa;
+    const int64_t ninner = int64_t(nA - 1 - ii) * span;
+    for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
+      const int64_t q = q0 + lane;
+      unsigned g = 255;
+      if(q < ninner) {
+        const int qd = small_div(q, 1.0f / float(span));
+        const int j = occA[ii + 1 + qd],
+                  b = virA[aa + 1 + (int(q) - qd * span)];
+        const double Gv =
+            __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
+        if(!(fabs(Gv) < tol))
+          g = grp[alpha_bin<NSW>(
+              sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b))];
       }
+      const unsigned peers = __match_any_sync(0xffffffffu, g);
+      if(g != 255) {
+        out[run[g] + __popc(peers & lanemask_lt())] = uint16_t(q);
+      }
+      __syncwarp();
+      if(g != 255 && (peers & lanemask_lt()) == 0) run[g] += __popc(peers);
+      __syncwarp();
     }
-    if(lane == 0) rc[u] = cnt;
   }
 }
 
 // Count pass of an unsplit range with alpha lists: one thread per unit.
 // Fixed-alpha units (kinds 1, 3, 4) are in the range as a whole, with the
-// count of the whole-search pass (ucnt). Alpha doubles (kind 2) are counted
-// by units2_count_k, alpha singles (kind 0, whose threshold test depends on
-// the beta string) by units0_count_k.
+// count of the whole-search pass (ucnt); alpha doubles (kind 2) read their
+// group's list length. Alpha singles (kind 0, whose threshold test depends
+// on the beta string) are counted by units0_count_k.
 __global__ void range_count_k(CoreData cd, AlphaLists al, int64_t U,
                               const int64_t* ucnt, const uint8_t* umask,
                               uint32_t blo, uint32_t bhi, int64_t* rc) {
@@ -816,7 +860,8 @@ __global__ void range_count_k(CoreData cd, AlphaLists al, int64_t U,
       const size_t ua = size_t(al.aidx[c]);
       uint32_t bin = ASCI_BINS;
       if(t < 2 + KA && t >= 2) {
-        continue;  // units2_count_k
+        const uint16_t* rr = al.rel + (ua * al.NK + size_t(t - 2)) * (al.G + 1);
+        r = int64_t(rr[al.g + 1]) - rr[al.g];
       } else if(t == 1 || t < 2 + KA + KB) {
         bin = al.abin[ua];
       } else {
@@ -1685,17 +1730,20 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
   // alpha lists (AlphaLists) when the ranges need count passes of their own:
   // memory for them, at most 15 % of what is free, comes off the range size
   SpinPlan ap;
+  int g_est = 0;
   const char* al_env = getenv("MACIS_B200_ASCI_ALPHA_LISTS");
   const bool al_allowed = !(al_env && al_env[0] == '0');
   if(al_allowed && !pairs_only && !st.just_singles && bin_lo < bin_hi &&
      ((part && part->count > 1) || Ppart > uint64_t(cap))) {
     ap = alpha_plan();
     if(ap.nu) {
+      g_est = int(std::min<uint64_t>(254, 2 * ((Ppart + cap - 1) / cap) + 2));
       const double nk = double(ap.ne) * ap.nv;
-      const double nd = double(ap.ne) * (ap.ne - 1) / 2 * double(ap.nv) *
-                        (ap.nv - 1) / 2;
-      const double bytes = double(ap.nu) * (nd + 2.0 * nk + 2.0) +
-                           4.0 * double(ncdets + ap.nu) + 8192.0;
+      const double pairs2 = double(ap.ne) * (ap.ne - 1) / 2 * double(ap.nv) *
+                            (ap.nv - 1) / 2;
+      const double bytes =
+          double(ap.nu) * (nk * (18.0 + 2.0 * (g_est + 1)) + 2.0 * pairs2 + 2.0) +
+          4.0 * double(ncdets + ap.nu) + 8192.0;
       if(bytes <= 0.15 * double(device_bytes_available())) {
         if(!cap_env)
           cap = std::max<int64_t>(cap - int64_t(bytes / per_pair), int64_t(1) << 20);
@@ -1742,7 +1790,7 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     int G = 0;
     for(uint32_t r = 0; r < nr; ++r)
       if(rns[r] == 0) rgrp[r] = G++;
-    if(G > 254 || G == 0 || (G < 2 && 2 * ap.nu > ncdets)) {
+    if(G > g_est || G == 0 || (G < 2 && 2 * ap.nu > ncdets)) {
       std::fill(rgrp.begin(), rgrp.end(), -1);
     } else {
       std::vector<uint8_t> gt(ASCI_BINS, 255);
@@ -1759,19 +1807,34 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
                               cudaMemcpyHostToDevice, s));
       al.aidx = aidx;
       al.NK = ap.ne * ap.nv;
-      al.ND = int64_t(ap.ne) * (ap.ne - 1) / 2 * (int64_t(ap.nv) * (ap.nv - 1) / 2);
+      al.G = G;
       const size_t rows = ap.nu * size_t(al.NK);
       uint16_t* abin = A.get<uint16_t>(ap.nu);
       uint16_t* kbin = A.get<uint16_t>(rows + 1);
-      uint8_t* qgrp = A.get<uint8_t>(ap.nu * size_t(al.ND) + 1);
+      uint16_t* rel = A.get<uint16_t>(rows * (G + 1) + 1);
+      int64_t* base = A.get<int64_t>(rows + 1);
       al.abin = abin;
       al.kbin = kbin;
-      al.grp = qgrp;
-      if(rows)
-        alpha_groups_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, 0,
-                                s>>>(I, cd, rep, ap.nu, ap.ne, ap.nv,
-                                     st.h_el_tol, grp, al, qgrp, kbin, abin),
+      al.rel = rel;
+      al.base = base;
+      const size_t smem = 8 * size_t(G + 1) * sizeof(int);
+      if(rows) {
+        int64_t* tot = A.get<int64_t>(rows + 1);
+        alpha_count_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
+                               s>>>(I, cd, rep, ap.nu, ap.ne, ap.nv,
+                                    st.h_el_tol, grp, al, rel, kbin, abin, tot),
             note_launch();
+        MB_CUDA(cudaGetLastError());
+        exclusive_scan<int64_t, int64_t>(tot, base, rows, base + rows, A);
+        A.release(tot);
+      }
+      const int64_t E = rows ? to_host(base + rows, s) : 0;
+      uint16_t* ql = A.get<uint16_t>(size_t(E) + 1);
+      al.q = ql;
+      if(E)
+        alpha_fill_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
+                              s>>>(I, cd, rep, ap.nu, ap.ne, ap.nv,
+                                   st.h_el_tol, grp, al, ql), note_launch();
       MB_CUDA(cudaGetLastError());
       stats.alpha_strings = ap.nu;
     }
@@ -1850,8 +1913,6 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
         alr.g = rgrp[rr];
         range_count_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
             cd, alr, U, ucnt, umask, rlo[rr], rhi[rr], rc), note_launch();
-        units2_count_k<<<grid_for(ncdets * size_t(al.NK) * 32, 256, 16 * sms),
-                         256, 0, s>>>(cd, alr, umask, rc), note_launch();
         units0_count_k<NBITS><<<grid_for(ncdets * 32, 256, 16 * sms), 256, 0,
                                 s>>>(I, cd, E0, st.h_el_tol, umask, rlo[rr],
                                      rhi[rr], rc), note_launch();
