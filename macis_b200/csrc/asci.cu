@@ -1656,14 +1656,19 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       stats.rank_ms = ms_since(t_rk);
     }
   }
+  // bytes of a sorted record, and of a candidate with its determinant
+  // (the unique candidates of a range, the survivors)
   const double rs = ranked ? 16.0 : double(NW * 8 + 8);
-  // per raw contribution while a range is processed: record + sort copy,
-  // flags and radix tables (sort), then the unique list + kept copy + the
-  // running top-k concatenation (few duplicates: unique ~ raw)
-  const double per_pair = 4.0 * rs + 20.0;
+  const double rf = double(NW * 8 + 8);
+  // per raw contribution while a range is processed, whichever phase holds
+  // more: record + sort copy, flags and radix tables (sort); or the unique
+  // candidates as determinants, their flags and kept copy and the running
+  // top-k concatenation (few duplicates: unique ~ raw; 128 B at 256 bits,
+  // more than a ranked-key record's sort)
+  const double per_pair = std::max(4.0 * rs + 20.0, 3.0 * rf + 8.0);
   const size_t topk = ndets_max - ncdets;   // size_t arithmetic (:547)
   const double keep_reserve =
-      6.0 * rs * double(std::min<uint64_t>(topk, uint64_t(Ptot)));
+      6.0 * rf * double(std::min<uint64_t>(topk, uint64_t(Ptot)));
   // MACIS_B200_ASCI_BATCH_PAIRS caps the raw pairs per range (exercises the
   // partitioned path on small problems).
   int64_t cap = 0;
@@ -2082,8 +2087,13 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     // entries tied with it stay)
     Pairs cat;
     cat.n = surv.n + kept.n;
-    cat.keys = A.get<uint64_t>(cat.n * NW + NW);
-    cat.rv = A.get<double>(cat.n + 1);
+    if(surv.n == 0) {  // the first candidates: no copy
+      cat = kept;
+      kept = Pairs{};
+    } else {
+      cat.keys = A.get<uint64_t>(cat.n * NW + NW);
+      cat.rv = A.get<double>(cat.n + 1);
+    }
     if(surv.n) {
       MB_CUDA(cudaMemcpyAsync(cat.keys, surv.keys, surv.n * NW * 8,
                               cudaMemcpyDeviceToDevice, s));

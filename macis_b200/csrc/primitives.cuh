@@ -33,7 +33,16 @@ struct Arena {
     void* p = nullptr;
     size_t bytes = n * sizeof(T);
     if(bytes == 0) bytes = 256;
-    MB_CUDA(dev_malloc_async(&p, (bytes + 255) & ~size_t(255), s));
+    const cudaError_t e = dev_malloc_async(&p, (bytes + 255) & ~size_t(255), s);
+    if(e != cudaSuccess) {
+      size_t fr = 0, tot = 0;
+      cudaMemGetInfo(&fr, &tot);
+      throw Error(e == cudaErrorMemoryAllocation ? MACIS_B200_ENOMEM
+                                                 : MACIS_B200_ECUDA,
+                  "device allocation of " + std::to_string(bytes) +
+                      " bytes failed (" + std::to_string(fr) +
+                      " bytes free on the device): " + cudaGetErrorString(e));
+    }
     ptrs.push_back(p);
     return static_cast<T*>(p);
   }
