@@ -260,7 +260,9 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--ntdets", type=float, default=1e6)
     ap.add_argument("--mode", default="fp64")
-    ap.add_argument("--ncore", type=int, default=10000)
+    ap.add_argument("--ncore", type=int, default=None,
+                    help="core determinants (default 1e4 for the single "
+                         "searches, 1e5 for asci_iter_n48 and c3/c4/c5)")
     ap.add_argument("--refine", type=int, default=3)
     ap.add_argument("--compare", action="store_true")
     ap.add_argument("--save", default=None,
@@ -281,20 +283,21 @@ def main():
     elif a.case == "spmv_c1":
         spmv(10, 5, a.reps)
     elif a.case == "asci_n48":
-        asci_n48(a.reps, ncore=a.ncore)
+        asci_n48(a.reps, ncore=a.ncore or 10000)
     elif a.case == "asci_n100":
-        asci_n48(a.reps, ncore=a.ncore, ndets=20 * a.ncore, n=100, k=20,
+        asci_n48(a.reps, ncore=a.ncore or 10000,
+                 ndets=20 * (a.ncore or 10000), n=100, k=20,
                  nbits=256)
     elif a.case == "mlp_fwd":
         mlp_fwd(a.reps)
     elif a.case == "mlp_train":
         mlp_train(a.reps)
     elif a.case == "asci_iter_n48":
-        asci_iter_n48(a.ncore if a.ncore != 10000 else 100000,
+        asci_iter_n48(a.ncore or 100000,
                       int(a.ntdets))
     elif a.case in ("c3", "c4", "c5"):
         # --ncore: core determinants per search (default 1e5 for these)
-        nc = a.ncore if a.ncore != 10000 else 100000
+        nc = a.ncore or 100000
         if a.case == "c3":
             c3(a.ntdets, a.mode, refine=a.refine, ncore=nc, compare=a.compare,
                save=a.save)
