@@ -209,23 +209,27 @@ struct BinGroup {
 // Alpha lists of a partitioned search. The bins of the contributions of an
 // alpha same-spin double unit (kind 2) depend only on the core det's alpha
 // string, and so does their threshold test (|G| against the tolerance):
-// for every distinct alpha string u and outer pair k = ii * nvA + aa, the
-// inner indices q of the kept contributions are listed once per search,
-// grouped by the candidate range their bin falls into (ascending q inside a
-// group). A range's count pass then reads each unit's count from the lists
-// instead of evaluating the bins of all its contributions, and its fill
-// pass generates the listed contributions only. The bins of the units with
-// a fixed alpha string (kinds 1, 3, 4) are tabulated per alpha string too.
-// Used for the ranges that are not split by beta string (group g >= 0).
+// for a distinct alpha string u and outer pair k = ii * nvA + aa, the inner
+// indices q of the kept contributions are listed once per search, grouped
+// by the candidate range their bin falls into (ascending q inside a group).
+// A range's count pass then reads each unit's count from the lists instead
+// of evaluating the bins of all its contributions, and its fill pass
+// generates the listed contributions only. The lists cover the alpha
+// strings shared by the most core dets, as many as fit the memory budget
+// (lidx >= 0); the alpha doubles of the others keep the per-contribution
+// test. The bins of the units with a fixed alpha string (kinds 1, 3, 4) are
+// tabulated for every distinct alpha string. Used for the ranges that are
+// not split by beta string (group g >= 0).
 struct AlphaLists {
   const int32_t* aidx = nullptr;  // per core det: its alpha string
+  const int32_t* lidx = nullptr;  // per alpha string: its list block, or -1
   int NK = 0;                     // nA * nvA outer pairs per alpha string
   int G = 0;                      // groups: the unsplit ranges
   const uint16_t* abin = nullptr;  // per alpha string: its bin
   const uint16_t* kbin = nullptr;  // per (u, k): bin after the outer alpha
                                    // excitation (opposite-spin units)
-  const int64_t* base = nullptr;   // per (u, k): first list entry
-  const uint16_t* rel = nullptr;   // per (u, k): G + 1 group starts
+  const int64_t* base = nullptr;   // per (list block, k): first list entry
+  const uint16_t* rel = nullptr;   // per (list block, k): G + 1 group starts
   const uint16_t* q = nullptr;     // inner indices, by group
   int g = -1;                      // group of the range, -1: not used
 };
@@ -451,7 +455,9 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
   uint32_t ubin = 0;
   // with alpha lists the caller runs a unit only when it has contributions
   // in the range: no bin test
-  const bool listed = al.g >= 0 && kind != 0;
+  // list block of the unit's alpha string (alpha doubles)
+  const int32_t lb = (al.g >= 0 && kind == 2) ? al.lidx[al.aidx[c]] : -1;
+  const bool listed = al.g >= 0 && kind != 0 && (kind != 2 || lb >= 0);
   if(listed) chk = false;
   if(fixed_alpha && !listed && (part || hist)) {
     Spin<NSW> ua = sA;
@@ -500,7 +506,7 @@ __device__ void unit_run(const Ints& I, const CoreData& cd, size_t c, int64_t t,
   int64_t nloop = ninner;
   const uint16_t* qlist = nullptr;
   if(listed && kind == 2) {
-    const size_t row = size_t(al.aidx[c]) * al.NK + size_t(ii) * nvA + aa;
+    const size_t row = size_t(lb) * al.NK + size_t(ii) * nvA + aa;
     const uint16_t* rr = al.rel + row * (al.G + 1);
     const int e0 = rr[al.g];
     qlist = al.q + al.base[row] + e0;
@@ -702,6 +708,13 @@ __global__ void __launch_bounds__(256)
       own = cd.udet[ul];
       t = ul - cd.uoff[own];
     }
+    if(MODE == 0 && al.g >= 0 && run) {
+      // count pass of a range with alpha lists (list_rest): only the alpha
+      // singles and the alpha doubles of unlisted alpha strings; the others
+      // were counted by range_count_k
+      const int64_t KA = int64_t(cd.cnt[size_t(own) * 4]) * cd.cnt[size_t(own) * 4 + 2];
+      run = t == 0 || (t >= 2 && t < 2 + KA && al.lidx[al.aidx[own]] < 0);
+    }
     for(unsigned m = __ballot_sync(0xffffffffu, run); m; m &= m - 1) {
       const int l = __ffs(m) - 1;
       const int64_t u = ub + l;
@@ -720,18 +733,38 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Alpha lists, count pass: one warp per (alpha string u, outer pair k) row.
+// Alpha lists: the bin of every distinct alpha string and, per outer pair,
+// of the string after the outer alpha excitation (one thread per pair).
+template <int NBITS>
+__global__ void alpha_bins_k(CoreData cd, const int32_t* rep, size_t nua,
+                             int nvA, int NK, uint16_t* kbin, uint16_t* abin) {
+  using D = DetTraits<NBITS>;
+  constexpr int NSW = D::NSW;
+  const size_t rows = nua * size_t(NK);
+  for(size_t row = size_t(blockIdx.x) * blockDim.x + threadIdx.x; row < rows;
+      row += size_t(gridDim.x) * blockDim.x) {
+    const size_t u = row / NK;
+    const int k = int(row - u * NK);
+    const int ii = k / nvA, aa = k - ii * nvA;
+    const size_t c = size_t(rep[u]);
+    const Spin<NSW> sA = D::alpha(cd.dets + c * D::NW);
+    const int i = cd.occ[(c * 2) * MAXORB + ii], a = cd.vir[(c * 2) * MAXORB + aa];
+    kbin[row] = uint16_t(alpha_bin<NSW>(sp_flip(sp_flip(sA, i), a)));
+    if(k == 0) abin[u] = uint16_t(alpha_bin<NSW>(sA));
+  }
+}
+
+// Alpha lists, count pass: one warp per (list block, outer pair k) row.
 // Writes the row's group starts (prefix of the per-group counts, G + 1
-// entries) and the opposite-spin outer bin of the row; grp maps a bin to
-// its group (255: a split range or outside this search's bins). The lists
-// keep the inner indices whose integral passes the threshold test of
-// unit_run (kind 2) and whose bin has a group.
+// entries); grp maps a bin to its group (0xFFFF: a split range or outside
+// this search's bins). The lists keep the inner indices whose integral
+// passes the threshold test of unit_run (kind 2) and whose bin has a group.
+// rep: per list block, a core det with its alpha string.
 template <int NBITS>
 __global__ void __launch_bounds__(256)
     alpha_count_k(Ints I, CoreData cd, const int32_t* rep, size_t nua, int nA,
-                  int nvA, double tol, const uint8_t* grp, AlphaLists al,
-                  uint16_t* rel, uint16_t* kbin, uint16_t* abin,
-                  int64_t* tot) {
+                  int nvA, double tol, const uint16_t* grp, AlphaLists al,
+                  uint16_t* rel, int64_t* tot) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
   extern __shared__ int gcnt[];  // per warp: G counters
@@ -752,10 +785,6 @@ __global__ void __launch_bounds__(256)
     for(int g = lane; g < al.G; g += 32) cnt[g] = 0;
     __syncwarp();
     const int i = occA[ii], a = virA[aa];
-    if(lane == 0) {
-      kbin[row] = uint16_t(alpha_bin<NSW>(sp_flip(sp_flip(sA, i), a)));
-      if(k == 0) abin[u] = uint16_t(alpha_bin<NSW>(sA));
-    }
     const int span = nvA - 1 - aa;
     const int64_t ninner = int64_t(nA - 1 - ii) * span;
     for(int64_t q = lane; q < ninner; q += 32) {
@@ -764,9 +793,9 @@ __global__ void __launch_bounds__(256)
       const double Gv =
           __ldg(I.G + size_t(a + size_t(i) * n) * n * n + b + size_t(j) * n);
       if(!(fabs(Gv) < tol)) {
-        const uint8_t g = grp[alpha_bin<NSW>(
+        const unsigned g = grp[alpha_bin<NSW>(
             sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b))];
-        if(g != 255) atomicAdd(cnt + g, 1);
+        if(g != 0xFFFFu) atomicAdd(cnt + g, 1);
       }
     }
     __syncwarp();
@@ -790,7 +819,7 @@ __global__ void __launch_bounds__(256)
 template <int NBITS>
 __global__ void __launch_bounds__(256)
     alpha_fill_k(Ints I, CoreData cd, const int32_t* rep, size_t nua, int nA,
-                 int nvA, double tol, const uint8_t* grp, AlphaLists al,
+                 int nvA, double tol, const uint16_t* grp, AlphaLists al,
                  uint16_t* qout) {
   using D = DetTraits<NBITS>;
   constexpr int NSW = D::NSW;
@@ -818,7 +847,7 @@ __global__ void __launch_bounds__(256)
     const int64_t ninner = int64_t(nA - 1 - ii) * span;
     for(int64_t q0 = 0; q0 < ninner; q0 += 32) {
       const int64_t q = q0 + lane;
-      unsigned g = 255;
+      unsigned g = 0xFFFFu;
       if(q < ninner) {
         const int qd = small_div(q, 1.0f / float(span));
         const int j = occA[ii + 1 + qd],
@@ -830,11 +859,11 @@ __global__ void __launch_bounds__(256)
               sp_flip(sp_flip(sp_flip(sp_flip(sA, i), j), a), b))];
       }
       const unsigned peers = __match_any_sync(0xffffffffu, g);
-      if(g != 255) {
+      if(g != 0xFFFFu) {
         out[run[g] + __popc(peers & lanemask_lt())] = uint16_t(q);
       }
       __syncwarp();
-      if(g != 255 && (peers & lanemask_lt()) == 0) run[g] += __popc(peers);
+      if(g != 0xFFFFu && (peers & lanemask_lt()) == 0) run[g] += __popc(peers);
       __syncwarp();
     }
   }
@@ -842,9 +871,10 @@ __global__ void __launch_bounds__(256)
 
 // Count pass of an unsplit range with alpha lists: one thread per unit.
 // Fixed-alpha units (kinds 1, 3, 4) are in the range as a whole, with the
-// count of the whole-search pass (ucnt); alpha doubles (kind 2) read their
-// group's list length. Alpha singles (kind 0, whose threshold test depends
-// on the beta string) are counted by units0_count_k.
+// count of the whole-search pass (ucnt); alpha doubles (kind 2) of listed
+// alpha strings read their group's list length. The alpha singles (kind 0,
+// whose threshold test depends on the beta string) and the alpha doubles of
+// unlisted strings are left to units_k's count pass (list_rest).
 __global__ void range_count_k(CoreData cd, AlphaLists al, int64_t U,
                               const int64_t* ucnt, const uint8_t* umask,
                               uint32_t blo, uint32_t bhi, int64_t* rc) {
@@ -860,7 +890,9 @@ __global__ void range_count_k(CoreData cd, AlphaLists al, int64_t U,
       const size_t ua = size_t(al.aidx[c]);
       uint32_t bin = ASCI_BINS;
       if(t < 2 + KA && t >= 2) {
-        const uint16_t* rr = al.rel + (ua * al.NK + size_t(t - 2)) * (al.G + 1);
+        const int32_t lb = al.lidx[ua];
+        if(lb < 0) continue;  // counted by units_k
+        const uint16_t* rr = al.rel + (size_t(lb) * al.NK + size_t(t - 2)) * (al.G + 1);
         r = int64_t(rr[al.g + 1]) - rr[al.g];
       } else if(t == 1 || t < 2 + KA + KB) {
         bin = al.abin[ua];
@@ -870,27 +902,6 @@ __global__ void range_count_k(CoreData cd, AlphaLists al, int64_t U,
       if(bin < ASCI_BINS && bin >= blo && bin < bhi) r = ucnt[u];
     }
     rc[u] = r;
-  }
-}
-
-// Alpha-single units (t = 0) of a range with alpha lists: one warp per core
-// det, the per-contribution path of unit_run.
-template <int NBITS>
-__global__ void __launch_bounds__(256)
-    units0_count_k(Ints I, CoreData cd, double E0, double tol,
-                   const uint8_t* umask, uint32_t blo, uint32_t bhi,
-                   int64_t* rc) {
-  const size_t nwarp = size_t(gridDim.x) * (blockDim.x >> 5);
-  for(size_t c = size_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      c < cd.ncdets; c += nwarp) {
-    const int64_t u = cd.uoff[c];
-    if(umask && !umask[u]) {
-      if((threadIdx.x & 31) == 0) rc[u] = 0;
-      continue;
-    }
-    unit_run<NBITS, 0>(I, cd, c, 0, E0, tol, rc + u, 0, nullptr, nullptr,
-                       nullptr, blo, bhi, 0u, 0u, nullptr, AlphaLists{},
-                       RankTables{});
   }
 }
 
@@ -1733,27 +1744,35 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     for(uint32_t b = bin_lo; b < bin_hi; ++b) Ppart += hh[b];
   }
   // alpha lists (AlphaLists) when the ranges need count passes of their own:
-  // memory for them, at most 15 % of what is free, comes off the range size
+  // bin tables for every distinct alpha string, and lists for as many of
+  // the strings shared by the most core dets as fit 15 % of the free memory
+  // (MACIS_B200_ASCI_ALPHA_LISTS: 0 none, N at most N listed strings); the
+  // memory comes off the range size
   SpinPlan ap;
   int g_est = 0;
+  size_t nlist = 0;
   const char* al_env = getenv("MACIS_B200_ASCI_ALPHA_LISTS");
-  const bool al_allowed = !(al_env && al_env[0] == '0');
-  if(al_allowed && !pairs_only && !st.just_singles && bin_lo < bin_hi &&
+  const long long al_max = al_env ? atoll(al_env) : -1;
+  if(al_max != 0 && !pairs_only && !st.just_singles && bin_lo < bin_hi &&
      ((part && part->count > 1) || Ppart > uint64_t(cap))) {
     ap = alpha_plan();
     if(ap.nu) {
-      g_est = int(std::min<uint64_t>(254, 2 * ((Ppart + cap - 1) / cap) + 2));
+      g_est = int(std::min<uint64_t>(1024, 2 * ((Ppart + cap - 1) / cap) + 2));
       const double nk = double(ap.ne) * ap.nv;
       const double pairs2 = double(ap.ne) * (ap.ne - 1) / 2 * double(ap.nv) *
                             (ap.nv - 1) / 2;
-      const double bytes =
-          double(ap.nu) * (nk * (18.0 + 2.0 * (g_est + 1)) + 2.0 * pairs2 + 2.0) +
-          4.0 * double(ncdets + ap.nu) + 8192.0;
-      if(bytes <= 0.15 * double(device_bytes_available())) {
+      const double fixed = 4.0 * double(ncdets + 2 * ap.nu) +
+                           2.0 * double(ap.nu) * (nk + 1.0) + 16384.0;
+      const double per_list = nk * (18.0 + 2.0 * (g_est + 1)) + 2.0 * pairs2;
+      const double budget = 0.15 * double(device_bytes_available()) - fixed;
+      if(budget < 0) {
+        ap = SpinPlan{};
+      } else {
+        nlist = std::min<size_t>(ap.nu, size_t(budget / per_list));
+        if(al_max > 0) nlist = std::min<size_t>(nlist, size_t(al_max));
+        const double bytes = fixed + double(nlist) * per_list;
         if(!cap_env)
           cap = std::max<int64_t>(cap - int64_t(bytes / per_pair), int64_t(1) << 20);
-      } else {
-        ap = SpinPlan{};
       }
     }
   }
@@ -1795,39 +1814,64 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
     int G = 0;
     for(uint32_t r = 0; r < nr; ++r)
       if(rns[r] == 0) rgrp[r] = G++;
-    if(G > g_est || G == 0 || (G < 2 && 2 * ap.nu > ncdets)) {
+    if(G == 0) {
       std::fill(rgrp.begin(), rgrp.end(), -1);
     } else {
-      std::vector<uint8_t> gt(ASCI_BINS, 255);
+      // lists only where their memory was planned and they pay
+      if(G > g_est || (G < 2 && 2 * ap.nu > ncdets)) nlist = 0;
+      std::vector<uint16_t> gt(ASCI_BINS, 0xFFFFu);
       for(uint32_t r = 0; r < nr; ++r)
         if(rgrp[r] >= 0)
-          for(uint32_t b = rlo[r]; b < rhi[r]; ++b) gt[b] = uint8_t(rgrp[r]);
-      uint8_t* grp = A.get<uint8_t>(ASCI_BINS);
-      MB_CUDA(cudaMemcpyAsync(grp, gt.data(), ASCI_BINS, cudaMemcpyHostToDevice, s));
+          for(uint32_t b = rlo[r]; b < rhi[r]; ++b) gt[b] = uint16_t(rgrp[r]);
+      // list blocks: the alpha strings of the most core dets first
+      std::vector<int32_t> mult(ap.nu, 0), order(ap.nu), lx(ap.nu, -1),
+          lrep(nlist + 1, 0);
+      for(size_t c = 0; c < ncdets; ++c) ++mult[ap.idx[c]];
+      for(size_t u = 0; u < ap.nu; ++u) order[u] = int32_t(u);
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int32_t x, int32_t y) { return mult[x] > mult[y]; });
+      for(size_t b = 0; b < nlist; ++b) {
+        lx[order[b]] = int32_t(b);
+        lrep[b] = ap.rep[order[b]];
+      }
+      uint16_t* grp = A.get<uint16_t>(ASCI_BINS);
+      MB_CUDA(cudaMemcpyAsync(grp, gt.data(), ASCI_BINS * 2,
+                              cudaMemcpyHostToDevice, s));
       int32_t* aidx = A.get<int32_t>(ncdets);
       int32_t* rep = A.get<int32_t>(ap.nu);
+      int32_t* lidx = A.get<int32_t>(ap.nu);
+      int32_t* lrp = A.get<int32_t>(nlist + 1);
       MB_CUDA(cudaMemcpyAsync(aidx, ap.idx.data(), ncdets * 4,
                               cudaMemcpyHostToDevice, s));
       MB_CUDA(cudaMemcpyAsync(rep, ap.rep.data(), ap.nu * 4,
                               cudaMemcpyHostToDevice, s));
+      MB_CUDA(cudaMemcpyAsync(lidx, lx.data(), ap.nu * 4,
+                              cudaMemcpyHostToDevice, s));
+      MB_CUDA(cudaMemcpyAsync(lrp, lrep.data(), (nlist + 1) * 4,
+                              cudaMemcpyHostToDevice, s));
       al.aidx = aidx;
+      al.lidx = lidx;
       al.NK = ap.ne * ap.nv;
       al.G = G;
-      const size_t rows = ap.nu * size_t(al.NK);
+      const size_t brows = ap.nu * size_t(al.NK);
       uint16_t* abin = A.get<uint16_t>(ap.nu);
-      uint16_t* kbin = A.get<uint16_t>(rows + 1);
-      uint16_t* rel = A.get<uint16_t>(rows * (G + 1) + 1);
-      int64_t* base = A.get<int64_t>(rows + 1);
+      uint16_t* kbin = A.get<uint16_t>(brows + 1);
       al.abin = abin;
       al.kbin = kbin;
+      if(brows)
+        alpha_bins_k<NBITS><<<grid_for(brows, 256, 16 * sms), 256, 0, s>>>(
+            cd, rep, ap.nu, ap.nv, al.NK, kbin, abin), note_launch();
+      const size_t rows = nlist * size_t(al.NK);
+      uint16_t* rel = A.get<uint16_t>(rows * (G + 1) + 1);
+      int64_t* base = A.get<int64_t>(rows + 1);
       al.rel = rel;
       al.base = base;
       const size_t smem = 8 * size_t(G + 1) * sizeof(int);
       if(rows) {
         int64_t* tot = A.get<int64_t>(rows + 1);
         alpha_count_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
-                               s>>>(I, cd, rep, ap.nu, ap.ne, ap.nv,
-                                    st.h_el_tol, grp, al, rel, kbin, abin, tot),
+                               s>>>(I, cd, lrp, nlist, ap.ne, ap.nv,
+                                    st.h_el_tol, grp, al, rel, tot),
             note_launch();
         MB_CUDA(cudaGetLastError());
         exclusive_scan<int64_t, int64_t>(tot, base, rows, base + rows, A);
@@ -1838,10 +1882,10 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
       al.q = ql;
       if(E)
         alpha_fill_k<NBITS><<<grid_for(rows * 32, 256, 16 * sms), 256, smem,
-                              s>>>(I, cd, rep, ap.nu, ap.ne, ap.nv,
+                              s>>>(I, cd, lrp, nlist, ap.ne, ap.nv,
                                    st.h_el_tol, grp, al, ql), note_launch();
       MB_CUDA(cudaGetLastError());
-      stats.alpha_strings = ap.nu;
+      stats.alpha_strings = nlist;
     }
   }
   stats.pairs_ms = ms_since(t_all);
@@ -1918,9 +1962,11 @@ static void asci_impl(macis_b200_ham* h, const macis_b200_asci_settings& st,
         alr.g = rgrp[rr];
         range_count_k<<<grid_for(size_t(U), 256, 16 * sms), 256, 0, s>>>(
             cd, alr, U, ucnt, umask, rlo[rr], rhi[rr], rc), note_launch();
-        units0_count_k<NBITS><<<grid_for(ncdets * 32, 256, 16 * sms), 256, 0,
-                                s>>>(I, cd, E0, st.h_el_tol, umask, rlo[rr],
-                                     rhi[rr], rc), note_launch();
+        // alpha singles and the alpha doubles of unlisted strings
+        units_k<NBITS, 0><<<grid_for(size_t(U), 256, 32 * sms), 256, 0, s>>>(
+            I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc, nullptr, nullptr,
+            nullptr, umask, nullptr, rlo[rr], rhi[rr], rns[rr], rsub[rr],
+            nullptr, alr, RankTables{}), note_launch();
       } else {
         units_k<NBITS, 0><<<grid_for(size_t(U), 256, 32 * sms), 256, 0,
                             s>>>(I, cd, 0, U, 0, ncdets, E0, st.h_el_tol, rc,

@@ -286,6 +286,7 @@ def test_ranked_keys_and_alpha_lists_match_plain_search(monkeypatch, nbits, n,
     beta string ranks; the default above 2^22 contributions), and candidate
     ranges that take their alpha-double counts and contributions from
     per-alpha-string lists (the default once a search needs several ranges)
+    for the most frequent alpha strings only (MACIS_B200_ASCI_ALPHA_LISTS=3)
     or test every contribution's bin (MACIS_B200_ASCI_ALPHA_LISTS=0), with a
     range cap that leaves every range whole and one small enough to split
     the heaviest alpha-string bin by beta string. Identical accumulated
@@ -301,9 +302,12 @@ def test_ranked_keys_and_alpha_lists_match_plain_search(monkeypatch, nbits, n,
     rec = mb.ScreenSettings(network=mb.ScreeningNetwork(nbits=nbits, seed=1),
                             max_samples=200000)
 
-    def run(ranks, lists="1", cap=None):
+    def run(ranks, lists=None, cap=None):
         monkeypatch.setenv("MACIS_B200_ASCI_RANKS", ranks)
-        monkeypatch.setenv("MACIS_B200_ASCI_ALPHA_LISTS", lists)
+        if lists is None:
+            monkeypatch.delenv("MACIS_B200_ASCI_ALPHA_LISTS", raising=False)
+        else:
+            monkeypatch.setenv("MACIS_B200_ASCI_ALPHA_LISTS", lists)
         if cap is None:
             monkeypatch.delenv("MACIS_B200_ASCI_BATCH_PAIRS", raising=False)
         else:
@@ -335,9 +339,11 @@ def test_ranked_keys_and_alpha_lists_match_plain_search(monkeypatch, nbits, n,
     assert np.array_equal(pr[0], pp[0]) and np.array_equal(pr[1], pp[1])
     raw = st["raw_pairs"]
     for cap in (raw // 12, raw // 150):
-        for ranks, lists in (("1", "1"), ("1", "0"), ("0", "1")):
+        for ranks, lists in (("1", None), ("1", "0"), ("0", None), ("1", "3")):
             got = run(ranks, lists, cap)
             assert got[3]["batches"] > 3
-            assert (got[3]["alpha_strings"] > 0) == (lists == "1")
+            assert (got[3]["alpha_strings"] > 0) == (lists != "0")
+            if lists == "3":
+                assert got[3]["alpha_strings"] == 3
             assert (got[3]["key_bits"] > 0) == (ranks == "1")
             same(got, plain)
