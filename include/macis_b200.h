@@ -80,9 +80,10 @@ typedef struct {
   uint64_t sort_pass_items; /* sum over the sorted candidate ranges of
                                (radix digit passes x records): each pass
                                reads and writes every record once */
-  uint64_t alpha_strings;   /* distinct alpha strings of the core dets when
-                               the candidate ranges used per-alpha-string
-                               lists of the alpha doubles, else 0 */
+  uint64_t alpha_strings;   /* alpha strings of the core dets whose alpha
+                               doubles the candidate ranges read from
+                               per-range lists (those shared by the most
+                               core dets), else 0 */
   uint64_t key_bits;        /* bits of the ranked candidate keys (alpha and
                                beta string ranks) the candidates were sorted
                                by, 0 when sorted by the determinant bitset */
