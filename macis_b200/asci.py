@@ -13,6 +13,7 @@ The search returns the top-k states in ascending determinant order followed
 by the core determinants; the reference returns them in nth_element order.
 """
 import ctypes as ct
+import dataclasses
 import logging
 import time
 from dataclasses import dataclass, field
@@ -238,21 +239,42 @@ def _use_net(screen, ham_gen, cdets, E0, C):
     return use_net
 
 
-def _recall_check(screen, use_net, st, got, ncore, ham_gen, exact_search):
+def _recall_check(screen, use_net, st, got, ncore, ham_gen, exact_search,
+                  pruned_search):
     """The recall check of ScreenSettings after a pruning search `got` with
     statistics st: when it applies, the exact search of the same core set
     (exact_search(), recording unbiased samples for the training that
-    follows) replaces the result, its top-k recall is measured and
-    keep_frac doubles below recall_target. Returns (dets, recall or None,
+    follows) replaces the result and the top-k recall of `got` against it
+    is measured. Below recall_target keep_frac doubles. At or above it,
+    pruned_search(k) (no recording) tries halving keep_frac, down to
+    keep_min, while the recall stays at the target; keep_frac becomes the
+    smallest fraction that met it. Returns (dets, recall or None,
     statistics for the training)."""
     if not (use_net and screen.recall_target and
             st["units_total"] <= screen.check_units_max):
         return got, None, st
     exact = exact_search()
+    st_train = dict(st, samples=last_search_stats(ham_gen)["samples"])
     recall = topk_recall(got, exact, ncore)
     if recall < screen.recall_target:
         screen.keep_frac = min(1.0, 2.0 * screen.keep_frac)
-    return exact, recall, dict(st, samples=last_search_stats(ham_gen)["samples"])
+    else:
+        k = screen.keep_frac
+        while k / 2.0 >= screen.keep_min:
+            trial = pruned_search(k / 2.0)
+            if topk_recall(trial, exact, ncore) < screen.recall_target:
+                break
+            k /= 2.0
+        screen.keep_frac = k
+    return exact, recall, st_train
+
+
+def _trial_search(screen, search):
+    """pruned_search for _recall_check: the same network at keep fraction k,
+    without recording samples."""
+    def run(k):
+        return search(dataclasses.replace(screen, keep_frac=k, train=False))
+    return run
 
 
 def _train_after_search(screen, stats):
@@ -289,7 +311,10 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
     wfn, recall, st = _recall_check(
         screen, use_net, st, wfn, nkeep, ham_gen,
         lambda: asci_search(asci_settings, ndets_max, core, E0, Cc, norb,
-                            ham_gen, screen=screen, use_net=False))
+                            ham_gen, screen=screen, use_net=False),
+        _trial_search(screen, lambda sc: asci_search(
+            asci_settings, ndets_max, core, E0, Cc, norb, ham_gen, screen=sc,
+            use_net=True)))
     t1 = time.perf_counter()
     train_ms = _train_after_search(screen, st)
     t1b = time.perf_counter()

@@ -427,8 +427,9 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
     eigenvector all-gathered to every rank. screen as in asci.asci_iter,
     with an equal network on every rank. Only the reference solver is
     distributed: FP64 values, no thick restart."""
-    from .asci import (_dets, _recall_check, _train_after_search, _use_net,
-                       last_search_stats, reorder_ci_on_coeff)
+    from .asci import (_dets, _recall_check, _train_after_search,
+                       _trial_search, _use_net, last_search_stats,
+                       reorder_ci_on_coeff)
     from .solvers import FP64
     if mcscf_settings.precision != FP64 or mcscf_settings.davidson_restart_keep:
         raise NotImplementedError(
@@ -449,7 +450,10 @@ def asci_iter(asci_settings, mcscf_settings, ndets_max, E0, wfn, X, ham_gen,
         wfn, _, st = _recall_check(
             screen, use_net, last_search_stats(ham_gen), wfn, nkeep, ham_gen,
             lambda: asci_search(asci_settings, ndets_max, core, E0, Cc, norb,
-                                ham_gen, group, screen=screen, use_net=False))
+                                ham_gen, group, screen=screen, use_net=False),
+            _trial_search(screen, lambda sc: asci_search(
+                asci_settings, ndets_max, core, E0, Cc, norb, ham_gen, group,
+                screen=sc, use_net=True)))
         _train_after_search(screen, st)
     E, X_local = selected_ci_diag(wfn, ham_gen, mcscf_settings.ci_matel_tol,
                                   mcscf_settings.ci_max_subspace,

@@ -149,11 +149,14 @@ class ScreenSettings:
     searches: int = 0             # searches run so far (updated)
     # Recall check: a pruning search of asci_iter / asci_grow / asci_refine
     # with at most check_units_max units is also run exactly; its top-k
-    # recall against the exact selection is measured, the exact selection is
-    # kept, and below recall_target keep_frac doubles (at 1 pruning stops).
-    # 0 turns the check off.
+    # recall against the exact selection is measured and the exact
+    # selection is kept. Below recall_target keep_frac doubles (at 1 pruning
+    # stops); at or above it, pruned searches of the same core set at half
+    # the fraction (down to keep_min) are tried, and keep_frac becomes the
+    # smallest that meets the target. recall_target 0 turns the check off.
     recall_target: float = 0.95
     check_units_max: int = 20_000_000
+    keep_min: float = 0.2
 
     def c_struct(self, use_net):
         return _lib.AsciScreenC(

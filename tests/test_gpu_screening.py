@@ -238,7 +238,8 @@ def test_recall_check_keeps_exact_selections():
     selection: a screened grow follows the unscreened grow determinant for
     determinant, the measured recalls are logged, and keep_frac doubles
     after every check below recall_target (above 1 here, so every check
-    fails) until pruning stops at keep_frac 1."""
+    fails) until pruning stops at keep_frac 1; a check that passes halves
+    keep_frac down to keep_min."""
     norb, nbits, na, nb = 16, 64, 5, 5
     T, V, H = _ham(norb, nbits, seed=2)
     _, _, (E0, d0, X0) = _grow(H, norb, nbits, na, nb, 6000, 1500)
@@ -264,3 +265,14 @@ def test_recall_check_keeps_exact_selections():
     assert m2.iteration_log[-1]["screened"]
     assert m2.iteration_log[-1]["recall_check"] is not None
     assert sc2.keep_frac == 0.2
+    # a check that passes tries halving keep_frac, down to keep_min, while
+    # the trial searches keep the recall (here always: a tiny target)
+    sc3 = mb.ScreenSettings(network=scr.network, recall_target=1e-9,
+                            keep_frac=0.8, keep_min=0.2, min_units=0,
+                            check_units_max=10 ** 12)
+    sc3.searches = sc3.warmup_searches
+    E3, d3, _ = mb.asci_iter(s, m2, 6000, E1, d1, X1, H, norb, sc3)
+    assert sc3.keep_frac == 0.2
+    # the selection is still the exact search's
+    E4, d4, _ = mb.asci_iter(s, m2, 6000, E1, d1, X1, H, norb, None)
+    assert np.array_equal(d3, d4) and abs(E3 - E4) < 1e-9
