@@ -1459,17 +1459,20 @@ static int build_ranks(const SpinPlan& pa, const SpinPlan& pb, size_t ncdets,
   const size_t ta = pa.nu * size_t(spin_candidates(pa.ne, pa.nv));
   const size_t tb = pb.nu * size_t(spin_candidates(pb.ne, pb.nv));
   if(ta >= (size_t(1) << 32) - 1 || tb >= (size_t(1) << 32) - 1) return 0;
+  // the rank tables (4 B per candidate) first; the distinct candidate
+  // strings, far fewer where core strings share candidates, are checked
+  // once they are known
   const double avail = double(device_bytes_available());
-  const double persist = (4.0 + 8.0 * NSW + 2.0) * double(ta + tb) +
-                         8.0 * double(ncdets);
+  const double tables = 4.0 * double(ta + tb) + 8.0 * double(ncdets);
   const double trans = double(std::max(ta, tb)) * (16.0 * NSW + 20.0);
-  if(persist > 0.1 * avail || persist + trans > 0.5 * avail) return 0;
+  if(tables > 0.1 * avail || tables + trans > 0.5 * avail) return 0;
   uint64_t *La = nullptr, *Lb = nullptr;
   SpinRanks ra, rb;
   const size_t na = build_spin_ranks<NBITS>(pa, A, s, ra, &La);
   const size_t nb = build_spin_ranks<NBITS>(pb, A, s, rb, &Lb);
   const int ba = bits_for(na), bb = bits_for(nb);
-  if(ba + bb > 64) {
+  const double strings = (8.0 * NSW + 2.0) * double(na) + 8.0 * NSW * double(nb);
+  if(ba + bb > 64 || tables + strings > 0.15 * avail) {
     for(const void* q : {static_cast<const void*>(ra.R),
                          static_cast<const void*>(rb.R),
                          static_cast<const void*>(La),
