@@ -182,6 +182,68 @@ def test_screening_decision_and_retraining():
     assert [c[0] for c in net.calls] == ["train"]
 
 
+def test_recall_check_policy(monkeypatch):
+    """The recall check's decisions (asci._recall_check), with stand-ins for
+    the searches: no check for unscreened or large searches; the exact
+    selection replaces the pruned one; keep_frac doubles below the target
+    (at most 1) and otherwise halves through trial searches while they keep
+    the target, not below keep_min; training uses the exact search's
+    sample count; and topk_recall counts the exact search's new
+    determinants found by the other."""
+    from macis_b200 import asci
+    monkeypatch.setattr(asci, "last_search_stats",
+                        lambda h: {"samples": 77})
+    ncore = 2
+    exact = np.arange(24, dtype=np.uint64).reshape(12, 2)   # 10 new + 2 core
+    half = exact.copy()
+    half[:5] += 1000                                       # 5 of 10 found
+    assert mb.topk_recall(exact, exact, ncore) == 1.0
+    assert mb.topk_recall(half, exact, ncore) == 0.5
+    net = _FakeNet(trained_steps=1)
+    st = {"units_total": 100, "samples": 5}
+    trials = []
+
+    def check(sc, got, recall_of_trial):
+        def pruned(k):
+            trials.append(k)
+            return exact if recall_of_trial(k) else half
+        return asci._recall_check(sc, True, st, got, ncore, None,
+                                  lambda: exact, pruned)
+
+    sc = mb.ScreenSettings(network=net, keep_frac=0.4, keep_min=0.1,
+                           check_units_max=1000)
+    # not screened, or too many units: no check, the result is kept
+    assert asci._recall_check(sc, False, st, half, ncore, None,
+                              None, None) == (half, None, st)
+    big = dict(st, units_total=10 ** 6)
+    assert asci._recall_check(sc, True, big, half, ncore, None, None,
+                              None)[1] is None
+    # below the target: doubles, no trials, exact selection and samples
+    dets, rec, st2 = check(sc, half, lambda k: True)
+    assert dets is exact and rec == 0.5 and st2["samples"] == 77
+    assert sc.keep_frac == 0.8 and trials == []
+    check(sc, half, lambda k: True)
+    assert sc.keep_frac == 1.0
+    check(sc, half, lambda k: True)
+    assert sc.keep_frac == 1.0
+    # at the target: halves while the trials keep it (0.8 -> 0.4 -> 0.2)
+    sc.keep_frac = 0.8
+    dets, rec, _ = check(sc, exact, lambda k: k >= 0.2)
+    assert rec == 1.0 and sc.keep_frac == 0.2 and trials == [0.4, 0.2, 0.1]
+    # down to keep_min, never below
+    trials.clear()
+    sc.keep_frac = 0.2
+    check(sc, exact, lambda k: True)
+    assert sc.keep_frac == 0.1 and trials == [0.1]
+    trials.clear()
+    check(sc, exact, lambda k: True)
+    assert sc.keep_frac == 0.1 and trials == []
+    # recall_target 0: the check is off
+    sc.recall_target = 0.0
+    assert asci._recall_check(sc, True, st, half, ncore, None, None,
+                              None)[1] is None
+
+
 def test_product_does_not_use_the_oracle():
     """The package (the product path) imports neither the oracle nor any
     working file; only the tests, smoke() and bench.py's baseline legs do."""
